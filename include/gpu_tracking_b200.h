@@ -1,0 +1,201 @@
+/*
+ * gpu_tracking_b200 — C ABI of the B200 particle locating + linking engine.
+ *
+ * This is the drop-in boundary for the hot path of amfaber/gpu_tracking
+ * (Crocker–Grier / LoG locate -> characterize -> filter_close -> doughnut ->
+ * trackpy-style subnet linking).  Every entry point takes plain pointers and
+ * sizes; no CUDA or torch types cross it.  Each declaration names the
+ * reference interface it replaces (file:line within the reference project).
+ *
+ * Conventions
+ *   - Frames are C-contiguous (T, H, W) arrays, row index first ("y" in the
+ *     output table is the row coordinate, "x" the column coordinate, exactly
+ *     as src/execute_gpu.rs:482-519 names them).
+ *   - A frame pointer may be host memory or device memory of the context's
+ *     device; the library detects which (cudaPointerGetAttributes).
+ *   - Status codes mirror the reference's error enum (src/error.rs:5-94) plus
+ *     GT_ERR_CAPACITY_EXCEEDED / GT_ERR_CUDA for conditions the reference
+ *     either truncates silently or panics on.
+ *   - Result tables are library-allocated; free them with gt_table_free.
+ *   - One context per host thread.  Calls are synchronous at the ABI.
+ */
+#ifndef GPU_TRACKING_B200_H
+#define GPU_TRACKING_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum gt_status {
+    GT_OK = 0,
+    GT_ERR_INVALID_ARGUMENT = 1,          /* Error::WrongBuilder and bad parameters   (src/error.rs:92)  */
+    GT_ERR_DIMENSION_MISMATCH = 2,        /* Error::DimensionMismatch                 (src/error.rs:20)  */
+    GT_ERR_EMPTY_ITERATOR = 3,            /* Error::EmptyIterator                     (src/error.rs:27)  */
+    GT_ERR_NON_SORTED_CHARACTERIZATION = 4, /* Error::NonSortedCharacterization       (src/error.rs:30)  */
+    GT_ERR_FRAME_OUT_OF_BOUNDS = 5,       /* Error::FrameOutOfBounds                  (src/error.rs:33)  */
+    GT_ERR_NON_STANDARD_ARRAY_LAYOUT = 6, /* Error::NonStandardArrayLayout            (src/error.rs:49)  */
+    GT_ERR_ARRAY_DIMENSIONS = 7,          /* Error::ArrayDimensionsError              (src/error.rs:58)  */
+    GT_ERR_TOO_DENSE_TO_LINK = 8,         /* Error::TooDenseToLink                    (src/error.rs:77)  */
+    GT_ERR_INTERRUPTED = 9,               /* Error::Interrupted                       (src/error.rs:83)  */
+    GT_ERR_CAPACITY_EXCEEDED = 10,        /* reference truncates silently (src/gpu_setup.rs:246-253)      */
+    GT_ERR_CUDA = 11,                     /* ~ Error::GpuDeviceError                  (src/error.rs:11)  */
+    GT_ERR_NO_DEVICE = 12,                /* ~ Error::GpuAdapterError                 (src/error.rs:8)   */
+    GT_ERR_SUBNET_TOO_EXPENSIVE = 13,     /* device subnet search exceeded its step budget (no ref analogue) */
+    GT_ERR_INTERNAL = 14
+} gt_status;
+
+/* ------------------------------------------------------------- parameters */
+typedef enum gt_style { GT_STYLE_TRACKPY = 0, GT_STYLE_LOG = 1 } gt_style;
+
+typedef enum gt_dtype { GT_DTYPE_U16 = 0, GT_DTYPE_F32 = 1, GT_DTYPE_U8 = 2 } gt_dtype;
+
+/*
+ * Mirror of the reference's TrackingParams + ParamStyle
+ * (src/gpu_setup.rs:10-59).  Option<T> fields carry an explicit has_* flag.
+ * Trackpy-only fields that the reference accepts and ignores (maxsize,
+ * threshold, invert, percentile, topn, preprocess) are not represented.
+ */
+typedef struct gt_params {
+    int32_t style;                 /* gt_style                                                */
+    /* ParamStyle::Trackpy */
+    uint32_t diameter;
+    uint32_t separation;
+    int32_t filter_close;
+    /* ParamStyle::Log */
+    float min_radius;
+    float max_radius;
+    uint32_t n_radii;
+    int32_t log_spacing;
+    float overlap_threshold;
+    /* common */
+    float minmass;
+    uint32_t max_iterations;
+    int32_t characterize;
+    int32_t has_search_range;  float search_range;
+    uint32_t memory;                                   /* memory.unwrap_or(0)                 */
+    int32_t doughnut_correction;
+    int32_t has_bg_radius;     float bg_radius;
+    int32_t has_gap_radius;    float gap_radius;
+    int32_t has_snr;           float snr;
+    int32_t has_minmass_snr;   float minmass_snr;
+    int32_t truncate_preprocessed;
+    int32_t has_illumination_sigma; float illumination_sigma;
+    int32_t illumination_correction_per_frame;
+    int32_t has_adaptive_background; uint32_t adaptive_background;
+    int32_t include_r_in_output;
+    float shift_threshold;
+    float noise_size;
+    int32_t has_smoothing_size; uint32_t smoothing_size;
+} gt_params;
+
+/* TrackingParams::default() (src/gpu_setup.rs:61-97). */
+void gt_params_default(gt_params* p);
+
+/* ------------------------------------------------------------- context */
+typedef struct gt_ctx gt_ctx;
+
+/* new_adapter + new_device_queue (src/gpu_setup.rs:582-609): binds a device. */
+gt_status gt_create(int32_t device, gt_ctx** out);
+void gt_destroy(gt_ctx* ctx);
+/* Human-readable message of the last failing call on this context. */
+const char* gt_last_error(const gt_ctx* ctx);
+/* Cooperative interrupt (the reference's Arc<AtomicBool>, src/execute_gpu.rs:1094-1099):
+ * a non-zero *flag makes the running call return GT_ERR_INTERRUPTED between
+ * frame chunks.  Pass NULL to clear. */
+gt_status gt_set_interrupt(gt_ctx* ctx, const volatile int32_t* flag);
+/* Progress of the running/last call: (frames done, frames total), the
+ * reference's Arc<Mutex<(usize, Option<usize>)>> (src/execute_gpu.rs:972-975). */
+gt_status gt_progress(const gt_ctx* ctx, int64_t* done, int64_t* total);
+
+/* ------------------------------------------------------------ result table */
+typedef struct gt_table gt_table;
+
+/* Superset of the reference's output columns (src/execute_gpu.rs:482-519)
+ * plus two diagnostics the reference computes but does not emit. */
+typedef enum gt_column {
+    GT_COL_FRAME = 0, GT_COL_Y, GT_COL_X, GT_COL_MASS, GT_COL_R,
+    GT_COL_RG, GT_COL_RAW, GT_COL_SIGNAL, GT_COL_ECC,
+    GT_COL_RAW_MASS, GT_COL_RAW_BG_MEDIAN, GT_COL_RAW_MASS_CORRECTED,
+    GT_COL_PARTICLE, GT_COL_DURATION,
+    GT_COL_MAX_INTENSITY, GT_COL_COUNT,
+    GT_NUM_COLUMNS
+} gt_column;
+
+int64_t gt_table_nrows(const gt_table* t);
+/* Copy one column to host memory as float32 (all value columns, and the
+ * integer columns converted the way the reference stores them). */
+gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst);
+/* Copy an integer column (frame / particle / duration) as int64. */
+gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst);
+/* 1 if the column was computed for this table (e.g. GT_COL_PARTICLE only
+ * when linking ran). */
+int32_t gt_table_has_column(const gt_table* t, int32_t column);
+void gt_table_free(gt_table* t);
+
+/* ---------------------------------------------------------------- entry points */
+/*
+ * Locate + characterize + filter_close + doughnut + link over a video.
+ * Replaces execute_ndarray / execute_provider / execute_gpu
+ * (src/execute_gpu.rs:1378-1403, 1272-1352, 886-1184), i.e. the pyo3
+ * functions batch_rust and LoG_rust (gpu_tracking_macros/src/lib.rs:57-156).
+ * style selects Crocker–Grier (batch) or LoG.
+ * frame_numbers (nullable, length T) gives the frame index written to the
+ * "frame" column and used for linker_reset_points; NULL means 0..T-1 (the
+ * reference's `frames`/keys selection, src/execute_gpu.rs:1041-1077).
+ * linker_reset_points (nullable, length n_reset) mirrors
+ * TrackingParams::linker_reset_points (src/execute_gpu.rs:792-798).
+ */
+gt_status gt_batch(gt_ctx* ctx, const gt_params* params,
+                   const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
+                   const int64_t* frame_numbers,
+                   const int64_t* linker_reset_points, int64_t n_reset,
+                   gt_table** out);
+
+/*
+ * Characterize given points instead of detected ones.  Replaces
+ * characterize_points_rust (gpu_tracking_macros/src/lib.rs:641-683) and the
+ * FrameSubsetter characterization path (src/execute_gpu.rs:189-229,
+ * src/linking.rs:97-196).  points is row-major (n_points, ncols) float32 with
+ * columns [frame,] y, x [, r] according to has_frames / has_r.
+ */
+gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params,
+                                 const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
+                                 const float* points, int64_t n_points,
+                                 int32_t has_frames, int32_t has_r,
+                                 gt_table** out);
+
+/*
+ * Link detections.  Replaces link_rust (gpu_tracking_python/src/python_bindings.rs:275-291)
+ * -> linker_all (src/linking.rs:818-831).  frame_y_x is row-major (n, 3)
+ * float32, sorted by frame.  particle_out receives one id per row.
+ */
+gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n,
+                  float search_range, uint32_t memory, int64_t* particle_out);
+
+/*
+ * Connect two detection sets frame by frame.  Replaces connect_rust
+ * (gpu_tracking_python/src/python_bindings.rs:293-312) -> connect_all
+ * (src/linking.rs:960-1020).
+ */
+gt_status gt_connect(gt_ctx* ctx, const float* frame_y_x1, int64_t n1,
+                     const float* frame_y_x2, int64_t n2, float search_range,
+                     int64_t* out1, int64_t* out2);
+
+/*
+ * Mean frame of a video (src/execute_gpu.rs:819-847, mean_from_file_rust
+ * gpu_tracking_python/src/python_bindings.rs:361-371), out is (H, W) float32.
+ */
+gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype,
+                        int64_t T, int32_t H, int32_t W, float* out);
+
+/* Library version string. */
+const char* gt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPU_TRACKING_B200_H */

@@ -1,0 +1,245 @@
+// ref_driver.cpp — runs the reference's own WGSL shaders on the CPU.
+//
+// TEST INFRASTRUCTURE ONLY (part of the oracle).  The shader bodies are
+// included from oracle/_ref/gen_*.inc, which oracle/wgsl2cpp.py generates
+// from the reference checkout at build time; this file only provides the
+// WGSL builtins and dispatches the shaders in the reference's pass order
+// (src/gpu_setup.rs:872-895, src/execute_gpu.rs:231-286 and 368-375,
+// src/utils.rs:114-296 for Laplace<2>), one invocation at a time in
+// row-major order (the canonical order for the reference's atomics).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+struct vec2f {
+    float v[2];
+    vec2f() : v{0.0f, 0.0f} {}
+    vec2f(float a, float b) : v{a, b} {}
+    float& operator[](int i) { return v[i]; }
+    float operator[](int i) const { return v[i]; }
+};
+struct ivec2 {
+    int32_t v[2];
+    ivec2() : v{0, 0} {}
+    ivec2(int32_t a, int32_t b) : v{a, b} {}
+    int32_t& operator[](int i) { return v[i]; }
+    int32_t operator[](int i) const { return v[i]; }
+};
+struct uvec3 {
+    uint32_t x, y, z;
+    uint32_t operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+
+inline float wgsl_f32(float x) { return x; }
+inline float wgsl_f32(int32_t x) { return (float)x; }
+inline float wgsl_f32(uint32_t x) { return (float)x; }
+inline int32_t wgsl_i32(int32_t x) { return x; }
+inline int32_t wgsl_i32(uint32_t x) { return (int32_t)x; }
+inline int32_t wgsl_i32(float x) {
+    if (std::isnan(x)) return 0;
+    if (x >= 2147483647.0f) return INT32_MAX;
+    if (x <= -2147483648.0f) return INT32_MIN;
+    return (int32_t)x;
+}
+inline uint32_t wgsl_u32(uint32_t x) { return x; }
+inline uint32_t wgsl_u32(int32_t x) { return (uint32_t)x; }
+inline uint32_t wgsl_u32(float x) { return x <= 0.0f ? 0u : (uint32_t)x; }
+inline float wgsl_exp(float x) { return std::exp(x); }
+inline float wgsl_sqrt(float x) { return std::sqrt(x); }
+inline float wgsl_atan2(float y, float x) { return std::atan2(y, x); }
+inline float wgsl_sin(float x) { return std::sin(x); }
+inline float wgsl_cos(float x) { return std::cos(x); }
+inline float wgsl_ceil(float x) { return std::ceil(x); }
+inline float wgsl_round(float x) { return std::rint(x); }  // WGSL: round half to even
+inline float wgsl_max(float a, float b) { return (a < b) ? b : a; }
+inline int32_t wgsl_max(int32_t a, int32_t b) { return (a < b) ? b : a; }
+inline float wgsl_fma(float a, float b, float c) { return std::fmaf(a, b, c); }
+inline uint32_t wgsl_atomicAdd(uint32_t* p, uint32_t v) {
+    uint32_t o = *p;
+    *p += v;
+    return o;
+}
+
+#include "_ref/gen_preprocess_rows.inc"
+#include "_ref/gen_preprocess_cols_trunc.inc"
+#include "_ref/gen_preprocess_cols_notrunc.inc"
+#include "_ref/gen_max_rows.inc"
+#include "_ref/gen_extract_max.inc"
+#include "_ref/gen_walk.inc"
+#include "_ref/gen_characterize.inc"
+#include "_ref/gen_characterize_points.inc"
+#include "_ref/gen_separable_log.inc"
+#include "_ref/gen_logspace_max.inc"
+
+// Flat copy of the WGSL Params uniform (params.wgsl:1-20).
+struct RefParams {
+    int32_t pic_nrows, pic_ncols, preprocess_nrows, preprocess_ncols;
+    float sigma2;
+    int32_t circle_nrows, circle_ncols, dilation_nrows, dilation_ncols;
+    uint32_t max_iterations;
+    float threshold, minmass;
+    int32_t margin;
+    float snr, minmass_snr, rough_snr_factor;
+};
+
+template <class P>
+void set_params(P& dst, const RefParams* src) {
+    static_assert(sizeof(P) == sizeof(RefParams), "Params layout");
+    std::memcpy(&dst, src, sizeof(RefParams));
+}
+
+template <class F>
+void dispatch2d(int32_t H, int32_t W, F&& f) {
+    for (int32_t x = 0; x < H; x++)
+        for (int32_t y = 0; y < W; y++) f(uvec3{(uint32_t)x, (uint32_t)y, 0u});
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_preprocess(const RefParams* p, int32_t truncate, const float* frame, float* processed) {
+    const int32_t H = p->pic_nrows, W = p->pic_ncols;
+    std::vector<vec2f> temp((size_t)H * W);
+    set_params(sh_preprocess_rows::params, p);
+    sh_preprocess_rows::picture = const_cast<float*>(frame);
+    sh_preprocess_rows::temp = temp.data();
+    dispatch2d(H, W, [](uvec3 g) { sh_preprocess_rows::main_(g); });
+    if (truncate) {
+        set_params(sh_preprocess_cols_trunc::params, p);
+        sh_preprocess_cols_trunc::temp = temp.data();
+        sh_preprocess_cols_trunc::processed_buffer = processed;
+        dispatch2d(H, W, [](uvec3 g) { sh_preprocess_cols_trunc::main_(g); });
+    } else {
+        set_params(sh_preprocess_cols_notrunc::params, p);
+        sh_preprocess_cols_notrunc::temp = temp.data();
+        sh_preprocess_cols_notrunc::processed_buffer = processed;
+        dispatch2d(H, W, [](uvec3 g) { sh_preprocess_cols_notrunc::main_(g); });
+    }
+    return 0;
+}
+
+int64_t ref_candidates(const RefParams* p, const float* processed, float pic_std, int32_t* uv, int64_t cap) {
+    const int32_t H = p->pic_nrows, W = p->pic_ncols;
+    std::vector<float> mr((size_t)H * W);
+    set_params(sh_max_rows::params, p);
+    sh_max_rows::processed_buffer = const_cast<float*>(processed);
+    sh_max_rows::max_rows = mr.data();
+    dispatch2d(H, W, [](uvec3 g) { sh_max_rows::main_(g); });
+    // every pixel may be a candidate; the reference's own buffer holds H*W/4
+    // entries and drops the rest, which the callers treat as an error case
+    std::vector<sh_extract_max::ParticleLocation> pts((size_t)H * W + 1);
+    set_params(sh_extract_max::params, p);
+    sh_extract_max::processed_buffer = const_cast<float*>(processed);
+    sh_extract_max::max_rows = mr.data();
+    sh_extract_max::n_particles = 0;
+    sh_extract_max::max_points = pts.data();
+    sh_extract_max::pic_std = pic_std;
+    sh_extract_max::wg_size = {};
+    dispatch2d(H, W, [](uvec3 g) { sh_extract_max::main_(g); });
+    int64_t n = sh_extract_max::n_particles;
+    for (int64_t i = 0; i < n && i < cap; i++) {
+        uv[2 * i] = pts[i].x;
+        uv[2 * i + 1] = pts[i].y;
+    }
+    return n;
+}
+
+// walk over candidates (with radius r, -1 for trackpy), then characterize the
+// kept rows when characterize != 0.  rows_out: 10 floats per kept row.
+int64_t ref_walk(const RefParams* p, const float* processed, const float* raw, const int32_t* uv, int64_t n,
+                 float r, float pic_std, int32_t characterize, float* rows_out) {
+    std::vector<sh_walk::ParticleLocation> parts((size_t)n + 1);
+    for (int64_t i = 0; i < n; i++) parts[i] = {uv[2 * i], uv[2 * i + 1], r, -1.0f};
+    std::vector<sh_walk::ResultRow> res((size_t)n + 1);
+    set_params(sh_walk::params, p);
+    sh_walk::processed_buffer = const_cast<float*>(processed);
+    sh_walk::particles = parts.data();
+    sh_walk::n_particles = (uint32_t)n;
+    sh_walk::n_particles_filtered = 0;
+    sh_walk::results = res.data();
+    sh_walk::raw_frame = const_cast<float*>(raw);
+    sh_walk::image_std = pic_std;
+    sh_walk::next_dispatch = {};
+    for (int64_t i = 0; i < n; i++) sh_walk::main_(uvec3{(uint32_t)i, 0u, 0u});
+    int64_t nk = sh_walk::n_particles_filtered;
+    if (characterize) {
+        static_assert(sizeof(sh_walk::ResultRow) == sizeof(sh_characterize::ResultRow), "row");
+        std::vector<sh_characterize::ResultRow> cr((size_t)nk + 1);
+        std::memcpy(cr.data(), res.data(), (size_t)nk * sizeof(sh_walk::ResultRow));
+        set_params(sh_characterize::params, p);
+        sh_characterize::processed_buffer = const_cast<float*>(processed);
+        sh_characterize::raw_frame = const_cast<float*>(raw);
+        sh_characterize::n_particles = (uint32_t)nk;
+        sh_characterize::results = cr.data();
+        for (int64_t i = 0; i < nk; i++) sh_characterize::main_(uvec3{(uint32_t)i, 0u, 0u});
+        std::memcpy(res.data(), cr.data(), (size_t)nk * sizeof(sh_walk::ResultRow));
+    }
+    std::memcpy(rows_out, res.data(), (size_t)nk * 10 * sizeof(float));
+    return nk;
+}
+
+// characterize_points: rows_inout holds 10-float ResultRows with x, y, r set.
+int ref_characterize_points(const RefParams* p, const float* processed, const float* raw, float* rows_inout,
+                            int64_t n) {
+    std::vector<sh_characterize_points::ResultRow> cr((size_t)n + 1);
+    std::memcpy(cr.data(), rows_inout, (size_t)n * 10 * sizeof(float));
+    set_params(sh_characterize_points::params, p);
+    sh_characterize_points::processed_buffer = const_cast<float*>(processed);
+    sh_characterize_points::raw_frame = const_cast<float*>(raw);
+    sh_characterize_points::n_particles = (uint32_t)n;
+    sh_characterize_points::results = cr.data();
+    for (int64_t i = 0; i < n; i++) sh_characterize_points::main_(uvec3{(uint32_t)i, 0u, 0u});
+    std::memcpy(rows_inout, cr.data(), (size_t)n * 10 * sizeof(float));
+    return 0;
+}
+
+// Laplace<2>::execute with SeparableConvolution<2> buffers: input = frame,
+// temp2 = first output, final = log-space plane (src/utils.rs:114-296).
+int ref_laplace(const RefParams* p, const float* frame, float sigma, float* final_out) {
+    const int32_t H = p->pic_nrows, W = p->pic_ncols;
+    std::vector<float> temp2((size_t)H * W), temp1((size_t)H * W);
+    set_params(sh_separable_log::params, p);
+    sh_separable_log::final_output = final_out;
+    for (uint32_t diff_dim = 0; diff_dim < 2; diff_dim++) {
+        sh_separable_log::pc = {0u, diff_dim, sigma};
+        sh_separable_log::input = const_cast<float*>(frame);
+        sh_separable_log::output = temp2.data();
+        dispatch2d(H, W, [](uvec3 g) { sh_separable_log::main_(g); });
+        sh_separable_log::pc = {1u, diff_dim, sigma};
+        sh_separable_log::input = temp2.data();
+        sh_separable_log::output = temp1.data();
+        dispatch2d(H, W, [](uvec3 g) { sh_separable_log::main_(g); });
+    }
+    return 0;
+}
+
+int64_t ref_logspace_max(const RefParams* p, const float* bottom, const float* middle, const float* top,
+                         const float* processed, float pic_std, int32_t edge, float radius, int32_t* uv,
+                         int64_t cap) {
+    const int32_t H = p->pic_nrows, W = p->pic_ncols;
+    std::vector<sh_logspace_max::ParticleLocation> pts((size_t)H * W + 1);
+    set_params(sh_logspace_max::params, p);
+    sh_logspace_max::bottom = const_cast<float*>(bottom);
+    sh_logspace_max::middle = const_cast<float*>(middle);
+    sh_logspace_max::top = const_cast<float*>(top);
+    sh_logspace_max::n_particles = 0;
+    sh_logspace_max::particles = pts.data();
+    sh_logspace_max::wg_size = {};
+    sh_logspace_max::std_pic = pic_std;
+    sh_logspace_max::processed = const_cast<float*>(processed);
+    sh_logspace_max::pc = {edge, radius};
+    dispatch2d(H, W, [](uvec3 g) { sh_logspace_max::main_(g); });
+    int64_t n = sh_logspace_max::n_particles;
+    for (int64_t i = 0; i < n && i < cap; i++) {
+        uv[2 * i] = pts[i].x;
+        uv[2 * i + 1] = pts[i].y;
+    }
+    return n;
+}
+
+}  // extern "C"
