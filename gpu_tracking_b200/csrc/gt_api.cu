@@ -1,0 +1,1437 @@
+// gt_api.cu — the C ABI (include/gpu_tracking_b200.h) and its host runtime.
+//
+// The runtime replaces execute_gpu / submit_work / get_work / post_process
+// (src/execute_gpu.rs:95-467, 671-1184) and setup_state (src/gpu_setup.rs:611-1292):
+//   * frames are processed in chunks on one compute stream; host frames are
+//     staged through two device buffers filled on a copy stream, so the H2D
+//     copy of chunk c+1 overlaps the kernels of chunk c;
+//   * every per-frame result stays in HBM until the whole video is done
+//     (filter, doughnut and linking included), then one table is assembled
+//     on the device and copied out column by column on request;
+//   * capacities (candidates / detections per frame) grow and the call is
+//     replayed when a kernel reports an overflow, so nothing is truncated.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gt_kernels.h"
+
+using namespace gt;
+
+namespace {
+
+struct DBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) n = want;
+        return e;
+    }
+    template <class T>
+    T* as() const {
+        return (T*)p;
+    }
+};
+
+struct KernelStat {
+    int64_t launches = 0;
+    double ms = 0.0;
+};
+
+}  // namespace
+
+struct gt_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;   // compute
+    cudaStream_t cp = nullptr;   // host -> device copies
+    cudaEvent_t used[2] = {nullptr, nullptr};    // compute finished with staging buffer b
+    cudaEvent_t filled[2] = {nullptr, nullptr};  // staging buffer b holds its chunk
+    std::string err;
+    const volatile int32_t* interrupt = nullptr;
+    std::atomic<int64_t> done{0}, total{0};
+    // profiling of the main kernels (CUDA events on the compute stream)
+    bool profile = false;
+    std::map<std::string, KernelStat> stats;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> event_pool;
+    // device buffers, grown on demand and kept for the next call
+    DBuf stage[2], processed, planes, cand_count, cand_keys, feats_raw, feat_count, feats_out, kept_count,
+        fin_scratch, flags, ident, tabs_f, tabs_i, tabs_s, tabs_m, row_off, frame_num;
+    DBuf l_srt, l_sortscr, l_fcnt, l_bcnt, l_foff, l_boff, l_fpts, l_bpts, l_bdist, l_scan, l_scratch, l_ids, l_cnt,
+        l_dur, l_flags, l_goff, l_pgroup, l_vgrp, l_reset, l_vpoff, l_px, l_py, l_ge, l_rowdur, l_part;
+    uint32_t cand_cap = 16384;
+    uint32_t feat_cap = 4096;
+};
+
+struct gt_table {
+    int device = 0;
+    int64_t n = 0;
+    DBuf frame, particle, duration;
+    DBuf col[GT_NUM_COLUMNS];
+    bool has[GT_NUM_COLUMNS] = {};
+};
+
+namespace {
+
+gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return st;
+}
+
+#define CK(expr)                                                                                             \
+    do {                                                                                                     \
+        cudaError_t e_ = (expr);                                                                             \
+        if (e_ != cudaSuccess)                                                                               \
+            return set_err(ctx, GT_ERR_CUDA, "CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_), __FILE__, \
+                           __LINE__, #expr);                                                                 \
+    } while (0)
+
+#define CKS(expr)                        \
+    do {                                 \
+        gt_status s_ = (expr);           \
+        if (s_ != GT_OK) return s_;      \
+    } while (0)
+
+// --------------------------------------------------------------- profiling
+struct Prof {
+    gt_ctx* ctx;
+    const char* name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Prof(gt_ctx* c, const char* n) : ctx(c), name(n) {
+        if (!ctx->profile) return;
+        a = take();
+        b = take();
+        cudaEventRecord(a, ctx->st);
+    }
+    cudaEvent_t take() {
+        if (!ctx->event_pool.empty()) {
+            cudaEvent_t e = ctx->event_pool.back();
+            ctx->event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    ~Prof() {
+        if (!ctx->profile) return;
+        cudaEventRecord(b, ctx->st);
+        ctx->pending.push_back({name, {a, b}});
+    }
+};
+
+void drain_profile(gt_ctx* ctx) {
+    for (auto& p : ctx->pending) {
+        float ms = 0.0f;
+        cudaEventSynchronize(p.second.second);
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        auto& s = ctx->stats[p.first];
+        s.launches++;
+        s.ms += ms;
+        ctx->event_pool.push_back(p.second.first);
+        ctx->event_pool.push_back(p.second.second);
+    }
+    ctx->pending.clear();
+}
+
+// ------------------------------------------------------- derived parameters
+struct Derived {
+    int32_t smoothing, circle, dilation, margin;
+};
+
+// gpuparams_from_tracking_params (src/gpu_setup.rs:528-580)
+Derived derive(const gt_params& p) {
+    Derived d;
+    if (p.style == GT_STYLE_TRACKPY) {
+        uint32_t smoothing = p.has_smoothing_size ? p.smoothing_size : p.diameter;
+        float dil = 2.0f * (float)p.separation / std::sqrt(2.0f);
+        uint32_t a = p.diameter / 2, b = p.separation / 2 - 1u, c = smoothing / 2;
+        uint32_t m = std::max(a, std::max(b, c));
+        d.smoothing = (int32_t)smoothing;
+        d.circle = (int32_t)p.diameter;
+        d.dilation = (int32_t)(uint32_t)dil;
+        d.margin = (int32_t)m;
+    } else {
+        uint32_t smoothing = p.has_smoothing_size ? p.smoothing_size : ((uint32_t)(p.max_radius + 0.5f)) * 2 + 1;
+        d.smoothing = (int32_t)smoothing;
+        d.circle = 0;
+        d.dilation = 0;
+        d.margin = 0;
+    }
+    return d;
+}
+
+gt_status make_locate_consts(gt_ctx* ctx, const gt_params& p, int32_t H, int32_t W, LocateConsts& c) {
+    Derived d = derive(p);
+    std::memset(&c, 0, sizeof(c));
+    c.H = H;
+    c.W = W;
+    c.R = d.smoothing / 2;
+    if (2 * c.R + 1 > kMaxTaps)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size %d exceeds the supported %d", d.smoothing,
+                       kMaxTaps);
+    // preprocess_rows.wgsl:46-47: exp(-x*x / (2.0 * sigma2)) with sigma2 = noise_size
+    float gnorm = 0.0f;
+    for (int i = -c.R; i <= c.R; i++) {
+        float x = (float)i;
+        float g = std::exp(-x * x / (2.0f * p.noise_size));
+        c.taps[i + c.R] = g;
+        gnorm += g;
+    }
+    c.gnorm = gnorm;
+    c.kk = (float)(d.smoothing * d.smoothing);
+    c.truncate = p.truncate_preprocessed ? 1 : 0;
+    c.kd = d.dilation;
+    c.o = (int32_t)((float)d.dilation / 2.0f - 0.5f);
+    c.margin = d.margin;
+    c.thr = 0.0f;  // pic_std (0 unless snr/minmass_snr) * snr * rough
+    c.circle = d.circle;
+    c.max_iter = p.max_iterations;
+    c.shift_thr = p.shift_threshold;
+    c.minmass = p.minmass;
+    c.minmass_snr = p.has_minmass_snr ? p.minmass_snr : 0.0f;
+    c.image_std = 0.0f;
+    c.rough = p.has_adaptive_background ? 0.5f : 1.0f;
+    c.characterize = p.characterize ? 1 : 0;
+    return GT_OK;
+}
+
+// (sin 2θ, cos 2θ) tables per integer radius 0..max_rint (characterize.wgsl:120-124)
+void angle_tables(int max_rint, std::vector<float2>& tab, std::vector<int32_t>& off) {
+    tab.clear();
+    off.clear();
+    for (int r = 0; r <= max_rint; r++) {
+        off.push_back((int32_t)tab.size());
+        for (int i = -r; i <= r; i++)
+            for (int j = -r; j <= r; j++) {
+                float x = (float)i, y = (float)j;
+                float2 v = make_float2(0.0f, 0.0f);
+                if (i != 0 || j != 0) {
+                    float theta = std::atan2(y, x);
+                    v = make_float2(std::sin(2.0f * theta), std::cos(2.0f * theta));
+                }
+                tab.push_back(v);
+            }
+    }
+}
+
+// circle_inds / annulus_inds (src/kernels.rs:138-171)
+void circle_inds(float radius, std::vector<short2>& v) {
+    int rb = (int)std::ceil(radius);
+    float r2 = radius * radius;
+    for (int i = -rb; i < rb + 1; i++)
+        for (int j = -rb; j < rb + 1; j++)
+            if ((float)(i * i + j * j) <= r2) v.push_back(make_short2((short)i, (short)j));
+}
+void annulus_inds(float outer, float inner, std::vector<short2>& v) {
+    int b = (int)std::ceil(outer);
+    float or2 = outer * outer, ir2 = inner * inner;
+    for (int i = -b; i < b + 1; i++)
+        for (int j = -b; j < b + 1; j++) {
+            float r2 = (float)(i * i + j * j);
+            if (r2 <= or2 && r2 >= ir2) v.push_back(make_short2((short)i, (short)j));
+        }
+}
+
+// Doughnut tables for the given particle radii (one entry per radius index).
+void doughnut_tables(const gt_params& p, const std::vector<float>& radii, std::vector<short2>& inds,
+                     std::vector<int4>& meta) {
+    inds.clear();
+    meta.clear();
+    for (float radius : radii) {
+        int4 m;
+        m.x = (int)inds.size();
+        circle_inds(radius, inds);
+        m.y = (int)inds.size() - m.x;
+        float outer = p.has_bg_radius ? p.bg_radius : 2.0f * radius;
+        float gap = (p.has_bg_radius && p.has_gap_radius) ? p.gap_radius : 0.0f;
+        m.z = (int)inds.size();
+        annulus_inds(outer, gap + radius, inds);
+        m.w = (int)inds.size() - m.z;
+        meta.push_back(m);
+    }
+}
+
+// LoG radii (src/gpu_setup.rs:958-984)
+std::vector<float> log_radii(const gt_params& p) {
+    std::vector<float> out;
+    size_t n = p.n_radii;
+    if (n == 0) return out;
+    if (p.log_spacing) {
+        float start = std::log(p.min_radius) / std::log(10.0f);
+        float end = std::log(p.max_radius) / std::log(10.0f);
+        float diff = (end - start) / (float)(n - 1);
+        for (size_t i = 0; i + 1 < n; i++) {
+            float temp = start;
+            start += diff;
+            out.push_back(std::pow(10.0f, temp));
+        }
+        out.push_back(std::pow(10.0f, start));
+    } else {
+        float start = p.min_radius;
+        float end = p.max_radius;
+        float diff = (end - start) / (float)(n - 1);
+        for (size_t i = 0; i + 1 < n; i++) {
+            float temp = start;
+            start += diff;
+            out.push_back(temp);
+        }
+        out.push_back(start);
+    }
+    return out;
+}
+
+struct LogTables {
+    std::vector<float> radii, taps_g, taps_d, norm_g, norm_d;
+    std::vector<int32_t> tap_off, rints;
+    int max_rint = 0;
+};
+
+// separable_log.wgsl:27-76 tap values, computed per radius with sigma = r / sqrt(2)
+LogTables log_tables(const gt_params& p) {
+    LogTables t;
+    t.radii = log_radii(p);
+    const float sqrt2pi = (float)2.5066282746310002;
+    for (float r : t.radii) {
+        float sigma = r / std::sqrt(2.0f);
+        float sigma2 = sigma * sigma;
+        int rint = (int)(4.0f * sigma + 0.5f);
+        t.tap_off.push_back((int32_t)t.taps_g.size());
+        t.rints.push_back(rint);
+        t.max_rint = std::max(t.max_rint, rint);
+        for (int i = -rint; i <= rint; i++) {
+            float x = (float)i;
+            float x2 = x * x;
+            float g = std::exp(-x2 / (2.0f * sigma2));
+            t.taps_g.push_back(g);
+            t.taps_d.push_back(g * (x2 - sigma2));
+        }
+        t.norm_d.push_back(1.0f / (sqrt2pi * sigma * sigma2));
+        t.norm_g.push_back(1.0f / (sqrt2pi * sigma));
+    }
+    return t;
+}
+
+gt_status check_frames_ptr(gt_ctx* ctx, const void* frames, bool* on_device) {
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, frames);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *on_device = false;
+        return GT_OK;
+    }
+    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+        if (at.device != ctx->device)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "frames live on device %d, context is on device %d",
+                           at.device, ctx->device);
+        *on_device = true;
+    } else {
+        *on_device = false;
+    }
+    return GT_OK;
+}
+
+bool interrupted(gt_ctx* ctx) { return ctx->interrupt && *ctx->interrupt != 0; }
+
+template <class T>
+gt_status upload(gt_ctx* ctx, DBuf& b, const std::vector<T>& v) {
+    CK(b.ensure(std::max<size_t>(1, v.size()) * sizeof(T)));
+    if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
+    return GT_OK;
+}
+
+// ---------------------------------------------------------------- linking
+struct LinkJob {
+    // host description of the groups (frames) and videos to link
+    std::vector<int64_t> goff;   // ngroups + 1, row offsets into px/py
+    std::vector<int32_t> vgrp;   // nvideos + 1
+    std::vector<uint8_t> reset;  // per group
+    float radius = 0;
+    int32_t memory = 0;
+};
+
+// Runs the linker over px/py (device, npoints) and writes ids (device) and,
+// when row_dur is given, per-row durations and f32-rounded particle ids.
+gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float* py, int64_t* ids_out,
+                   int64_t* row_dur, int64_t* row_particle, std::vector<int64_t>* counters) {
+    const int ngroups = (int)job.goff.size() - 1;
+    const int nvideos = (int)job.vgrp.size() - 1;
+    const int64_t N = job.goff.back();
+    const int K = job.memory + 1;
+    int max_group = 0;
+    for (int g = 0; g < ngroups; g++) max_group = std::max<int64_t>(max_group, job.goff[g + 1] - job.goff[g]);
+    std::vector<int32_t> pgroup(N);
+    for (int g = 0; g < ngroups; g++)
+        for (int64_t i = job.goff[g]; i < job.goff[g + 1]; i++) pgroup[i] = g;
+    CKS(upload(ctx, ctx->l_goff, job.goff));
+    CKS(upload(ctx, ctx->l_pgroup, pgroup));
+    CKS(upload(ctx, ctx->l_vgrp, job.vgrp));
+    CKS(upload(ctx, ctx->l_reset, job.reset));
+    LinkInput in;
+    in.px = px;
+    in.py = py;
+    in.goff = ctx->l_goff.as<int64_t>();
+    in.pgroup = ctx->l_pgroup.as<int32_t>();
+    in.vgrp = ctx->l_vgrp.as<int32_t>();
+    in.reset = ctx->l_reset.as<uint8_t>();
+    in.ngroups = ngroups;
+    in.nvideos = nvideos;
+    in.npoints = N;
+    in.radius = job.radius;
+    in.memory = job.memory;
+
+    int np2 = 1;
+    while (np2 < max_group) np2 <<= 1;
+    size_t per_group = (np2 > 4096) ? (size_t)np2 * 8 : 0;
+    CK(ctx->l_srt.ensure(std::max<int64_t>(N, 1) * 4));
+    CK(ctx->l_sortscr.ensure(std::max<size_t>(per_group * ngroups, 8)));
+    {
+        Prof pf(ctx, "link_sort");
+        CK(link_sort_groups(in, ctx->l_srt.as<uint32_t>(), ctx->l_sortscr.as<uint8_t>(), per_group, max_group,
+                            ctx->st));
+    }
+    const size_t NK = (size_t)N * K;
+    CK(ctx->l_fcnt.ensure((NK + 1) * 8));
+    CK(ctx->l_bcnt.ensure((NK + 1) * 8));
+    CK(ctx->l_foff.ensure((NK + 1) * 8));
+    CK(ctx->l_boff.ensure((NK + 1) * 8));
+    CK(cudaMemsetAsync(ctx->l_fcnt.p, 0, (NK + 1) * 8, ctx->st));
+    CK(cudaMemsetAsync(ctx->l_bcnt.p, 0, (NK + 1) * 8, ctx->st));
+    {
+        Prof pf(ctx, "link_lists");
+        CK(link_count_lists(in, ctx->l_srt.as<uint32_t>(), ctx->l_fcnt.as<int64_t>(), ctx->l_bcnt.as<int64_t>(),
+                            ctx->st));
+    }
+    size_t tmp_bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, ctx->l_fcnt.as<int64_t>(), ctx->l_foff.as<int64_t>(),
+                                     (int64_t)NK + 1, ctx->st));
+    CK(ctx->l_scan.ensure(tmp_bytes));
+    CK(cub::DeviceScan::ExclusiveSum(ctx->l_scan.p, tmp_bytes, ctx->l_fcnt.as<int64_t>(), ctx->l_foff.as<int64_t>(),
+                                     (int64_t)NK + 1, ctx->st));
+    CK(cub::DeviceScan::ExclusiveSum(ctx->l_scan.p, tmp_bytes, ctx->l_bcnt.as<int64_t>(), ctx->l_boff.as<int64_t>(),
+                                     (int64_t)NK + 1, ctx->st));
+    int64_t ftot = 0, btot = 0;
+    CK(cudaMemcpyAsync(&ftot, ctx->l_foff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&btot, ctx->l_boff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
+    // per-group backward-edge totals bound the per-frame edge list
+    std::vector<int64_t> gb(ngroups + 1);
+    std::vector<int64_t> boff_at(ngroups + 1);
+    for (int g = 0; g <= ngroups; g++)
+        CK(cudaMemcpyAsync(&boff_at[g], ctx->l_boff.as<int64_t>() + job.goff[g] * K, 8, cudaMemcpyDeviceToHost,
+                           ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    int64_t max_edges = 1;
+    for (int g = 0; g < ngroups; g++) max_edges = std::max(max_edges, boff_at[g + 1] - boff_at[g]);
+    CK(ctx->l_fpts.ensure(std::max<int64_t>(ftot, 1) * 4));
+    CK(ctx->l_bpts.ensure(std::max<int64_t>(btot, 1) * 4));
+    CK(ctx->l_bdist.ensure(std::max<int64_t>(btot, 1) * 4));
+    LinkLists L;
+    L.f_off = ctx->l_foff.as<int64_t>();
+    L.b_off = ctx->l_boff.as<int64_t>();
+    L.f_pts = ctx->l_fpts.as<int32_t>();
+    L.b_pts = ctx->l_bpts.as<int32_t>();
+    L.b_dist = ctx->l_bdist.as<float>();
+    L.srt = ctx->l_srt.as<uint32_t>();
+    {
+        Prof pf(ctx, "link_lists");
+        CK(link_fill_lists(in, L, ctx->st));
+    }
+    // scratch per video
+    int64_t max_np = 1;
+    for (int v = 0; v < nvideos; v++) max_np = std::max(max_np, job.goff[job.vgrp[v + 1]] - job.goff[job.vgrp[v]]);
+    LinkScratch S;
+    S.max_group = std::max(max_group, 1);
+    S.max_edges = max_edges;
+    S.bytes_per_video = link_scratch_bytes(S.max_group, S.max_edges, max_np, job.memory);
+    CK(ctx->l_scratch.ensure(S.bytes_per_video * nvideos));
+    S.base = ctx->l_scratch.as<uint8_t>();
+    LinkOutput out;
+    CK(ctx->l_cnt.ensure(nvideos * 8));
+    CK(ctx->l_dur.ensure(std::max<int64_t>(N, 1) * 8));
+    CK(ctx->l_flags.ensure(nvideos * 4));
+    CK(cudaMemsetAsync(ctx->l_flags.p, 0, nvideos * 4, ctx->st));
+    out.ids = ids_out;
+    out.counter = ctx->l_cnt.as<int64_t>();
+    out.dur = ctx->l_dur.as<int64_t>();
+    out.vpoff = nullptr;
+    out.flags = ctx->l_flags.as<uint32_t>();
+    {
+        Prof pf(ctx, "link_video");
+        CK(link_run(in, L, S, out, ctx->st));
+    }
+    std::vector<uint32_t> flags(nvideos);
+    CK(cudaMemcpyAsync(flags.data(), out.flags, nvideos * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    uint32_t all = 0;
+    for (auto f : flags) all |= f;
+    if (all & kFlagTooDense)
+        return set_err(ctx, GT_ERR_TOO_DENSE_TO_LINK,
+                       "computational load during linking is abnormally high. try setting a smaller search range "
+                       "or track with settings that give fewer detections.");
+    if (all & kFlagSubnetBudget)
+        return set_err(ctx, GT_ERR_SUBNET_TOO_EXPENSIVE, "a linking subnet exceeded the device search budget");
+    if (all & kFlagScratch) return set_err(ctx, GT_ERR_INTERNAL, "linker scratch overflow");
+    if (counters) {
+        counters->resize(nvideos);
+        CK(cudaMemcpy(counters->data(), out.counter, nvideos * 8, cudaMemcpyDeviceToHost));
+    }
+    if (row_dur) {
+        CK(link_durations(in, out, row_dur, ctx->st));
+        CK(cudaMemcpyAsync(flags.data(), out.flags, nvideos * 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (auto f : flags)
+            if (f & kFlagScratch)
+                return set_err(ctx, GT_ERR_INTERNAL,
+                               "a particle id has no duration entry after a linker reset (the reference panics here)");
+    }
+    (void)row_particle;
+    return GT_OK;
+}
+
+__global__ void f32_round_ids_kernel(const int64_t* ids, int64_t* out, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (int64_t)(float)ids[i];
+}
+
+// --------------------------------------------------------------- locate
+struct Chunking {
+    int F;
+};
+
+int pick_chunk(int64_t T, int32_t H, int32_t W, int n_planes) {
+    const size_t px = (size_t)H * W;
+    size_t per_frame = px * 4 * (1 + n_planes);
+    int F = (int)std::max<size_t>(1, (size_t)(256u << 20) / per_frame);
+    F = std::min<int>(F, 64);
+    F = (int)std::min<int64_t>(F, T);
+    return std::max(F, 1);
+}
+
+template <typename T>
+gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
+                      int32_t W, const LocateConsts& c, const LogTables* lt, int F, uint32_t* out_flags) {
+    const size_t npx = (size_t)H * W;
+    const bool log_style = (p.style == GT_STYLE_LOG);
+    const int nslots = log_style ? (int)lt->radii.size() : 1;
+    const uint32_t cand_cap = ctx->cand_cap, feat_cap = ctx->feat_cap;
+    const int nchunks = (int)((NT + F - 1) / F);
+    CK(ctx->processed.ensure((size_t)F * npx * 4));
+    if (log_style) CK(ctx->planes.ensure((size_t)F * nslots * npx * 4));
+    CK(ctx->cand_count.ensure((size_t)F * nslots * 4));
+    CK(ctx->cand_keys.ensure((size_t)F * nslots * cand_cap * 4));
+    CK(ctx->feats_raw.ensure((size_t)F * feat_cap * sizeof(Feature)));
+    CK(ctx->feat_count.ensure((size_t)F * 4));
+    CK(ctx->feats_out.ensure((size_t)NT * feat_cap * sizeof(Feature)));
+    CK(ctx->kept_count.ensure((size_t)NT * 4));
+    CK(ctx->flags.ensure(16));
+    CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
+    // finalize scratch for frames with more detections than shared memory sorts
+    size_t fin_per_frame = 0;
+    if (feat_cap > (uint32_t)kFinalizeSmemSort) {
+        size_t np2 = 1;
+        while (np2 < feat_cap) np2 <<= 1;
+        fin_per_frame = (np2 * 17 + 255) & ~(size_t)255;
+    }
+    CK(ctx->fin_scratch.ensure(std::max<size_t>(fin_per_frame * F, 256)));
+    {
+        std::vector<int32_t> ident(F);
+        for (int i = 0; i < F; i++) ident[i] = i;
+        CKS(upload(ctx, ctx->ident, ident));
+    }
+    // constant tables
+    std::vector<float2> atab;
+    std::vector<int32_t> aoff;
+    int max_rint = log_style ? 0 : std::max(0, (c.circle - 1) / 2);
+    if (log_style)
+        for (float r : lt->radii) max_rint = std::max(max_rint, (int)std::ceil(r));
+    angle_tables(max_rint, atab, aoff);
+    std::vector<short2> dn;
+    std::vector<int4> dmeta;
+    std::vector<float> dradii;
+    if (log_style) dradii = lt->radii;
+    else dradii.push_back((float)p.diameter / 2.0f);
+    doughnut_tables(p, dradii, dn, dmeta);
+    CKS(upload(ctx, ctx->tabs_f, atab));
+    CKS(upload(ctx, ctx->tabs_i, aoff));
+    CKS(upload(ctx, ctx->tabs_s, dn));
+    CKS(upload(ctx, ctx->tabs_m, dmeta));
+    // LoG tables
+    DBuf ltg, ltd, loff, lrint, lng, lnd, lrad;
+    if (log_style) {
+        CKS(upload(ctx, ltg, lt->taps_g));
+        CKS(upload(ctx, ltd, lt->taps_d));
+        CKS(upload(ctx, loff, lt->tap_off));
+        CKS(upload(ctx, lrint, lt->rints));
+        CKS(upload(ctx, lng, lt->norm_g));
+        CKS(upload(ctx, lnd, lt->norm_d));
+        CKS(upload(ctx, lrad, lt->radii));
+    }
+    FinalizeConsts fc;
+    std::memset(&fc, 0, sizeof(fc));
+    fc.H = H;
+    fc.W = W;
+    fc.log_style = log_style ? 1 : 0;
+    fc.prune = (log_style && p.overlap_threshold < 1.0f) ? 1 : 0;
+    fc.overlap_threshold = p.overlap_threshold;
+    fc.filter_close = (!log_style && p.filter_close) ? 1 : 0;
+    fc.separation = (float)p.separation;
+    {
+        // every filter_close neighbour's candidate row lies within this band
+        // when the processed image is non-negative (centroid offsets <= rint)
+        int rint = std::max(0, (c.circle - 1) / 2);
+        long long band = (long long)std::ceil(fc.separation) + 2LL * ((long long)c.max_iter + rint) + 2;
+        fc.band = (c.truncate && band < (1LL << 30)) ? (int32_t)band : -1;
+    }
+    fc.doughnut = p.doughnut_correction ? 1 : 0;
+    fc.presorted = 0;
+    fc.scratch_per_frame = fin_per_frame;
+    if (log_style) {
+        for (size_t k = 0; k < lt->radii.size(); k++) {
+            int rank = 0;
+            for (size_t q = 0; q < lt->radii.size(); q++)
+                if (lt->radii[q] > lt->radii[k]) rank++;
+            fc.radius_rank_desc[k] = (uint8_t)rank;
+        }
+    }
+    LogConsts lc;
+    lc.H = H;
+    lc.W = W;
+    lc.n_radii = nslots;
+    lc.thr = 0.0f;
+
+    const size_t chunk_bytes = (size_t)F * npx * sizeof(T);
+    if (!on_device) {
+        CK(ctx->stage[0].ensure(chunk_bytes));
+        CK(ctx->stage[1].ensure(chunk_bytes));
+    }
+    auto issue_copy = [&](int chunk) -> gt_status {
+        int b = chunk & 1;
+        int64_t f0 = (int64_t)chunk * F;
+        int nf = (int)std::min<int64_t>(F, NT - f0);
+        CK(cudaStreamWaitEvent(ctx->cp, ctx->used[b], 0));
+        CK(cudaMemcpyAsync(ctx->stage[b].p, frames + f0 * npx, (size_t)nf * npx * sizeof(T), cudaMemcpyHostToDevice,
+                           ctx->cp));
+        CK(cudaEventRecord(ctx->filled[b], ctx->cp));
+        return GT_OK;
+    };
+    if (!on_device) {
+        // both staging buffers start free
+        CK(cudaEventRecord(ctx->used[0], ctx->st));
+        CK(cudaEventRecord(ctx->used[1], ctx->st));
+        CKS(issue_copy(0));
+    }
+    uint32_t* flags = ctx->flags.as<uint32_t>();
+    for (int ch = 0; ch < nchunks; ch++) {
+        if (interrupted(ctx)) {
+            cudaStreamSynchronize(ctx->st);
+            cudaStreamSynchronize(ctx->cp);
+            return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
+        }
+        const int64_t f0 = (int64_t)ch * F;
+        const int nf = (int)std::min<int64_t>(F, NT - f0);
+        const T* src;
+        if (on_device) {
+            src = frames + f0 * npx;
+        } else {
+            if (ch + 1 < nchunks) CKS(issue_copy(ch + 1));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->filled[ch & 1], 0));
+            src = ctx->stage[ch & 1].as<T>();
+        }
+        CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
+        CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)nf * 4, ctx->st));
+        float* proc = ctx->processed.as<float>();
+        if (!log_style) {
+            Prof pf(ctx, "bandpass_localmax");
+            CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
+                                  ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+        } else {
+            {
+                Prof pf(ctx, "bandpass");
+                CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags, ctx->st));
+            }
+            {
+                Prof pf(ctx, "laplace");
+                CK(launch_laplace<T>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
+                                     ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
+                                     lnd.as<float>(), lt->max_rint, nf, ctx->st));
+            }
+            {
+                Prof pf(ctx, "logspace_max");
+                CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
+                                       ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+            }
+        }
+        {
+            Prof pf(ctx, "walk_characterize");
+            CK(launch_walk<T>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
+                              ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap,
+                              log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
+                              ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
+                              feat_cap, flags, ctx->st));
+        }
+        {
+            Prof pf(ctx, "finalize");
+            CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
+                                  ctx->feats_out.as<Feature>() + (size_t)f0 * feat_cap,
+                                  ctx->kept_count.as<uint32_t>() + f0, ctx->fin_scratch.as<uint8_t>(), fc, src,
+                                  (int64_t)npx, ctx->ident.as<int32_t>(), ctx->tabs_s.as<short2>(),
+                                  ctx->tabs_m.as<int4>(), flags, nf, ctx->st));
+        }
+        if (!on_device) CK(cudaEventRecord(ctx->used[ch & 1], ctx->st));
+        ctx->done = f0 + nf;
+    }
+    CK(cudaMemcpyAsync(out_flags, flags, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    drain_profile(ctx);
+    return GT_OK;
+}
+
+// Assemble the output table from per-frame results (kept_count, feats_out).
+gt_status assemble_table(gt_ctx* ctx, int64_t NT, const std::vector<int64_t>& frame_numbers, bool log_style,
+                         gt_table* tab, std::vector<int64_t>& row_off) {
+    std::vector<uint32_t> kept(NT);
+    CK(cudaMemcpyAsync(kept.data(), ctx->kept_count.p, NT * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    row_off.assign(NT + 1, 0);
+    uint32_t maxk = 0;
+    for (int64_t t = 0; t < NT; t++) {
+        row_off[t + 1] = row_off[t] + kept[t];
+        maxk = std::max(maxk, kept[t]);
+    }
+    const int64_t N = row_off[NT];
+    tab->n = N;
+    const size_t n1 = std::max<int64_t>(N, 1);
+    CK(tab->frame.ensure(n1 * 8));
+    for (int c = 0; c < GT_NUM_COLUMNS; c++) {
+        if (c == GT_COL_FRAME || c == GT_COL_PARTICLE || c == GT_COL_DURATION) continue;
+        CK(tab->col[c].ensure(n1 * 4));
+        tab->has[c] = true;
+    }
+    tab->has[GT_COL_FRAME] = true;
+    (void)log_style;
+    CKS(upload(ctx, ctx->row_off, row_off));
+    CKS(upload(ctx, ctx->frame_num, frame_numbers));
+    TableCols tc;
+    tc.frame = tab->frame.as<int64_t>();
+    for (int c = 0; c < GT_NUM_COLUMNS; c++) tc.col[c] = tab->col[c].as<float>();
+    tc.particle = nullptr;
+    tc.duration = nullptr;
+    for (int64_t g0 = 0; g0 < NT; g0 += 65535) {
+        int ng = (int)std::min<int64_t>(65535, NT - g0);
+        CK(launch_scatter(ctx->feats_out.as<Feature>() + (size_t)g0 * ctx->feat_cap, ctx->feat_cap,
+                          ctx->kept_count.as<uint32_t>() + g0, maxk, ctx->row_off.as<int64_t>(),
+                          ctx->frame_num.as<int64_t>(), tc, (int32_t)g0, ng, ctx->st));
+    }
+    return GT_OK;
+}
+
+template <typename T>
+gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
+                     int32_t W, const int64_t* frame_numbers, const int64_t* reset_points, int64_t n_reset,
+                     gt_table* tab) {
+    LocateConsts c;
+    CKS(make_locate_consts(ctx, p, H, W, c));
+    LogTables lt;
+    const bool log_style = (p.style == GT_STYLE_LOG);
+    if (log_style) {
+        lt = log_tables(p);
+        if (lt.radii.empty()) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "n_radii must be >= 1");
+        if (lt.radii.size() > (size_t)kMaxRadii) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "n_radii > 256");
+        if (laplace_smem_bytes(lt.max_rint) > 227 * 1024)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "max_radius too large for the LoG tile kernel");
+    } else {
+        if (bandpass_smem_bytes(c.R, c.kd, true) > 227 * 1024)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "separation/smoothing_size too large for the tile kernel");
+    }
+    if (bandpass_smem_bytes(c.R, 1, false) > 227 * 1024)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size too large for the tile kernel");
+    const int F = pick_chunk(NT, H, W, log_style ? (int)lt.radii.size() : 0);
+    ctx->total = NT;
+    ctx->done = 0;
+    for (int attempt = 0;; attempt++) {
+        uint32_t fl = 0;
+        CKS(locate_pass<T>(ctx, p, frames, on_device, NT, H, W, c, log_style ? &lt : nullptr, F, &fl));
+        if (!(fl & (kFlagCandOverflow | kFlagFeatOverflow))) break;
+        const uint64_t npx = (uint64_t)H * W;
+        if (attempt > 8) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame capacity exceeded");
+        if (fl & kFlagCandOverflow) {
+            uint64_t nc = std::min<uint64_t>((uint64_t)ctx->cand_cap * 4, npx + 1);
+            if (nc <= ctx->cand_cap)
+                return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "candidate capacity exceeded");
+            ctx->cand_cap = (uint32_t)nc;
+        }
+        if (fl & kFlagFeatOverflow) {
+            uint64_t nf = std::min<uint64_t>((uint64_t)ctx->feat_cap * 4, std::min<uint64_t>(npx + 1, 1u << 24));
+            if (nf <= ctx->feat_cap)
+                return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame detection capacity exceeded");
+            ctx->feat_cap = (uint32_t)nf;
+        }
+    }
+    std::vector<int64_t> fnum(NT);
+    for (int64_t t = 0; t < NT; t++) fnum[t] = frame_numbers ? frame_numbers[t] : t;
+    std::vector<int64_t> row_off;
+    CKS(assemble_table(ctx, NT, fnum, log_style, tab, row_off));
+    if (p.has_search_range) {
+        LinkJob job;
+        job.goff = row_off;
+        job.vgrp = {0, (int32_t)NT};
+        job.reset.assign(NT, 0);
+        for (int64_t t = 0; t < NT; t++)
+            for (int64_t k = 0; k < n_reset; k++)
+                if (reset_points[k] == fnum[t]) job.reset[t] = 1;
+        job.radius = p.search_range;
+        job.memory = (int32_t)p.memory;
+        const size_t n1 = std::max<int64_t>(tab->n, 1);
+        CK(ctx->l_ids.ensure(n1 * 8));
+        CK(tab->particle.ensure(n1 * 8));
+        CK(tab->duration.ensure(n1 * 8));
+        CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
+                     ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
+        if (tab->n > 0)
+            f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
+                ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+        CK(cudaGetLastError());
+        tab->has[GT_COL_PARTICLE] = true;
+        tab->has[GT_COL_DURATION] = true;
+    }
+    if (!p.doughnut_correction) {
+        tab->has[GT_COL_RAW_MASS] = tab->has[GT_COL_RAW_BG_MEDIAN] = tab->has[GT_COL_RAW_MASS_CORRECTED] = false;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    drain_profile(ctx);
+    return GT_OK;
+}
+
+gt_status validate(gt_ctx* ctx, const gt_params* p, const void* frames, int32_t dtype, int64_t T, int32_t H,
+                   int32_t W) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    if (!p || !frames) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
+    if (T <= 0) return set_err(ctx, GT_ERR_EMPTY_ITERATOR, "the provided video doesn't contain any frames.");
+    if (H <= 0 || W <= 0) return set_err(ctx, GT_ERR_DIMENSION_MISMATCH, "frame dimensions must be positive");
+    if ((int64_t)H * W >= (1LL << 31)) return set_err(ctx, GT_ERR_DIMENSION_MISMATCH, "frame too large");
+    if (dtype != GT_DTYPE_U16 && dtype != GT_DTYPE_F32 && dtype != GT_DTYPE_U8)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype);
+    if (p->style != GT_STYLE_TRACKPY && p->style != GT_STYLE_LOG)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unknown style %d", p->style);
+    if (p->has_snr || p->has_minmass_snr || p->has_adaptive_background || p->has_illumination_sigma)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                       "snr / minmass_snr / adaptive_background / illumination correction are not supported by "
+                       "this build");
+    if (p->style == GT_STYLE_TRACKPY && p->diameter == 0)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "diameter must be positive");
+    CK(cudaSetDevice(ctx->device));
+    return GT_OK;
+}
+
+// FrameSubsetter grouping of rows sorted by their frame column
+// (src/linking.rs:97-196): a group is emitted whenever the frame number
+// increases (so a positive first frame yields a leading empty group 0); a
+// decreasing frame number is NonSortedCharacterization.
+gt_status subset_groups(gt_ctx* ctx, const float* rows, int64_t n, int ncols, std::vector<int64_t>& goff,
+                        std::vector<int64_t>& gframe) {
+    goff.assign(1, 0);
+    gframe.clear();
+    float cur = 0.0f;
+    int64_t idx = 0;
+    while (true) {
+        if (idx < n) {
+            float f = rows[idx * ncols];
+            if (f > cur) {
+                goff.push_back(idx);
+                gframe.push_back((int64_t)cur);
+                cur = f;
+                continue;
+            }
+            if (f < cur)
+                return set_err(ctx, GT_ERR_NON_SORTED_CHARACTERIZATION,
+                               "the points provided for characterization aren't sorted in ascending frame number.");
+            idx++;
+        } else {
+            if (idx > goff.back()) {
+                goff.push_back(idx);
+                gframe.push_back((int64_t)cur);
+            }
+            break;
+        }
+    }
+    return GT_OK;
+}
+
+template <typename T>
+__global__ void mean_accumulate_kernel(const T* __restrict__ frames, int nf, int64_t npix, float* __restrict__ acc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    float a = acc[i];
+    for (int t = 0; t < nf; t++) a = __fadd_rn(a, load_px<T>(frames, (size_t)t * npix + i));
+    acc[i] = a;
+}
+
+__global__ void mean_divide_kernel(float* acc, int64_t npix, float n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < npix) acc[i] = __fdiv_rn(acc[i], n);
+}
+
+template <typename T>
+gt_status mean_impl(gt_ctx* ctx, const T* frames, bool on_device, int64_t NT, int32_t H, int32_t W, float* out) {
+    const size_t npx = (size_t)H * W;
+    const int F = pick_chunk(NT, H, W, 0);
+    CK(ctx->processed.ensure(npx * 4));
+    float* acc = ctx->processed.as<float>();
+    CK(cudaMemsetAsync(acc, 0, npx * 4, ctx->st));
+    if (!on_device) CK(ctx->stage[0].ensure((size_t)F * npx * sizeof(T)));
+    for (int64_t f0 = 0; f0 < NT; f0 += F) {
+        if (interrupted(ctx)) return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
+        int nf = (int)std::min<int64_t>(F, NT - f0);
+        const T* src = frames + f0 * npx;
+        if (!on_device) {
+            CK(cudaMemcpyAsync(ctx->stage[0].p, src, (size_t)nf * npx * sizeof(T), cudaMemcpyHostToDevice,
+                               ctx->st));
+            src = ctx->stage[0].as<T>();
+        }
+        mean_accumulate_kernel<T><<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(src, nf, npx, acc);
+        CK(cudaGetLastError());
+    }
+    mean_divide_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(acc, npx, (float)NT);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, acc, npx * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GT_OK;
+}
+
+// characterize_points (src/execute_gpu.rs:189-229, 1286-1319;
+// gpu_tracking_macros/src/lib.rs:641-683)
+template <typename T>
+gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, bool on_device, int64_t NT, int32_t H,
+                          int32_t W, const float* points, int64_t n, int32_t has_frames, int32_t has_r,
+                          gt_table* tab) {
+    gt_params p = p0;
+    p.style = GT_STYLE_TRACKPY;
+    p.filter_close = 0;
+    p.characterize = 1;
+    const int ncols = 2 + (has_frames ? 1 : 0) + (has_r ? 1 : 0);
+    const int c0 = has_frames ? 1 : 0;
+    std::vector<int64_t> goff, gframe;
+    if (has_frames) {
+        CKS(subset_groups(ctx, points, n, ncols, goff, gframe));
+    } else {
+        goff.assign(1, 0);
+        for (int64_t t = 0; t < NT; t++) {
+            goff.push_back(goff.back() + n);
+            gframe.push_back(t);
+        }
+    }
+    const int64_t G = (int64_t)gframe.size();
+    if (G == 0) return set_err(ctx, GT_ERR_EMPTY_ITERATOR, "the provided video doesn't contain any frames.");
+    for (int64_t g = 0; g < G; g++)
+        if (gframe[g] >= NT)
+            return set_err(ctx, GT_ERR_FRAME_OUT_OF_BOUNDS,
+                           "Requested a frame outside the length\n of the video. Video length is %lld, requested "
+                           "frame %lld",
+                           (long long)NT, (long long)gframe[g]);
+    // (y, x, r) per point in group order
+    std::vector<float> pts((size_t)goff.back() * 3);
+    int64_t maxg = 0;
+    float max_r = 0.0f;
+    for (int64_t g = 0; g < G; g++) {
+        maxg = std::max(maxg, goff[g + 1] - goff[g]);
+        for (int64_t i = goff[g]; i < goff[g + 1]; i++) {
+            int64_t src = has_frames ? i : (i - goff[g]);
+            pts[3 * i + 0] = points[src * ncols + c0];
+            pts[3 * i + 1] = points[src * ncols + c0 + 1];
+            pts[3 * i + 2] = has_r ? points[src * ncols + c0 + 2] : 0.0f;
+            if (has_r && pts[3 * i + 2] > max_r) max_r = pts[3 * i + 2];
+        }
+    }
+    LocateConsts c;
+    CKS(make_locate_consts(ctx, p, H, W, c));
+    if (bandpass_smem_bytes(c.R, 1, false) > 227 * 1024)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size too large for the tile kernel");
+    const size_t npx = (size_t)H * W;
+    const int F = pick_chunk(G, H, W, 0);
+    const uint32_t feat_cap = (uint32_t)std::max<int64_t>(maxg, 1);
+    if (feat_cap >= (1u << 24)) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "too many points in one frame");
+    CK(ctx->processed.ensure((size_t)F * npx * 4));
+    CK(ctx->stage[0].ensure((size_t)F * npx * sizeof(T)));
+    CK(ctx->feats_raw.ensure((size_t)F * feat_cap * sizeof(Feature)));
+    CK(ctx->feat_count.ensure((size_t)F * 4));
+    CK(ctx->feats_out.ensure((size_t)G * feat_cap * sizeof(Feature)));
+    CK(ctx->kept_count.ensure((size_t)G * 4));
+    CK(ctx->flags.ensure(16));
+    CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
+    size_t fin_per_frame = 0;
+    if (feat_cap > (uint32_t)kFinalizeSmemSort) {
+        size_t np2 = 1;
+        while (np2 < feat_cap) np2 <<= 1;
+        fin_per_frame = (np2 * 17 + 255) & ~(size_t)255;
+    }
+    CK(ctx->fin_scratch.ensure(std::max<size_t>(fin_per_frame * F, 256)));
+    DBuf dpts, dgoff, dgloc;
+    CKS(upload(ctx, dpts, pts));
+    CKS(upload(ctx, dgoff, goff));
+    std::vector<int32_t> gloc(G);
+    for (int64_t g = 0; g < G; g++) gloc[g] = (int32_t)(g % F);
+    CKS(upload(ctx, dgloc, gloc));
+    std::vector<int32_t> ident(F);
+    for (int i = 0; i < F; i++) ident[i] = i;
+    CKS(upload(ctx, ctx->ident, ident));
+    std::vector<float2> atab;
+    std::vector<int32_t> aoff;
+    int max_rint = std::max(std::max(0, (c.circle - 1) / 2), (int)std::ceil(max_r));
+    angle_tables(max_rint, atab, aoff);
+    std::vector<short2> dn;
+    std::vector<int4> dmeta;
+    doughnut_tables(p, std::vector<float>{(float)p.diameter / 2.0f}, dn, dmeta);
+    CKS(upload(ctx, ctx->tabs_f, atab));
+    CKS(upload(ctx, ctx->tabs_i, aoff));
+    CKS(upload(ctx, ctx->tabs_s, dn));
+    CKS(upload(ctx, ctx->tabs_m, dmeta));
+    FinalizeConsts fc;
+    std::memset(&fc, 0, sizeof(fc));
+    fc.H = H;
+    fc.W = W;
+    fc.doughnut = p.doughnut_correction ? 1 : 0;
+    fc.presorted = 1;
+    fc.band = -1;
+    fc.scratch_per_frame = fin_per_frame;
+    ctx->total = G;
+    ctx->done = 0;
+    for (int64_t g0 = 0; g0 < G; g0 += F) {
+        if (interrupted(ctx)) return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
+        const int ng = (int)std::min<int64_t>(F, G - g0);
+        T* stage = ctx->stage[0].as<T>();
+        for (int g = 0; g < ng; g++)
+            CK(cudaMemcpyAsync(stage + (size_t)g * npx, frames + (size_t)gframe[g0 + g] * npx, npx * sizeof(T),
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)ng * 4, ctx->st));
+        CK(launch_bandpass<T>(stage, (int64_t)npx, ctx->processed.as<float>(), c, ng, false, nullptr, nullptr, 0,
+                              ctx->flags.as<uint32_t>(), ctx->st));
+        CK(launch_characterize_points<T>(ctx->processed.as<float>(), stage, (int64_t)npx, c, dpts.as<float>(),
+                                         dgoff.as<int64_t>(), dgloc.as<int32_t>(), (int32_t)g0, ng, maxg,
+                                         ctx->tabs_f.as<float2>(), ctx->tabs_i.as<int32_t>(), (int32_t)aoff.size(),
+                                         has_r, ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
+                                         feat_cap, ctx->st));
+        CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
+                              ctx->feats_out.as<Feature>() + (size_t)g0 * feat_cap,
+                              ctx->kept_count.as<uint32_t>() + g0, ctx->fin_scratch.as<uint8_t>(), fc, stage,
+                              (int64_t)npx, ctx->ident.as<int32_t>(), ctx->tabs_s.as<short2>(),
+                              ctx->tabs_m.as<int4>(), ctx->flags.as<uint32_t>(), ng, ctx->st));
+        ctx->done = g0 + ng;
+    }
+    const uint32_t saved_cap = ctx->feat_cap;
+    ctx->feat_cap = feat_cap;
+    std::vector<int64_t> row_off;
+    gt_status st = assemble_table(ctx, G, gframe, false, tab, row_off);
+    ctx->feat_cap = saved_cap;
+    CKS(st);
+    tab->has[GT_COL_R] = has_r != 0;
+    tab->has[GT_COL_MAX_INTENSITY] = tab->has[GT_COL_COUNT] = false;
+    if (!p.doughnut_correction)
+        tab->has[GT_COL_RAW_MASS] = tab->has[GT_COL_RAW_BG_MEDIAN] = tab->has[GT_COL_RAW_MASS_CORRECTED] = false;
+    if (p.has_search_range) {
+        LinkJob job;
+        job.goff = row_off;
+        job.vgrp = {0, (int32_t)G};
+        job.reset.assign(G, 0);
+        job.radius = p.search_range;
+        job.memory = (int32_t)p.memory;
+        const size_t n1 = std::max<int64_t>(tab->n, 1);
+        CK(ctx->l_ids.ensure(n1 * 8));
+        CK(tab->particle.ensure(n1 * 8));
+        CK(tab->duration.ensure(n1 * 8));
+        CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
+                     ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
+        if (tab->n > 0)
+            f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
+                ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+        CK(cudaGetLastError());
+        tab->has[GT_COL_PARTICLE] = true;
+        tab->has[GT_COL_DURATION] = true;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return GT_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* gt_version(void) { return "gpu_tracking_b200 0.1 (sm_100a)"; }
+
+void gt_params_default(gt_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    // TrackingParams::default() (src/gpu_setup.rs:61-97)
+    p->style = GT_STYLE_TRACKPY;
+    p->diameter = 9;
+    p->separation = 10;
+    p->filter_close = 1;
+    p->max_iterations = 10;
+    p->minmass = 0.0f;
+    p->characterize = 0;
+    p->doughnut_correction = 0;
+    p->truncate_preprocessed = 1;
+    p->shift_threshold = 0.6f;
+    p->noise_size = 1.0f;
+    p->n_radii = 10;
+}
+
+gt_status gt_create(int32_t device, gt_ctx** out) {
+    if (!out) return GT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return GT_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return GT_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return GT_ERR_NO_DEVICE;
+    gt_ctx* ctx = new gt_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return GT_ERR_CUDA;
+    }
+    for (int i = 0; i < 2; i++) {
+        cudaEventCreateWithFlags(&ctx->used[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ctx->filled[i], cudaEventDisableTiming);
+    }
+    *out = ctx;
+    return GT_OK;
+}
+
+void gt_destroy(gt_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->st);
+    cudaStreamSynchronize(ctx->cp);
+    drain_profile(ctx);
+    for (auto e : ctx->event_pool) cudaEventDestroy(e);
+    for (int i = 0; i < 2; i++) {
+        cudaEventDestroy(ctx->used[i]);
+        cudaEventDestroy(ctx->filled[i]);
+    }
+    cudaStreamDestroy(ctx->st);
+    cudaStreamDestroy(ctx->cp);
+    delete ctx;
+}
+
+const char* gt_last_error(const gt_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+gt_status gt_set_interrupt(gt_ctx* ctx, const volatile int32_t* flag) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    ctx->interrupt = flag;
+    return GT_OK;
+}
+
+gt_status gt_progress(const gt_ctx* ctx, int64_t* done, int64_t* total) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    if (done) *done = ctx->done.load();
+    if (total) *total = ctx->total.load();
+    return GT_OK;
+}
+
+int64_t gt_table_nrows(const gt_table* t) { return t ? t->n : 0; }
+
+int32_t gt_table_has_column(const gt_table* t, int32_t column) {
+    if (!t || column < 0 || column >= GT_NUM_COLUMNS) return 0;
+    return t->has[column] ? 1 : 0;
+}
+
+gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst) {
+    if (!t || !dst || column < 0 || column >= GT_NUM_COLUMNS) return GT_ERR_INVALID_ARGUMENT;
+    if (!t->has[column]) return GT_ERR_INVALID_ARGUMENT;
+    if (t->n == 0) return GT_OK;
+    cudaSetDevice(t->device);
+    if (column == GT_COL_FRAME || column == GT_COL_PARTICLE || column == GT_COL_DURATION) {
+        std::vector<int64_t> v(t->n);
+        const DBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
+        if (cudaMemcpy(v.data(), b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
+        for (int64_t i = 0; i < t->n; i++) dst[i] = (float)v[i];
+        return GT_OK;
+    }
+    if (cudaMemcpy(dst, t->col[column].p, t->n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
+    return GT_OK;
+}
+
+gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst) {
+    if (!t || !dst) return GT_ERR_INVALID_ARGUMENT;
+    if (column != GT_COL_FRAME && column != GT_COL_PARTICLE && column != GT_COL_DURATION)
+        return GT_ERR_INVALID_ARGUMENT;
+    if (!t->has[column]) return GT_ERR_INVALID_ARGUMENT;
+    if (t->n == 0) return GT_OK;
+    cudaSetDevice(t->device);
+    const DBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
+    if (cudaMemcpy(dst, b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
+    return GT_OK;
+}
+
+void gt_table_free(gt_table* t) {
+    if (!t) return;
+    cudaSetDevice(t->device);
+    delete t;
+}
+
+gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int32_t dtype, int64_t T, int32_t H,
+                   int32_t W, const int64_t* frame_numbers, const int64_t* linker_reset_points, int64_t n_reset,
+                   gt_table** out) {
+    if (!out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    CKS(validate(ctx, params, frames, dtype, T, H, W));
+    bool on_device = false;
+    CKS(check_frames_ptr(ctx, frames, &on_device));
+    std::unique_ptr<gt_table> tab(new gt_table());
+    tab->device = ctx->device;
+    gt_status st;
+    if (dtype == GT_DTYPE_U16)
+        st = batch_impl<uint16_t>(ctx, *params, (const uint16_t*)frames, on_device, T, H, W, frame_numbers,
+                                  linker_reset_points, n_reset, tab.get());
+    else if (dtype == GT_DTYPE_F32)
+        st = batch_impl<float>(ctx, *params, (const float*)frames, on_device, T, H, W, frame_numbers,
+                               linker_reset_points, n_reset, tab.get());
+    else
+        st = batch_impl<uint8_t>(ctx, *params, (const uint8_t*)frames, on_device, T, H, W, frame_numbers,
+                                 linker_reset_points, n_reset, tab.get());
+    if (st != GT_OK) return st;
+    *out = tab.release();
+    return GT_OK;
+}
+
+gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const void* frames, int32_t dtype, int64_t T,
+                                 int32_t H, int32_t W, const float* points, int64_t n_points, int32_t has_frames,
+                                 int32_t has_r, gt_table** out) {
+    if (!out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    CKS(validate(ctx, params, frames, dtype, T, H, W));
+    if (n_points > 0 && !points) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null points");
+    bool on_device = false;
+    CKS(check_frames_ptr(ctx, frames, &on_device));
+    std::unique_ptr<gt_table> tab(new gt_table());
+    tab->device = ctx->device;
+    gt_status st;
+    if (dtype == GT_DTYPE_U16)
+        st = charpoints_impl<uint16_t>(ctx, *params, (const uint16_t*)frames, on_device, T, H, W, points, n_points,
+                                       has_frames, has_r, tab.get());
+    else if (dtype == GT_DTYPE_F32)
+        st = charpoints_impl<float>(ctx, *params, (const float*)frames, on_device, T, H, W, points, n_points,
+                                    has_frames, has_r, tab.get());
+    else
+        st = charpoints_impl<uint8_t>(ctx, *params, (const uint8_t*)frames, on_device, T, H, W, points, n_points,
+                                      has_frames, has_r, tab.get());
+    if (st != GT_OK) return st;
+    *out = tab.release();
+    return GT_OK;
+}
+
+gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n, float search_range, uint32_t memory,
+                  int64_t* particle_out) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    if (n == 0) return GT_OK;
+    if (!frame_y_x || !particle_out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    LinkJob job;
+    std::vector<int64_t> gframe;
+    CKS(subset_groups(ctx, frame_y_x, n, 3, job.goff, gframe));
+    const int64_t N = job.goff.back();
+    job.vgrp = {0, (int32_t)gframe.size()};
+    job.reset.assign(gframe.size(), 0);
+    job.radius = search_range;
+    job.memory = (int32_t)memory;
+    std::vector<float> px(N), py(N);
+    for (int64_t i = 0; i < N; i++) {
+        px[i] = frame_y_x[3 * i + 1];
+        py[i] = frame_y_x[3 * i + 2];
+    }
+    CKS(upload(ctx, ctx->l_px, px));
+    CKS(upload(ctx, ctx->l_py, py));
+    CK(ctx->l_ids.ensure(std::max<int64_t>(N, 1) * 8));
+    CKS(run_link(ctx, job, ctx->l_px.as<float>(), ctx->l_py.as<float>(), ctx->l_ids.as<int64_t>(), nullptr, nullptr,
+                 nullptr));
+    CK(cudaMemcpyAsync(particle_out, ctx->l_ids.p, N * 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return GT_OK;
+}
+
+// connect_all (src/linking.rs:960-1020): the frame bookkeeping runs on the
+// host exactly as the reference's iterators do; every connected frame pair is
+// an independent two-frame linking job, all of them solved in one launch.
+gt_status gt_connect(gt_ctx* ctx, const float* a1, int64_t n1, const float* a2, int64_t n2, float search_range,
+                     int64_t* out1, int64_t* out2) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<int64_t> g1, f1, g2, f2;
+    CKS(subset_groups(ctx, a1, n1, 3, g1, f1));
+    CKS(subset_groups(ctx, a2, n2, 3, g2, f2));
+    // operations in the reference's order
+    struct Op {
+        int kind;  // 0 fill side 1, 1 fill side 2, 2 connect
+        int64_t i1, i2;
+    };
+    std::vector<Op> ops;
+    size_t p1 = 0, p2 = 0;
+    auto next1 = [&](int64_t* g) { if (p1 < f1.size()) { *g = (int64_t)p1++; return true; } return false; };
+    auto next2 = [&](int64_t* g) { if (p2 < f2.size()) { *g = (int64_t)p2++; return true; } return false; };
+    while (true) {
+        int64_t a, b;
+        bool h1 = next1(&a), h2 = next2(&b);
+        if (h1 && h2) {
+            if (f1[a] == f2[b]) {
+                ops.push_back({2, a, b});
+                continue;
+            }
+            // sync_iterators (src/linking.rs:914-958)
+            bool left = f1[a] > f2[b];
+            int64_t hit = left ? a : b;
+            if (left) ops.push_back({1, -1, b}); else ops.push_back({0, a, -1});
+            while (true) {
+                int64_t nx;
+                bool got = left ? next2(&nx) : next1(&nx);
+                if (!got) {
+                    if (left) ops.push_back({0, hit, -1}); else ops.push_back({1, -1, hit});
+                    break;
+                }
+                int64_t fh = left ? f1[hit] : f2[hit];
+                int64_t fn = left ? f2[nx] : f1[nx];
+                if (fh > fn) {
+                    if (left) ops.push_back({1, -1, nx}); else ops.push_back({0, nx, -1});
+                } else if (fh == fn) {
+                    if (left) ops.push_back({2, hit, nx}); else ops.push_back({2, nx, hit});
+                    break;
+                } else {
+                    if (left) ops.push_back({1, -1, nx}); else ops.push_back({0, nx, -1});
+                    if (left) ops.push_back({0, hit, -1}); else ops.push_back({1, -1, hit});
+                    hit = nx;
+                    left = !left;
+                }
+            }
+        } else if (h1) {
+            ops.push_back({0, a, -1});
+        } else if (h2) {
+            ops.push_back({1, -1, b});
+        } else {
+            break;
+        }
+    }
+    // linking jobs for the connect operations
+    LinkJob job;
+    job.goff.assign(1, 0);
+    job.vgrp.assign(1, 0);
+    job.radius = search_range;
+    job.memory = 0;
+    std::vector<float> px, py;
+    std::vector<int64_t> op_video(ops.size(), -1);
+    for (size_t k = 0; k < ops.size(); k++) {
+        if (ops[k].kind != 2) continue;
+        op_video[k] = (int64_t)job.vgrp.size() - 1;
+        for (int side = 0; side < 2; side++) {
+            const float* arr = side ? a2 : a1;
+            const std::vector<int64_t>& go = side ? g2 : g1;
+            int64_t gi = side ? ops[k].i2 : ops[k].i1;
+            for (int64_t i = go[gi]; i < go[gi + 1]; i++) {
+                px.push_back(arr[3 * i + 1]);
+                py.push_back(arr[3 * i + 2]);
+            }
+            job.goff.push_back((int64_t)px.size());
+            job.reset.push_back(0);
+        }
+        job.vgrp.push_back((int32_t)job.goff.size() - 1);
+    }
+    std::vector<int64_t> local((size_t)px.size());
+    std::vector<int64_t> counters;
+    if (!px.empty()) {
+        CKS(upload(ctx, ctx->l_px, px));
+        CKS(upload(ctx, ctx->l_py, py));
+        CK(ctx->l_ids.ensure(px.size() * 8));
+        CKS(run_link(ctx, job, ctx->l_px.as<float>(), ctx->l_py.as<float>(), ctx->l_ids.as<int64_t>(), nullptr,
+                     nullptr, &counters));
+        CK(cudaMemcpy(local.data(), ctx->l_ids.p, px.size() * 8, cudaMemcpyDeviceToHost));
+    }
+    std::vector<int64_t> r1, r2;
+    int64_t part = 0;
+    for (size_t k = 0; k < ops.size(); k++) {
+        const Op& o = ops[k];
+        if (o.kind == 0) {
+            for (int64_t i = g1[o.i1]; i < g1[o.i1 + 1]; i++) r1.push_back(part++);
+        } else if (o.kind == 1) {
+            for (int64_t i = g2[o.i2]; i < g2[o.i2 + 1]; i++) r2.push_back(part++);
+        } else {
+            int64_t v = op_video[k];
+            int64_t b0 = job.goff[job.vgrp[v]], b1 = job.goff[job.vgrp[v] + 1], b2 = job.goff[job.vgrp[v] + 2];
+            for (int64_t i = b0; i < b1; i++) r1.push_back(part + local[i]);
+            for (int64_t i = b1; i < b2; i++) r2.push_back(part + local[i]);
+            part += counters[v];
+        }
+    }
+    if ((int64_t)r1.size() != n1 || (int64_t)r2.size() != n2)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                       "connect produced %lld/%lld ids for %lld/%lld rows (frame interleaving the reference "
+                       "double-counts)",
+                       (long long)r1.size(), (long long)r2.size(), (long long)n1, (long long)n2);
+    if (n1) std::memcpy(out1, r1.data(), n1 * 8);
+    if (n2) std::memcpy(out2, r2.data(), n2 * 8);
+    return GT_OK;
+}
+
+gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
+                        float* out) {
+    gt_params p;
+    gt_params_default(&p);
+    CKS(validate(ctx, &p, frames, dtype, T, H, W));
+    if (!out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null output");
+    bool on_device = false;
+    CKS(check_frames_ptr(ctx, frames, &on_device));
+    if (dtype == GT_DTYPE_U16) return mean_impl<uint16_t>(ctx, (const uint16_t*)frames, on_device, T, H, W, out);
+    if (dtype == GT_DTYPE_F32) return mean_impl<float>(ctx, (const float*)frames, on_device, T, H, W, out);
+    return mean_impl<uint8_t>(ctx, (const uint8_t*)frames, on_device, T, H, W, out);
+}
+
+// Per-kernel CUDA-event timing on the compute stream (diagnostics; no
+// counterpart in the reference).  name_out receives a comma-separated list.
+gt_status gt_profile_enable(gt_ctx* ctx, int32_t enable) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    ctx->profile = enable != 0;
+    ctx->stats.clear();
+    return GT_OK;
+}
+
+gt_status gt_profile_read(gt_ctx* ctx, const char* name, int64_t* launches, double* total_ms) {
+    if (!ctx || !name) return GT_ERR_INVALID_ARGUMENT;
+    drain_profile(ctx);
+    auto it = ctx->stats.find(name);
+    if (it == ctx->stats.end()) {
+        if (launches) *launches = 0;
+        if (total_ms) *total_ms = 0.0;
+        return GT_OK;
+    }
+    if (launches) *launches = it->second.launches;
+    if (total_ms) *total_ms = it->second.ms;
+    return GT_OK;
+}
+
+}  // extern "C"

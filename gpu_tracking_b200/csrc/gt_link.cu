@@ -1,0 +1,794 @@
+// gt_link.cu — trackpy-style optimal subnet linking on the GPU.
+//
+// Replaces Linker / link / recurse / recurse2 (src/linking.rs:345-816) and
+// the kd-tree neighbour search (within_radius_rd2, src/linking.rs:211-247).
+//
+//   sort_groups_kernel   points of every frame group sorted by row (the
+//                        grid-free neighbour index: a binary search on rows
+//                        plus the exact within_radius_rd2 predicate).
+//   count/fill_lists     for every point and every lag k = 1..memory+1, the
+//                        forward (dests in group+k) and backward (sources in
+//                        group-k) neighbour lists in ascending point order; all
+//                        frame pairs in parallel.
+//   link_video_kernel    one CTA per video walks its frames in order (the
+//                        linker's only true sequential dependency) doing each
+//                        frame's work in parallel: memory merge, subnet
+//                        detection by union-find, the reference's DFS order
+//                        per subnet, the exact branch-and-bound per subnet
+//                        (one thread each, same float operation sequence),
+//                        new ids in destination order, memory ring and
+//                        duration bookkeeping.
+#include "gt_kernels.h"
+
+namespace gt {
+
+constexpr int kLinkThreads = 1024;
+constexpr int kSortSmem = 4096;
+constexpr long long kSubnetBudget = 1ll << 28;
+
+// ------------------------------------------------------------ group sorting
+__global__ void __launch_bounds__(kLinkThreads)
+sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restrict__ scratch, size_t per_group) {
+    __shared__ uint64_t sk[kSortSmem];
+    const int g = blockIdx.x;
+    const int64_t a = in.goff[g], n = in.goff[g + 1] - a;
+    if (n == 0) return;
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    uint64_t* keys = (np2 <= kSortSmem) ? sk : scratch + (size_t)g * per_group;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x)
+        keys[i] = (i < n) ? (((uint64_t)float_order_key(in.px[a + i]) << 32) | (uint64_t)i) : ~0ull;
+    __syncthreads();
+    block_sort_u64(keys, np2);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) srt[a + i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
+}
+
+// First sorted position of group t whose row key is >= klo, and first > khi.
+__device__ __forceinline__ void row_range(const LinkInput& in, const uint32_t* srt, int t, float lo, float hi,
+                                          int64_t* p0, int64_t* p1) {
+    const int64_t a = in.goff[t], n = in.goff[t + 1] - a;
+    const uint32_t klo = float_order_key(lo), khi = float_order_key(hi);
+    int64_t x = 0, y = n;
+    while (x < y) {
+        int64_t m = (x + y) >> 1;
+        if (float_order_key(in.px[a + srt[a + m]]) < klo) x = m + 1; else y = m;
+    }
+    *p0 = x;
+    y = n;
+    while (x < y) {
+        int64_t m = (x + y) >> 1;
+        if (float_order_key(in.px[a + srt[a + m]]) <= khi) x = m + 1; else y = m;
+    }
+    *p1 = x;
+}
+
+__device__ __forceinline__ void search_bounds(float q, float R, float* lo, float* hi) {
+    // conservative superset of the rows within_rd2 can accept
+    float delta = __fmul_rn(fmaxf(fabsf(q), R), 1.0f / 1048576.0f) + 1e-30f;
+    *lo = __fsub_rn(__fsub_rn(q, R), delta);
+    *hi = __fadd_rn(__fadd_rn(q, R), delta);
+}
+
+__device__ __forceinline__ void group_video_range(const LinkInput& in, int h, int* vb, int* ve) {
+    int x = 0, y = in.nvideos;  // last video with vgrp[v] <= h
+    while (y - x > 1) {
+        int m = (x + y) >> 1;
+        if (in.vgrp[m] <= h) x = m; else y = m;
+    }
+    *vb = in.vgrp[x];
+    *ve = in.vgrp[x + 1];
+}
+
+// mode 0: count, mode 1: fill (and sort ascending)
+template <int kMode>
+__global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t* b_cnt) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= in.npoints) return;
+    const int K = in.memory + 1;
+    const int h = in.pgroup[p];
+    int vb, ve;
+    group_video_range(in, h, &vb, &ve);
+    const float qx = in.px[p], qy = in.py[p];
+    const float R = in.radius;
+    float lo, hi;
+    search_bounds(qx, R, &lo, &hi);
+    const bool qnan = (qx != qx) || (qy != qy);
+    for (int k = 1; k <= K; k++) {
+        // forward: p is a source, dests in group h + k
+        int t = h + k;
+        int64_t cnt = 0;
+        if (t < ve && !qnan) {
+            int64_t s0, s1;
+            row_range(in, L.srt, t, lo, hi, &s0, &s1);
+            const int64_t a = in.goff[t];
+            int32_t* out = kMode ? L.f_pts + L.f_off[p * K + (k - 1)] : nullptr;
+            for (int64_t m = s0; m < s1; m++) {
+                int64_t d = a + L.srt[a + m];
+                float dist;
+                if (within_rd2(in.px[d], in.py[d], qx, qy, R, &dist)) {
+                    if (kMode) out[cnt] = (int32_t)(d - a);
+                    cnt++;
+                }
+            }
+            if (kMode) {  // ascending destination order
+                for (int64_t i = 1; i < cnt; i++) {
+                    int32_t v = out[i];
+                    int64_t j = i - 1;
+                    while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; j--; }
+                    out[j + 1] = v;
+                }
+            }
+        }
+        if (!kMode) f_cnt[p * K + (k - 1)] = cnt;
+        // backward: p is a dest, sources in group h - k
+        t = h - k;
+        cnt = 0;
+        if (t >= vb && !qnan) {
+            int64_t s0, s1;
+            row_range(in, L.srt, t, lo, hi, &s0, &s1);
+            const int64_t a = in.goff[t];
+            int32_t* out = kMode ? L.b_pts + L.b_off[p * K + (k - 1)] : nullptr;
+            float* outd = kMode ? L.b_dist + L.b_off[p * K + (k - 1)] : nullptr;
+            for (int64_t m = s0; m < s1; m++) {
+                int64_t s = a + L.srt[a + m];
+                float dist;
+                if (within_rd2(qx, qy, in.px[s], in.py[s], R, &dist)) {
+                    if (kMode) {
+                        out[cnt] = (int32_t)(s - a);
+                        outd[cnt] = dist;
+                    }
+                    cnt++;
+                }
+            }
+            if (kMode) {  // ascending source order
+                for (int64_t i = 1; i < cnt; i++) {
+                    int32_t v = out[i];
+                    float vd = outd[i];
+                    int64_t j = i - 1;
+                    while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; outd[j + 1] = outd[j]; j--; }
+                    out[j + 1] = v;
+                    outd[j + 1] = vd;
+                }
+            }
+        }
+        if (!kMode) b_cnt[p * K + (k - 1)] = cnt;
+    }
+}
+
+// ---------------------------------------------------------- scratch layout
+struct Lay {
+    size_t start, idstamp, firstpos, srcidx, srcstamp, src_pt, ring_pt, ring_n, ringpre, d_off, e_src, e_dist,
+        out_src, parent, comp_nd, comp_ns, comp_off, comp_soff, roots, pathD, pathS, srcLocal, srcUsed, vis_d,
+        vis_s, stack, r2a, r2b, r2c, r2used, tmp, total;
+};
+
+__host__ __device__ inline size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline Lay make_lay(int64_t G, int64_t E, int64_t NP, int64_t M) {
+    Lay l;
+    const int64_t Smax = G * (M + 1);
+    size_t o = 0;
+    l.start = o; o = al(o + 8 * NP);
+    l.idstamp = o; o = al(o + 4 * NP);
+    l.firstpos = o; o = al(o + 8 * NP);
+    l.srcidx = o; o = al(o + 4 * NP);
+    l.srcstamp = o; o = al(o + 4 * NP);
+    l.src_pt = o; o = al(o + 4 * Smax);
+    l.ring_pt = o; o = al(o + 4 * (M * G + 1));
+    l.ring_n = o; o = al(o + 4 * (M + 1));
+    l.ringpre = o; o = al(o + 4 * (M + 2));
+    l.d_off = o; o = al(o + 4 * (G + 1));
+    l.e_src = o; o = al(o + 4 * (E + 1));
+    l.e_dist = o; o = al(o + 4 * (E + 1));
+    l.out_src = o; o = al(o + 4 * G);
+    l.parent = o; o = al(o + 4 * G);
+    l.comp_nd = o; o = al(o + 4 * G);
+    l.comp_ns = o; o = al(o + 4 * G);
+    l.comp_off = o; o = al(o + 4 * G);
+    l.comp_soff = o; o = al(o + 4 * G);
+    l.roots = o; o = al(o + 4 * G);
+    l.pathD = o; o = al(o + 4 * G);
+    l.pathS = o; o = al(o + 4 * Smax);
+    l.srcLocal = o; o = al(o + 4 * Smax);
+    l.srcUsed = o; o = al(o + Smax);
+    l.vis_d = o; o = al(o + 4 * G);
+    l.vis_s = o; o = al(o + 4 * Smax);
+    l.stack = o; o = al(o + 8 * (G + Smax));
+    l.r2a = o; o = al(o + 4 * G);
+    l.r2b = o; o = al(o + 4 * G);
+    l.r2c = o; o = al(o + 4 * G);
+    l.r2used = o; o = al(o + Smax);
+    l.tmp = o; o = al(o + 4 * (G + Smax));
+    l.total = o;
+    return l;
+}
+
+size_t link_scratch_bytes(int32_t max_group, int64_t max_edges, int64_t npoints_video, int32_t memory) {
+    return make_lay(max_group, max_edges, npoints_video, memory).total;
+}
+
+// union-find over the destinations of one frame; roots are minimal indices
+__device__ __forceinline__ int uf_find(volatile int* parent, int x) {
+    while (true) {
+        int p = parent[x];
+        if (p == x) return x;
+        int gp = parent[p];
+        if (gp != p) parent[x] = gp;
+        x = p;
+    }
+}
+__device__ __forceinline__ void uf_union(volatile int* parent, int a, int b) {
+    while (true) {
+        a = uf_find(parent, a);
+        b = uf_find(parent, b);
+        if (a == b) return;
+        if (a > b) { int t = a; a = b; b = t; }
+        int old = atomicCAS((int*)&parent[b], b, a);
+        if (old == b) return;
+    }
+}
+
+__global__ void __launch_bounds__(kLinkThreads)
+link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
+    __shared__ int wsum[33];
+    __shared__ long long sh_counter, sh_frame, sh_load;
+    __shared__ int sh_prevg, sh_head, sh_nroots, sh_ringtot;
+    const int v = blockIdx.x;
+    const int gb = in.vgrp[v], ge = in.vgrp[v + 1];
+    const int64_t P0 = in.goff[gb];
+    const int64_t NP = in.goff[ge] - P0;
+    const int M = in.memory, K = M + 1;
+    const int G = S.max_group;
+    const Lay lay = make_lay(G, S.max_edges, NP, M);
+    uint8_t* base = S.base + (size_t)v * S.bytes_per_video;
+    int64_t* start = (int64_t*)(base + lay.start);
+    int32_t* idstamp = (int32_t*)(base + lay.idstamp);
+    unsigned long long* firstpos = (unsigned long long*)(base + lay.firstpos);
+    int32_t* srcidx = (int32_t*)(base + lay.srcidx);
+    int32_t* srcstamp = (int32_t*)(base + lay.srcstamp);
+    int32_t* src_pt = (int32_t*)(base + lay.src_pt);
+    int32_t* ring_pt = (int32_t*)(base + lay.ring_pt);
+    int32_t* ring_n = (int32_t*)(base + lay.ring_n);
+    int32_t* ringpre = (int32_t*)(base + lay.ringpre);
+    int32_t* d_off = (int32_t*)(base + lay.d_off);
+    int32_t* e_src = (int32_t*)(base + lay.e_src);
+    float* e_dist = (float*)(base + lay.e_dist);
+    int32_t* out_src = (int32_t*)(base + lay.out_src);
+    volatile int* parent = (volatile int*)(base + lay.parent);
+    int32_t* comp_nd = (int32_t*)(base + lay.comp_nd);
+    int32_t* comp_ns = (int32_t*)(base + lay.comp_ns);
+    int32_t* comp_off = (int32_t*)(base + lay.comp_off);
+    int32_t* comp_soff = (int32_t*)(base + lay.comp_soff);
+    int32_t* roots = (int32_t*)(base + lay.roots);
+    int32_t* pathD = (int32_t*)(base + lay.pathD);
+    int32_t* pathS = (int32_t*)(base + lay.pathS);
+    int32_t* srcLocal = (int32_t*)(base + lay.srcLocal);
+    uint8_t* srcUsed = base + lay.srcUsed;
+    int32_t* vis_d = (int32_t*)(base + lay.vis_d);
+    int32_t* vis_s = (int32_t*)(base + lay.vis_s);
+    int2* stack = (int2*)(base + lay.stack);
+    int32_t* r2opt = (int32_t*)(base + lay.r2a);
+    int32_t* r2cho = (int32_t*)(base + lay.r2b);
+    int32_t* r2best = (int32_t*)(base + lay.r2c);
+    uint8_t* r2used = base + lay.r2used;
+    int32_t* tmp = (int32_t*)(base + lay.tmp);
+    int64_t* dur = out.dur + P0;
+    int64_t* ids = out.ids;
+    const int Smax = G * K;
+    const float R = in.radius;
+    const float R2 = __fmul_rn(R, R);
+    const int tid = threadIdx.x, nth = blockDim.x;
+
+    for (int64_t i = tid; i < NP; i += nth) {
+        idstamp[i] = -1;
+        srcstamp[i] = -1;
+        firstpos[i] = 0ull;
+    }
+    for (int i = tid; i < Smax; i += nth) vis_s[i] = -1;
+    for (int i = tid; i < G; i += nth) vis_d[i] = -1;
+    for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
+    if (tid == 0) {
+        sh_counter = 0;
+        sh_frame = 0;
+        sh_prevg = -1;
+        sh_head = 0;
+    }
+    __syncthreads();
+
+    for (int g = gb; g < ge; g++) {
+        const int step = g - gb;
+        if (in.reset[g]) {
+            // Linker::reset (src/linking.rs:401-403, src/execute_gpu.rs:792-798)
+            if (tid == 0) {
+                sh_counter = 0;
+                sh_frame = 0;
+                sh_prevg = -1;
+                sh_head = 0;
+            }
+            for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
+            __syncthreads();
+        }
+        const int64_t a = in.goff[g];
+        const int D = (int)(in.goff[g + 1] - a);
+        const int prevg = sh_prevg;
+        const int S0 = (prevg == g - 1 && prevg >= gb) ? (int)(in.goff[g] - in.goff[g - 1]) : 0;
+        const int64_t pa = (S0 > 0) ? in.goff[g - 1] : 0;
+        // ---- P1: sources = previous frame + memory entries not already present
+        for (int i = tid; i < S0; i += nth) {
+            int64_t pt = pa + i;
+            int64_t id = ids[pt];
+            idstamp[id] = step;
+            src_pt[i] = (int32_t)(pt - P0);
+            srcidx[pt - P0] = i;
+            srcstamp[pt - P0] = step;
+        }
+        if (tid == 0) {
+            int tot = 0;
+            for (int q = 0; q < M; q++) {
+                ringpre[q] = tot;
+                tot += ring_n[(sh_head + q) % M];
+            }
+            ringpre[M] = tot;
+            sh_ringtot = tot;
+        }
+        __syncthreads();
+        const int RT = (M > 0) ? sh_ringtot : 0;
+        // ring entries in ring order: position r -> (slot q, entry e)
+        for (int r = tid; r < RT; r += nth) {
+            int q = 0;
+            while (ringpre[q + 1] <= r) q++;
+            int slot = (sh_head + q) % M;
+            int32_t lp = ring_pt[slot * G + (r - ringpre[q])];
+            int64_t id = ids[P0 + lp];
+            if (idstamp[id] != step)
+                atomicMax(&firstpos[id], ((unsigned long long)(uint32_t)step << 32) | (0xFFFFFFFFull - (uint32_t)r));
+        }
+        __syncthreads();
+        int kept_tot = 0;
+        for (int base0 = 0; base0 < RT; base0 += nth) {
+            int r = base0 + tid;
+            int keep = 0;
+            int32_t lp = 0;
+            if (r < RT) {
+                int q = 0;
+                while (ringpre[q + 1] <= r) q++;
+                int slot = (sh_head + q) % M;
+                lp = ring_pt[slot * G + (r - ringpre[q])];
+                int64_t id = ids[P0 + lp];
+                keep = (idstamp[id] != step) &&
+                       firstpos[id] == (((unsigned long long)(uint32_t)step << 32) | (0xFFFFFFFFull - (uint32_t)r));
+            }
+            int tot;
+            int pos = block_excl_scan(keep, &tot, wsum);
+            if (keep) {
+                int si = S0 + kept_tot + pos;
+                src_pt[si] = lp;
+                srcidx[lp] = si;
+                srcstamp[lp] = step;
+            }
+            kept_tot += tot;
+        }
+        const int Sn = S0 + kept_tot;
+        __syncthreads();
+        // ---- P2: destination -> source lists (ascending source index)
+        int etot = 0;
+        for (int base0 = 0; base0 < D; base0 += nth) {
+            int j = base0 + tid;
+            int deg = 0;
+            if (j < D) {
+                int64_t pt = a + j;
+                if (S0 > 0) deg += (int)(L.b_off[pt * K + 1] - L.b_off[pt * K + 0]);
+                for (int k = K; k >= 2; k--) {
+                    int t = g - k;
+                    if (t < gb) continue;
+                    int64_t o0 = L.b_off[pt * K + (k - 1)], o1 = L.b_off[pt * K + k];
+                    int64_t ta = in.goff[t] - P0;
+                    for (int64_t e = o0; e < o1; e++)
+                        if (srcstamp[ta + L.b_pts[e]] == step) deg++;
+                }
+            }
+            int tot;
+            int pos = block_excl_scan(deg, &tot, wsum);
+            if (j < D) d_off[j] = etot + pos;
+            etot += tot;
+        }
+        if (tid == 0) d_off[D] = etot;
+        __syncthreads();
+        if (etot > S.max_edges) {
+            if (tid == 0) atomicOr(out.flags + v, kFlagScratch);
+            break;
+        }
+        for (int j = tid; j < D; j += nth) {
+            int64_t pt = a + j;
+            int w = d_off[j];
+            if (S0 > 0) {
+                int64_t o0 = L.b_off[pt * K + 0], o1 = L.b_off[pt * K + 1];
+                for (int64_t e = o0; e < o1; e++) {
+                    e_src[w] = L.b_pts[e];  // index within group g-1 == source index
+                    e_dist[w] = L.b_dist[e];
+                    w++;
+                }
+            }
+            for (int k = K; k >= 2; k--) {
+                int t = g - k;
+                if (t < gb) continue;
+                int64_t o0 = L.b_off[pt * K + (k - 1)], o1 = L.b_off[pt * K + k];
+                int64_t ta = in.goff[t] - P0;
+                for (int64_t e = o0; e < o1; e++) {
+                    int64_t lp = ta + L.b_pts[e];
+                    if (srcstamp[lp] == step) {
+                        e_src[w] = srcidx[lp];
+                        e_dist[w] = L.b_dist[e];
+                        w++;
+                    }
+                }
+            }
+            parent[j] = j;
+            out_src[j] = -2;
+        }
+        for (int s = tid; s < Sn; s += nth) {
+            srcUsed[s] = 0;
+        }
+        __syncthreads();
+        // ---- P3: trivial links and subnets (connected components)
+        // forward list of source s toward this frame
+        auto fwd = [&](int s, int64_t* f0, int64_t* f1) {
+            int64_t lp = src_pt[s];
+            int64_t pt = P0 + lp;
+            int k = g - in.pgroup[pt];
+            *f0 = L.f_off[pt * K + (k - 1)];
+            *f1 = L.f_off[pt * K + k];
+        };
+        for (int j = tid; j < D; j += nth) {
+            int deg = d_off[j + 1] - d_off[j];
+            if (deg == 0) {
+                out_src[j] = -1;
+            } else if (deg == 1) {
+                int s = e_src[d_off[j]];
+                int64_t f0, f1;
+                fwd(s, &f0, &f1);
+                if (f1 - f0 == 1) out_src[j] = s;
+            }
+        }
+        for (int s = tid; s < Sn; s += nth) {
+            int64_t f0, f1;
+            fwd(s, &f0, &f1);
+            if (f1 - f0 >= 2) {
+                int j0 = L.f_pts[f0];
+                for (int64_t e = f0 + 1; e < f1; e++) uf_union(parent, j0, L.f_pts[e]);
+            }
+        }
+        __syncthreads();
+        for (int j = tid; j < D; j += nth) {
+            int r = uf_find(parent, j);
+            tmp[j] = r;
+            comp_nd[j] = 0;
+            comp_ns[j] = 0;
+        }
+        __syncthreads();
+        for (int j = tid; j < D; j += nth)
+            if (out_src[j] == -2) atomicAdd(&comp_nd[tmp[j]], 1);
+        for (int s = tid; s < Sn; s += nth) {
+            int64_t f0, f1;
+            fwd(s, &f0, &f1);
+            if (f1 > f0) {
+                int j0 = L.f_pts[f0];
+                if (out_src[j0] == -2) atomicAdd(&comp_ns[tmp[j0]], 1);
+            }
+        }
+        __syncthreads();
+        {
+            int nr = 0, offd = 0, offs = 0;
+            for (int base0 = 0; base0 < D; base0 += nth) {
+                int j = base0 + tid;
+                int isroot = (j < D && out_src[j] == -2 && tmp[j] == j) ? 1 : 0;
+                int nd = isroot ? comp_nd[j] : 0;
+                int ns = isroot ? comp_ns[j] : 0;
+                int t1, t2, t3;
+                int p1 = block_excl_scan(isroot, &t1, wsum);
+                int p2 = block_excl_scan(nd, &t2, wsum);
+                int p3 = block_excl_scan(ns, &t3, wsum);
+                if (isroot) {
+                    roots[nr + p1] = j;
+                    comp_off[j] = offd + p2;
+                    comp_soff[j] = offs + p3;
+                }
+                nr += t1;
+                offd += t2;
+                offs += t3;
+            }
+            if (tid == 0) {
+                sh_nroots = nr;
+                sh_load = 0;
+            }
+        }
+        __syncthreads();
+        const int nroots = sh_nroots;
+        // ---- P4: the reference's DFS order per subnet (recurse, linking.rs:595-621)
+        for (int q = tid; q < nroots; q += nth) {
+            const int r = roots[q];
+            const int od = comp_off[r], os = comp_soff[r];
+            int2* stk = stack + od + os;
+            int nd = 0, ns = 0, sp = 0;
+            vis_d[r] = step;
+            pathD[od + nd++] = r;
+            stk[sp++] = make_int2(r, 0);  // (node, next edge); dests tagged by >= 0 side bit below
+            // side encoding: dest nodes stored as node, sources as -(node+1)
+            while (sp > 0) {
+                int2& top = stk[sp - 1];
+                if (top.x >= 0) {  // destination: its sources in list order
+                    const int j = top.x;
+                    const int e0 = d_off[j], e1 = d_off[j + 1];
+                    bool pushed = false;
+                    while (e0 + top.y < e1) {
+                        int s = e_src[e0 + top.y];
+                        top.y++;
+                        if (vis_s[s] != step) {
+                            vis_s[s] = step;
+                            srcLocal[s] = ns;
+                            pathS[os + ns++] = s;
+                            stk[sp++] = make_int2(-(s + 1), 0);
+                            pushed = true;
+                            break;
+                        }
+                    }
+                    if (!pushed) sp--;
+                } else {  // source: its destinations in list order
+                    const int s = -top.x - 1;
+                    int64_t f0, f1;
+                    fwd(s, &f0, &f1);
+                    bool pushed = false;
+                    while (f0 + top.y < f1) {
+                        int j = L.f_pts[f0 + top.y];
+                        top.y++;
+                        if (vis_d[j] != step) {
+                            vis_d[j] = step;
+                            pathD[od + nd++] = j;
+                            stk[sp++] = make_int2(j, 0);
+                            pushed = true;
+                            break;
+                        }
+                    }
+                    if (!pushed) sp--;
+                }
+            }
+            if (nd > 1) atomicAdd((unsigned long long*)&sh_load, (unsigned long long)((long long)nd * ns));
+        }
+        __syncthreads();
+        if (sh_load > 5000) {
+            // TooDenseToLink (src/linking.rs:677-682)
+            if (tid == 0) atomicOr(out.flags + v, kFlagTooDense);
+            break;
+        }
+        // ---- P5: branch and bound per subnet (recurse2, linking.rs:687-766)
+        for (int q = tid; q < nroots; q += nth) {
+            const int r = roots[q];
+            const int od = comp_off[r], os = comp_soff[r];
+            const int nd = comp_nd[r], ns = comp_ns[r];
+            int* opt = r2opt + od;
+            int* cho = r2cho + od;
+            int* bst = r2best + od;
+            uint8_t* used = r2used + os;
+            for (int i = 0; i < ns; i++) used[i] = 0;
+            float score = 0.0f, best = INFINITY;
+            bool has_best = false;
+            long long budget = 0;
+            int level = 0;
+            opt[0] = 0;
+            bool over = false;
+            while (true) {
+                if (++budget > kSubnetBudget) { over = true; break; }
+                const int j = pathD[od + level];
+                const int e0 = d_off[j];
+                const int deg = d_off[j + 1] - e0;
+                const int o = opt[level];
+                bool ascend = false;
+                if (o > deg) {
+                    ascend = true;
+                } else if (score > best) {
+                    ascend = true;
+                } else {
+                    const bool is_null = (o == deg);
+                    const float c = is_null ? R2 : e_dist[e0 + o];
+                    score = __fadd_rn(score, c);
+                    int ls = -1;
+                    if (!is_null) {
+                        ls = srcLocal[e_src[e0 + o]];
+                        if (used[ls]) {
+                            score = __fsub_rn(score, c);
+                            opt[level] = o + 1;
+                            continue;
+                        }
+                        used[ls] = 1;
+                    }
+                    cho[level] = ls;
+                    if (level == nd - 1) {
+                        if (score < best) {
+                            best = score;
+                            has_best = true;
+                            for (int l = 0; l < nd; l++) bst[l] = cho[l];
+                        }
+                        if (!is_null) used[ls] = 0;
+                        score = __fsub_rn(score, c);
+                        opt[level] = o + 1;
+                    } else {
+                        level++;
+                        opt[level] = 0;
+                    }
+                    continue;
+                }
+                if (ascend) {
+                    level--;
+                    if (level < 0) break;
+                    const int jp = pathD[od + level];
+                    const int ep = d_off[jp];
+                    const int degp = d_off[jp + 1] - ep;
+                    const int op = opt[level];
+                    const bool nullp = (op == degp);
+                    const float cp = nullp ? R2 : e_dist[ep + op];
+                    if (!nullp) used[cho[level]] = 0;
+                    score = __fsub_rn(score, cp);
+                    opt[level] = op + 1;
+                }
+            }
+            if (over) atomicOr(out.flags + v, kFlagSubnetBudget);
+            for (int l = 0; l < nd; l++) {
+                int ch = has_best ? bst[l] : -1;
+                out_src[pathD[od + l]] = (ch >= 0) ? pathS[os + ch] : -1;
+            }
+        }
+        __syncthreads();
+        if (out.flags[v] & kFlagSubnetBudget) break;
+        // ---- P6: ids (new ones in destination order, src/linking.rs:788-798)
+        {
+            int newtot = 0;
+            const long long counter = sh_counter;
+            const long long frame = sh_frame;
+            for (int base0 = 0; base0 < D; base0 += nth) {
+                int j = base0 + tid;
+                int isnew = (j < D && out_src[j] < 0) ? 1 : 0;
+                int tot;
+                int pos = block_excl_scan(isnew, &tot, wsum);
+                if (j < D) {
+                    int64_t pt = a + j;
+                    if (isnew) {
+                        long long id = counter + newtot + pos;
+                        ids[pt] = id;
+                        start[id] = frame;
+                    } else {
+                        int s = out_src[j];
+                        ids[pt] = ids[P0 + src_pt[s]];
+                        srcUsed[s] = 1;
+                    }
+                }
+                newtot += tot;
+            }
+            __syncthreads();
+            if (tid == 0) sh_counter = counter + newtot;
+        }
+        // ---- P7: memory ring and durations (src/linking.rs:481-503)
+        {
+            const long long frame = sh_frame;
+            if (M > 0) {
+                const int hs = sh_head;
+                const int nleave = ring_n[hs];
+                for (int e = tid; e < nleave; e += nth) {
+                    int64_t id = ids[P0 + ring_pt[hs * G + e]];
+                    dur[id] = (frame - start[id]) - M;
+                }
+                __syncthreads();
+                int ut = 0;
+                for (int base0 = 0; base0 < S0; base0 += nth) {
+                    int s = base0 + tid;
+                    int un = (s < S0 && !srcUsed[s]) ? 1 : 0;
+                    int tot;
+                    int pos = block_excl_scan(un, &tot, wsum);
+                    if (un) ring_pt[hs * G + ut + pos] = src_pt[s];
+                    ut += tot;
+                }
+                if (tid == 0) {
+                    ring_n[hs] = ut;
+                    sh_head = (hs + 1) % M;
+                }
+            } else {
+                for (int s = tid; s < S0; s += nth) {
+                    if (!srcUsed[s]) {
+                        int64_t id = ids[P0 + src_pt[s]];
+                        dur[id] = frame - start[id];
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                sh_prevg = g;
+                sh_frame = frame + 1;
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    // ---- Linker::finish (src/linking.rs:505-520)
+    if (!(out.flags[v] & (kFlagTooDense | kFlagSubnetBudget | kFlagScratch))) {
+        const long long frame = sh_frame;
+        if (M > 0) {
+            for (int q = 0; q < M; q++) {
+                int slot = (sh_head + q) % M;
+                int n = ring_n[slot];
+                for (int e = tid; e < n; e += nth) {
+                    int64_t id = ids[P0 + ring_pt[slot * G + e]];
+                    dur[id] = (frame - start[id]) - (M - q);
+                }
+                __syncthreads();
+            }
+        }
+        if (sh_prevg >= gb) {
+            const int pg = sh_prevg;
+            for (int64_t p = in.goff[pg] + tid; p < in.goff[pg + 1]; p += nth) {
+                int64_t id = ids[p];
+                dur[id] = frame - start[id];
+            }
+        }
+    }
+    if (tid == 0) out.counter[v] = sh_counter;
+}
+
+// Per-row durations through the reference's f32 round trip of the particle
+// id (src/execute_gpu.rs:812-815, 1165-1181).
+__global__ void durations_kernel(LinkInput in, LinkOutput out, int64_t* row_dur) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= in.npoints) return;
+    const int h = in.pgroup[p];
+    int x = 0, y = in.nvideos;
+    while (y - x > 1) {
+        int m = (x + y) >> 1;
+        if (in.vgrp[m] <= h) x = m; else y = m;
+    }
+    const int v = x;
+    const int64_t P0 = in.goff[in.vgrp[v]];
+    const int64_t id = (int64_t)(float)out.ids[p];
+    if (id >= out.counter[v]) {
+        atomicOr(out.flags + v, kFlagScratch);
+        row_dur[p] = -1;
+        return;
+    }
+    row_dur[p] = out.dur[P0 + id];
+}
+
+// --------------------------------------------------------------- launchers
+cudaError_t link_sort_groups(const LinkInput& in, uint32_t* srt, uint8_t* scratch, size_t scratch_per_group,
+                             int max_group, cudaStream_t st) {
+    (void)max_group;
+    if (in.ngroups == 0) return cudaSuccess;
+    sort_groups_kernel<<<in.ngroups, kLinkThreads, 0, st>>>(in, srt, (uint64_t*)scratch, scratch_per_group / 8);
+    return cudaGetLastError();
+}
+
+cudaError_t link_count_lists(const LinkInput& in, const uint32_t* srt, int64_t* f_cnt, int64_t* b_cnt,
+                             cudaStream_t st) {
+    if (in.npoints == 0) return cudaSuccess;
+    LinkLists L = {};
+    L.srt = (uint32_t*)srt;
+    lists_kernel<0><<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, L, f_cnt, b_cnt);
+    return cudaGetLastError();
+}
+
+cudaError_t link_fill_lists(const LinkInput& in, const LinkLists& L, cudaStream_t st) {
+    if (in.npoints == 0) return cudaSuccess;
+    lists_kernel<1><<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, L, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t link_run(const LinkInput& in, const LinkLists& L, const LinkScratch& S, const LinkOutput& out,
+                     cudaStream_t st) {
+    if (in.nvideos == 0) return cudaSuccess;
+    link_video_kernel<<<in.nvideos, kLinkThreads, 0, st>>>(in, L, S, out);
+    return cudaGetLastError();
+}
+
+cudaError_t link_durations(const LinkInput& in, const LinkOutput& out, int64_t* row_dur, cudaStream_t st) {
+    if (in.npoints == 0) return cudaSuccess;
+    durations_kernel<<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, out, row_dur);
+    return cudaGetLastError();
+}
+
+}  // namespace gt

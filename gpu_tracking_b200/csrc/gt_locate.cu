@@ -1,0 +1,812 @@
+// gt_locate.cu — Crocker–Grier locate kernels for sm_100a.
+//
+//   bandpass_kernel   preprocess_rows.wgsl + preprocess_cols.wgsl (+ max_rows.wgsl
+//                     and extract_max.wgsl when kCand): one CTA per 32x64 tile of
+//                     one frame; the raw tile with its halo, the row-pass result
+//                     and the processed tile live in shared memory, only the
+//                     processed interior and the candidate pixels reach HBM.
+//   walk_kernel       walk.wgsl + characterize.wgsl, one thread per candidate.
+//   finalize_kernel   canonical order, filter_close_trackpy / prune_blobs_log and
+//                     the doughnut correction (src/execute_gpu.rs:556-790), one CTA
+//                     per frame.
+//   scatter_kernel    per-frame results into the output table columns.
+#include <math.h>
+
+#include "gt_internal.cuh"
+#include "gt_kernels.h"
+
+namespace gt {
+
+// ------------------------------------------------------------------ bandpass
+template <typename T, bool kCand>
+__global__ void __launch_bounds__(kLocateThreads)
+bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restrict__ processed,
+                const LocateConsts c, uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys,
+                uint32_t cand_cap, uint32_t* __restrict__ flags) {
+    extern __shared__ float smem[];
+    const int H = c.H, W = c.W, R = c.R;
+    const int kd = kCand ? c.kd : 1;
+    const int o = kCand ? c.o : 0;
+    constexpr int TH = kLocateTH, TW = kLocateTW;
+    const int r0 = blockIdx.y * TH, c0 = blockIdx.x * TW;
+    const int f = blockIdx.z;
+    const T* img = frames + (size_t)f * frame_stride;
+    float* proc = processed + (size_t)f * H * W;
+
+    const int PH = TH + kd - 1, PW = TW + kd - 1;
+    const int pr0 = r0 - o, pc0 = c0 - o;
+    const int XH = PH + 2 * R, RW = PW + 2 * R;
+    const int xr0 = pr0 - R, rc0 = pc0 - R;
+    float* sraw = smem;
+    float* sxg = sraw + XH * RW;
+    float* sxb = sxg + XH * PW;
+    float* sp = sxb + XH * PW;
+    float* sv = sp + PH * PW;
+    const int tid = threadIdx.x;
+
+    // raw tile with clamp-to-edge addressing (the boxcar's addressing)
+    for (int idx = tid; idx < XH * RW; idx += blockDim.x) {
+        int rr = idx / RW, cc = idx - rr * RW;
+        int gr = min(max(xr0 + rr, 0), H - 1);
+        int gc = min(max(rc0 + cc, 0), W - 1);
+        sraw[idx] = load_px<T>(img, (size_t)gr * W + gc);
+    }
+    __syncthreads();
+
+    // preprocess_rows.wgsl:30-54 — Gaussian taps skip out-of-frame columns,
+    // the boxcar sums clamped columns; temp = (g / gauss_norm, box)
+    for (int idx = tid; idx < XH * PW; idx += blockDim.x) {
+        int rr = idx / PW, cc = idx - rr * PW;
+        const float* rowp = sraw + rr * RW + cc;
+        const int gcol = pc0 + cc;
+        float gs = 0.0f, cs = 0.0f;
+        for (int i = 0; i <= 2 * R; i++) {
+            float x = rowp[i];
+            int gc = gcol + i - R;
+            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
+            cs = __fadd_rn(cs, x);
+        }
+        sxg[idx] = __fdiv_rn(gs, c.gnorm);
+        sxb[idx] = cs;
+    }
+    __syncthreads();
+
+    // preprocess_cols.wgsl:29-59
+    const float trunc_thr = 1.0f / 255.0f;
+    for (int idx = tid; idx < PH * PW; idx += blockDim.x) {
+        int pr = idx / PW, pc = idx - pr * PW;
+        int grow = pr0 + pr, gcol = pc0 + pc;
+        if (grow < 0 || grow >= H || gcol < 0 || gcol >= W) {
+            sp[idx] = -INFINITY;  // outside the frame: never part of a dilation window
+            continue;
+        }
+        float gs = 0.0f, cs = 0.0f;
+        for (int i = 0; i <= 2 * R; i++) {
+            int gr = grow + i - R;
+            int xrow = min(max(gr, 0), H - 1) - xr0;
+            float xg = sxg[xrow * PW + pc];
+            float xb = sxb[xrow * PW + pc];
+            if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], xg, gs);
+            cs = __fadd_rn(cs, xb);
+        }
+        float res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
+        if (c.truncate && res < trunc_thr) res = 0.0f;
+        sp[idx] = res;
+    }
+    __syncthreads();
+
+    // processed interior to HBM (the walk reads it back)
+    for (int idx = tid; idx < TH * TW; idx += blockDim.x) {
+        int r = idx / TW, cc = idx - r * TW;
+        int gr = r0 + r, gc = c0 + cc;
+        if (gr < H && gc < W) proc[(size_t)gr * W + gc] = sp[(r + o) * PW + cc + o];
+    }
+    if (!kCand) return;
+
+    // max_rows.wgsl + extract_max.wgsl: the pixel is a candidate iff no value in
+    // its kd x kd window (out-of-frame cells skipped) exceeds it
+    for (int idx = tid; idx < TH * PW; idx += blockDim.x) {
+        int r = idx / PW, cc = idx - r * PW;
+        float m = -INFINITY;
+        for (int j = 0; j < kd; j++) m = fmaxf(m, sp[(r + j) * PW + cc]);
+        sv[idx] = m;
+    }
+    __syncthreads();
+
+    constexpr int PER = (TH * TW) / kLocateThreads;  // 8 consecutive pixels per thread
+    uint32_t mask = 0;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        int idx = tid * PER + k;
+        int r = idx / TW, cc = idx - r * TW;
+        int gr = r0 + r, gc = c0 + cc;
+        if (gr >= H || gc >= W) continue;
+        if (gr < c.margin || gr >= H - c.margin || gc < c.margin || gc >= W - c.margin) continue;
+        float center = sp[(r + o) * PW + cc + o];
+        if (center < c.thr) continue;
+        float m = -INFINITY;
+        for (int j = 0; j < kd; j++) m = fmaxf(m, sv[r * PW + cc + j]);
+        if (m > center) continue;
+        mask |= 1u << k;
+        cnt++;
+    }
+    // block exclusive scan of the per-thread counts (row-major tile order)
+    __shared__ int warp_tot[kLocateThreads / 32];
+    __shared__ uint32_t s_base;
+    const int lane = tid & 31, wid = tid >> 5;
+    int incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int v = (lane < kLocateThreads / 32) ? warp_tot[lane] : 0;
+        int s = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, s, d);
+            if (lane >= d) s += t;
+        }
+        if (lane < kLocateThreads / 32) warp_tot[lane] = s - v;  // exclusive
+        if (lane == kLocateThreads / 32 - 1) {
+            s_base = s > 0 ? atomicAdd(cand_count + f, (uint32_t)s) : 0u;
+        }
+    }
+    __syncthreads();
+    uint32_t pos = s_base + warp_tot[wid] + (incl - cnt);
+    uint32_t* out = cand_keys + (size_t)f * cand_cap;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        if (!(mask & (1u << k))) continue;
+        int idx = tid * PER + k;
+        int r = idx / TW, cc = idx - r * TW;
+        if (pos < cand_cap) out[pos] = (uint32_t)((r0 + r) * W + (c0 + cc));
+        else atomicOr(flags, kFlagCandOverflow);
+        pos++;
+    }
+}
+
+// ---------------------------------------------------------------------- walk
+struct WalkRes {
+    float x, y, mass, max, count;
+};
+
+// walk.wgsl:67-102 get_center
+__device__ __forceinline__ WalkRes get_center(const float* __restrict__ p, int H, int W, int u, int v, int rint,
+                                              float r2) {
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int i = -rint; i <= rint; i++) {
+        float x = (float)i;
+        float x2 = __fmul_rn(x, x);
+        int pu = u + i;
+        for (int j = -rint; j <= rint; j++) {
+            float y = (float)j;
+            float mask = __fadd_rn(x2, __fmul_rn(y, y));
+            if (mask > r2) continue;
+            int pv = v + j;
+            if (pu < 0 || pu >= H || pv < 0 || pv >= W) continue;
+            float data = __ldg(p + (size_t)pu * W + pv);
+            res.x = __fmaf_rn(data, x, res.x);
+            res.y = __fmaf_rn(data, y, res.y);
+            res.mass = __fadd_rn(res.mass, data);
+            res.count = __fadd_rn(res.count, 1.0f);
+            res.max = wgsl_max(res.max, data);
+        }
+    }
+    res.x = __fdiv_rn(res.x, res.mass);
+    res.y = __fdiv_rn(res.y, res.mass);
+    return res;
+}
+
+// walk.wgsl:104-169
+__device__ __forceinline__ WalkRes walk_one(const float* __restrict__ p, const LocateConsts& c, int u0, int v0,
+                                            float r) {
+    int pu = u0, pv = v0;
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    int rint;
+    float r2;
+    if (r <= 0.0f) {
+        rint = (c.circle - 1) / 2;
+        float rr = (float)rint;
+        r2 = __fmul_rn(rr, rr);
+    } else {
+        rint = (int)ceilf(r);
+        r2 = __fmul_rn(r, r);
+    }
+    const int margin = rint;
+    const float thr = c.shift_thr;
+    for (uint32_t it = 0; it < c.max_iter; it++) {
+        res = get_center(p, c.H, c.W, pu, pv, rint, r2);
+        bool changed = false;
+        if ((res.x > thr) && (pu < c.H - 1 - margin)) { pu += 1; changed = true; }
+        else if (res.x < -thr && pu > margin) { pu -= 1; changed = true; }
+        if ((res.y > thr) && (pv < c.W - 1 - margin)) { pv += 1; changed = true; }
+        else if ((res.y < -thr) && (pv > margin)) { pv -= 1; changed = true; }
+        if (!changed) break;
+    }
+    res.x = __fadd_rn(res.x, (float)pu);
+    res.y = __fadd_rn(res.y, (float)pv);
+    return res;
+}
+
+// characterize.wgsl:61-143; angle table holds (sin 2θ, cos 2θ) for the
+// (2 rint + 1)^2 integer offsets of the circle.
+template <typename T>
+__device__ __forceinline__ void characterize_one(const float* __restrict__ p, const T* __restrict__ raw,
+                                                 const LocateConsts& c, Feature& ft, bool char_points,
+                                                 const float2* __restrict__ angle_tab,
+                                                 const int32_t* __restrict__ angle_off) {
+    float r = ft.r;
+    int rint;
+    if (r <= 0.0f) {
+        rint = (c.circle - 1) / 2;
+        r = (float)rint;
+    } else {
+        rint = (int)ceilf(r);
+    }
+    const float r2 = __fmul_rn(r, r);
+    const float2* angles = angle_tab + angle_off[rint];
+    const int u = sat_f2i(rintf(ft.x));
+    const int v = sat_f2i(rintf(ft.y));
+    const int H = c.H, W = c.W;
+    if (char_points) {
+        float mass = 0.0f;
+        for (int i = -rint; i <= rint; i++) {
+            float x = (float)i;
+            float x2 = __fmul_rn(x, x);
+            for (int j = -rint; j <= rint; j++) {
+                float y = (float)j;
+                float mask = __fadd_rn(x2, __fmul_rn(y, y));
+                if (mask > r2) continue;
+                int pu = u + i, pv = v + j;
+                if (pu < 0 || pu >= H || pv < 0 || pv >= W) continue;
+                mass = __fadd_rn(mass, __ldg(p + (size_t)pu * W + pv));
+            }
+        }
+        ft.mass = mass;
+    }
+    const float mass = ft.mass;
+    float middle = 0.0f;
+    const int64_t middle_idx = (int64_t)u * W + v;
+    if (middle_idx >= 0 && middle_idx < (int64_t)H * W) middle = __ldg(p + middle_idx);
+    float Rg = 0.0f, raw_mass = 0.0f, signal = 0.0f, es = 0.0f, ec = 0.0f;
+    const int side = 2 * rint + 1;
+    for (int i = -rint; i <= rint; i++) {
+        float x = (float)i;
+        float x2 = __fmul_rn(x, x);
+        int pu = u + i;
+        for (int j = -rint; j <= rint; j++) {
+            float y = (float)j;
+            float mask = __fadd_rn(x2, __fmul_rn(y, y));
+            if (mask > r2) continue;
+            int pv = v + j;
+            if (pu < 0 || pu >= H || pv < 0 || pv >= W) continue;
+            size_t idx = (size_t)pu * W + pv;
+            float data = __ldg(p + idx);
+            Rg = __fmaf_rn(data, mask, Rg);
+            raw_mass = __fadd_rn(raw_mass, load_px<T>(raw, idx));
+            signal = wgsl_max(signal, data);
+            if ((i != 0) | (j != 0)) {
+                float2 sc = __ldg(angles + (i + rint) * side + (j + rint));
+                es = __fmaf_rn(data, sc.x, es);
+                ec = __fmaf_rn(data, sc.y, ec);
+            } else {
+                ec = __fadd_rn(ec, data);
+            }
+        }
+    }
+    es = __fmul_rn(es, es);
+    ec = __fmul_rn(ec, ec);
+    ft.ecc = __fdiv_rn(__fsqrt_rn(__fadd_rn(es, ec)), __fsub_rn(mass, middle));
+    ft.Rg = __fsqrt_rn(__fdiv_rn(Rg, mass));
+    ft.raw = raw_mass;
+    ft.signal = signal;
+}
+
+// walk.wgsl:171-229 + characterize over kept rows.  cand_r < 0 selects the
+// trackpy circle; LoG passes the candidate's radius (per-radius candidates).
+template <typename T>
+__global__ void __launch_bounds__(128)
+walk_kernel(const float* __restrict__ processed, const T* __restrict__ frames, int64_t frame_stride,
+            const LocateConsts c, const uint32_t* __restrict__ cand_count, const uint32_t* __restrict__ cand_keys,
+            uint32_t cand_cap, const float* __restrict__ radii, const int32_t* __restrict__ angle_off,
+            const float2* __restrict__ angles, Feature* __restrict__ feats, uint32_t* __restrict__ feat_count,
+            uint32_t feat_cap, uint32_t* __restrict__ flags, int32_t n_radius_slots) {
+    const int f = blockIdx.y;
+    const int slot = blockIdx.z;  // radius index for LoG, 0 for trackpy
+    const int fs = f * n_radius_slots + slot;
+    const uint32_t n = min(cand_count[fs], cand_cap);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t key = cand_keys[(size_t)fs * cand_cap + i];
+    const int u = (int)(key / (uint32_t)c.W), v = (int)(key % (uint32_t)c.W);
+    const float* p = processed + (size_t)f * c.H * c.W;
+    const float r = radii ? radii[slot] : -1.0f;
+    WalkRes res = walk_one(p, c, u, v, r);
+    float minmass;
+    if (c.minmass > 0.0f) minmass = c.minmass;
+    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.image_std), c.rough);
+    if (!(res.mass >= minmass)) return;
+    Feature ft;
+    ft.key_hi = (uint32_t)slot;
+    ft.key_lo = key;
+    ft.x = res.x;
+    ft.y = res.y;
+    ft.mass = res.mass;
+    ft.r = (r > 0.0f) ? r : 0.0f;
+    ft.max_i = res.max;
+    ft.count = res.count;
+    ft.Rg = ft.raw = ft.signal = ft.ecc = 0.0f;
+    ft.d_raw = ft.d_bg = ft.d_corr = __int_as_float(0x7fc00000);
+    ft.ridx = slot;
+    if (c.characterize) {
+        const T* raw = frames + (size_t)f * frame_stride;
+        characterize_one<T>(p, raw, c, ft, false, angles, angle_off);
+    }
+    uint32_t pos = atomicAdd(feat_count + f, 1u);
+    if (pos < feat_cap) feats[(size_t)f * feat_cap + pos] = ft;
+    else atomicOr(flags, kFlagFeatOverflow);
+}
+
+// characterize_points: characterize.wgsl with _feat_characterize_points (mass
+// recomputed at the rounded position); one thread per given point.
+template <typename T>
+__global__ void __launch_bounds__(128)
+characterize_points_kernel(const float* __restrict__ processed, const T* __restrict__ frames, int64_t frame_stride,
+                           const LocateConsts c, const float* __restrict__ pts, const int64_t* __restrict__ grp_off,
+                           const int32_t* __restrict__ grp_frame, const float2* __restrict__ angle_tab,
+                           const int32_t* __restrict__ angle_off, const float* __restrict__ radii_tab,
+                           int32_t n_radii_tab, int32_t has_r, Feature* __restrict__ feats, uint32_t* feat_count,
+                           uint32_t feat_cap, int32_t g0) {
+    const int g = blockIdx.y;  // group within this chunk
+    const int64_t a = grp_off[g0 + g], b = grp_off[g0 + g + 1];
+    const int64_t i = a + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b) return;
+    Feature ft;
+    ft.key_hi = 0;
+    ft.key_lo = (uint32_t)(i - a);
+    ft.x = pts[3 * i + 0];
+    ft.y = pts[3 * i + 1];
+    ft.r = has_r ? pts[3 * i + 2] : 0.0f;
+    ft.mass = 0.0f;
+    ft.max_i = 0.0f;
+    ft.count = 0.0f;
+    ft.d_raw = ft.d_bg = ft.d_corr = __int_as_float(0x7fc00000);
+    ft.ridx = 0;
+    (void)radii_tab;
+    (void)n_radii_tab;
+    const float* p = processed + (size_t)g * c.H * c.W;
+    const T* raw = frames + (size_t)grp_frame[g0 + g] * frame_stride;
+    characterize_one<T>(p, raw, c, ft, true, angle_tab, angle_off);
+    uint32_t pos = (uint32_t)(i - a);
+    if (pos < feat_cap) feats[(size_t)g * feat_cap + pos] = ft;
+    if (threadIdx.x == 0 && blockIdx.x == 0) feat_count[g] = (uint32_t)((b - a) < (int64_t)feat_cap ? (b - a) : (int64_t)feat_cap);
+}
+
+// ------------------------------------------------------------------ finalize
+// disk_overlap / blob_overlap of prune_blobs_log (src/execute_gpu.rs:599-628);
+// Rust arithmetic, separately rounded.  acos is evaluated in double and
+// rounded, the oracle does the same.
+__device__ float make_acos(float d, float r1, float r1s, float r2s) {
+    float num = __fsub_rn(__fadd_rn(__fmul_rn(d, d), r1s), r2s);
+    float den = __fmul_rn(__fmul_rn(2.0f, d), r1);
+    float ratio = __fdiv_rn(num, den);
+    ratio = fminf(fmaxf(ratio, -1.0f), 1.0f);
+    return (float)acos((double)ratio);
+}
+__device__ float disk_overlap(float d, float r1, float r2) {
+    float r1s = __fmul_rn(r1, r1);
+    float r2s = __fmul_rn(r2, r2);
+    float acos1 = make_acos(d, r1, r1s, r2s);
+    float acos2 = make_acos(d, r2, r2s, r1s);
+    float a = __fadd_rn(__fadd_rn(-d, r2), r1);
+    float b = __fadd_rn(__fsub_rn(d, r2), r1);
+    float cc = __fsub_rn(__fadd_rn(d, r2), r1);
+    float dd = __fadd_rn(__fadd_rn(d, r2), r1);
+    float prod = __fmul_rn(__fmul_rn(__fmul_rn(a, b), cc), dd);
+    float area = __fsub_rn(__fadd_rn(__fmul_rn(r1s, acos1), __fmul_rn(r2s, acos2)),
+                           __fmul_rn(0.5f, __fsqrt_rn(fabsf(prod))));
+    const float pi = 3.14159265358979323846f;
+    return __fdiv_rn(area, __fmul_rn(pi, fminf(r1s, r2s)));
+}
+__device__ float blob_overlap(float r1, float r2, float distance) {
+    if (distance > __fadd_rn(r1, r2)) return 0.0f;
+    else if (distance <= fabsf(__fsub_rn(r1, r2))) return 1.0f;
+    else return disk_overlap(distance, r1, r2);
+}
+
+// Upper median (sorted[len/2]) of the valid annulus pixels by a warp-wide
+// radix select on order keys; exact.
+template <typename T>
+__device__ float warp_upper_median(const T* __restrict__ raw, int H, int W, int mu, int mv,
+                                   const short2* __restrict__ inds, int n_inds, uint32_t* hist, int* n_out) {
+    const int lane = threadIdx.x & 31;
+    int nvalid = 0;
+    for (int b = 0; b < n_inds; b += 32) {
+        int k = b + lane;
+        bool ok = false;
+        if (k < n_inds) {
+            short2 d = inds[k];
+            int64_t a = (int64_t)mu + d.x, bb = (int64_t)mv + d.y;
+            ok = (a >= 0 && a < H && bb >= 0 && bb < W);
+        }
+        nvalid += __popc(__ballot_sync(0xffffffffu, ok));
+    }
+    *n_out = nvalid;
+    if (nvalid == 0) return 0.0f;
+    uint32_t want = (uint32_t)(nvalid / 2);
+    uint32_t prefix = 0, pmask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int q = lane; q < 256; q += 32) hist[q] = 0;
+        __syncwarp();
+        for (int b = lane; b < n_inds; b += 32) {
+            short2 d = inds[b];
+            int64_t a = (int64_t)mu + d.x, bb = (int64_t)mv + d.y;
+            if (a >= 0 && a < H && bb >= 0 && bb < W) {
+                uint32_t key = float_order_key(load_px<T>(raw, (size_t)a * W + bb));
+                if ((key & pmask) == prefix) atomicAdd(hist + ((key >> shift) & 255u), 1u);
+            }
+        }
+        __syncwarp();
+        uint32_t local[8];
+        uint32_t s = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            local[q] = hist[lane * 8 + q];
+            s += local[q];
+        }
+        uint32_t incl = s;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        uint32_t excl = incl - s;
+        int found_bin = -1;
+        uint32_t below = 0;
+        if (want >= excl && want < incl) {
+            uint32_t acc = excl;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (found_bin < 0 && want < acc + local[q]) {
+                    found_bin = lane * 8 + q;
+                    below = acc;
+                }
+                acc += local[q];
+            }
+        }
+        unsigned bal = __ballot_sync(0xffffffffu, found_bin >= 0);
+        int src = __ffs(bal) - 1;
+        found_bin = __shfl_sync(0xffffffffu, found_bin, src);
+        below = __shfl_sync(0xffffffffu, below, src);
+        want -= below;
+        prefix |= ((uint32_t)found_bin) << shift;
+        pmask |= 255u << shift;
+        __syncwarp();
+    }
+    return float_from_order_key(prefix);
+}
+
+// Doughnut correction of one feature by one warp (src/execute_gpu.rs:717-790).
+template <typename T>
+__device__ void doughnut_warp(const T* __restrict__ raw, int H, int W, Feature& ft, const short2* __restrict__ sig,
+                              int n_sig, const short2* __restrict__ bg, int n_bg, uint32_t* hist) {
+    const int lane = threadIdx.x & 31;
+    const int mu = sat_f2i(roundf(ft.x));
+    const int mv = sat_f2i(roundf(ft.y));
+    // sequential sum in circle_inds order (Iterator::sum)
+    float sum = 0.0f;
+    int nsig = 0;
+    for (int b = 0; b < n_sig; b += 32) {
+        int k = b + lane;
+        float val = 0.0f;
+        bool ok = false;
+        if (k < n_sig) {
+            short2 d = sig[k];
+            int64_t a = (int64_t)mu + d.x, bb = (int64_t)mv + d.y;
+            ok = (a >= 0 && a < H && bb >= 0 && bb < W);
+            if (ok) val = load_px<T>(raw, (size_t)a * W + bb);
+        }
+        unsigned bal = __ballot_sync(0xffffffffu, ok);
+        nsig += __popc(bal);
+        for (int q = 0; q < 32; q++) {
+            float v = __shfl_sync(0xffffffffu, val, q);
+            if ((bal >> q) & 1u) sum = __fadd_rn(sum, v);
+        }
+    }
+    int nbg;
+    float med = warp_upper_median<T>(raw, H, W, mu, mv, bg, n_bg, hist, &nbg);
+    ft.d_raw = sum;
+    ft.d_bg = med;
+    ft.d_corr = __fsub_rn(sum, __fmul_rn(med, (float)nsig));
+}
+
+// One CTA per frame: canonical order, filter_close / prune_blobs_log, the
+// doughnut correction and compaction of the kept rows in output order.
+template <typename T>
+__global__ void __launch_bounds__(kFinalizeThreads)
+finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ feat_count, uint32_t feat_cap,
+                Feature* __restrict__ out, uint32_t* __restrict__ kept_count, uint8_t* __restrict__ gscratch,
+                const FinalizeConsts fc, const T* __restrict__ frames, int64_t frame_stride,
+                const int32_t* __restrict__ frame_index, const short2* __restrict__ dn_inds,
+                const int4* __restrict__ dn_meta, uint32_t* __restrict__ flags) {
+    extern __shared__ uint64_t fsm[];
+    __shared__ int wsum[33];
+    const int g = blockIdx.x;
+    const int n = (int)min(feat_count[g], feat_cap);
+    const Feature* F = feats + (size_t)g * feat_cap;
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    // working arrays: keys (u64), perm (i32), order (i32), keep (u8)
+    uint64_t* keys;
+    int32_t *perm, *order;
+    uint8_t* keep;
+    uint32_t* hist;
+    const size_t need = (size_t)np2 * (8 + 4 + 4 + 1);
+    if (np2 <= kFinalizeSmemSort) {
+        keys = fsm;
+        perm = (int32_t*)(keys + kFinalizeSmemSort);
+        order = perm + kFinalizeSmemSort;
+        keep = (uint8_t*)(order + kFinalizeSmemSort);
+        hist = (uint32_t*)(keep + kFinalizeSmemSort);
+    } else {
+        if (need > fc.scratch_per_frame) {
+            if (threadIdx.x == 0) atomicOr(flags, kFlagFeatOverflow);
+            if (threadIdx.x == 0) kept_count[g] = 0;
+            return;
+        }
+        uint8_t* base = gscratch + (size_t)g * fc.scratch_per_frame;
+        keys = (uint64_t*)base;
+        perm = (int32_t*)(keys + np2);
+        order = perm + np2;
+        keep = (uint8_t*)(order + np2);
+        uint8_t* sm_after = (uint8_t*)fsm;
+        hist = (uint32_t*)sm_after;
+    }
+    // 1. canonical order: (radius index, candidate pixel index), or input order
+    for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+        if (i < n) {
+            const Feature& ft = F[i];
+            keys[i] = fc.presorted ? (uint64_t)i
+                                   : (((uint64_t)ft.key_hi << 56) | ((uint64_t)ft.key_lo << 24) | (uint64_t)i);
+        } else {
+            keys[i] = ~0ull;
+        }
+    }
+    __syncthreads();
+    if (!fc.presorted) block_sort_u64(keys, np2);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        perm[i] = (int32_t)(keys[i] & 0xFFFFFFull);
+        keep[i] = 1;
+        order[i] = i;
+    }
+    __syncthreads();
+
+    if (!fc.log_style) {
+        // 2a. filter_close_trackpy (src/execute_gpu.rs:556-590) in canonical order
+        if (fc.filter_close) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const Feature& q = F[perm[i]];
+                int lo = 0, hi = n;
+                if (fc.band >= 0) {
+                    // rows of candidates that can hold a neighbour (|x - u| <= reach)
+                    int64_t u = (int64_t)q.key_lo / fc.W;
+                    int64_t ulo = u - fc.band, uhi = u + fc.band + 1;
+                    uint64_t klo = ulo <= 0 ? 0ull : ((uint64_t)(ulo * fc.W) << 24);
+                    uint64_t khi = ((uint64_t)(uhi * fc.W) << 24);
+                    int a = 0, b = n;
+                    while (a < b) { int m = (a + b) >> 1; if (keys[m] < klo) a = m + 1; else b = m; }
+                    lo = a;
+                    a = lo; b = n;
+                    while (a < b) { int m = (a + b) >> 1; if (keys[m] < khi) a = m + 1; else b = m; }
+                    hi = a;
+                }
+                bool kp = true;
+                for (int j = lo; j < hi && kp; j++) {
+                    if (j == i) continue;
+                    const Feature& nb = F[perm[j]];
+                    float dist;
+                    if (!within_rd2(nb.x, nb.y, q.x, q.y, fc.separation, &dist)) continue;
+                    if (q.mass < nb.mass) kp = false;
+                    else if (q.mass == nb.mass && i > j) kp = false;
+                }
+                keep[i] = kp ? 1 : 0;
+            }
+            __syncthreads();
+        }
+    } else if (fc.prune) {
+        // 2b. sort by (r desc, mass desc), stable w.r.t. the canonical order
+        for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+            if (i < n) {
+                const Feature& ft = F[perm[i]];
+                uint64_t rk = (uint64_t)fc.radius_rank_desc[ft.ridx];
+                uint64_t mk = (uint64_t)(~float_order_key(ft.mass));
+                keys[i] = (rk << 56) | (mk << 24) | (uint64_t)i;
+            } else {
+                keys[i] = ~0ull;
+            }
+        }
+        __syncthreads();
+        block_sort_u64(keys, np2);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = (int32_t)(keys[i] & 0xFFFFFFull);
+        __syncthreads();
+        // prune_blobs_log (src/execute_gpu.rs:592-669): greedy in priority order
+        for (int q = 0; q < n; q++) {
+            if (!keep[q]) continue;  // uniform: keep[] only changes between barriers
+            const Feature& Q = F[perm[order[q]]];
+            const float qr = __fmul_rn(Q.r, 2.0f);
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                if (j == q || !keep[j]) continue;
+                const Feature& Nb = F[perm[order[j]]];
+                float d2;
+                if (!within_rd2(Nb.x, Nb.y, Q.x, Q.y, qr, &d2)) continue;
+                float ov = blob_overlap(Q.r, Nb.r, __fsqrt_rn(d2));
+                if (ov > fc.overlap_threshold) keep[j] = 0;
+            }
+            __syncthreads();
+        }
+    }
+
+    // 3. doughnut correction of the kept rows, one warp per row
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const T* raw = frames + (size_t)frame_index[g] * frame_stride;
+    // 4. compaction in output order
+    int total = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int k = (i < n) ? keep[i] : 0;
+        int tot;
+        int pos = block_excl_scan(k, &tot, wsum);
+        if (k) {
+            Feature ft = F[perm[order[i]]];
+            out[(size_t)g * feat_cap + total + pos] = ft;
+        }
+        total += tot;
+        __syncthreads();
+    }
+    __syncthreads();
+    if (fc.doughnut) {
+        uint32_t* myhist = hist + wid * 256;
+        for (int q = wid; q < total; q += (blockDim.x >> 5)) {
+            Feature ft = out[(size_t)g * feat_cap + q];
+            int4 m = dn_meta[fc.log_style ? ft.ridx : 0];
+            doughnut_warp<T>(raw, fc.H, fc.W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);
+            if (lane == 0) {
+                Feature* o = out + (size_t)g * feat_cap + q;
+                o->d_raw = ft.d_raw;
+                o->d_bg = ft.d_bg;
+                o->d_corr = ft.d_corr;
+            }
+            __syncwarp();
+        }
+    }
+    if (threadIdx.x == 0) kept_count[g] = (uint32_t)total;
+}
+
+// Per-frame rows -> table columns at the frame's row offset.
+__global__ void scatter_kernel(const Feature* __restrict__ feats, uint32_t feat_cap,
+                               const uint32_t* __restrict__ kept_count, const int64_t* __restrict__ row_off,
+                               const int64_t* __restrict__ frame_number, TableCols tab, int32_t g0) {
+    const int g = blockIdx.y;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kept_count[g]) return;
+    const Feature& ft = feats[(size_t)g * feat_cap + k];
+    const int64_t row = row_off[g0 + g] + k;
+    tab.frame[row] = frame_number[g0 + g];
+    tab.col[GT_COL_Y][row] = ft.x;
+    tab.col[GT_COL_X][row] = ft.y;
+    tab.col[GT_COL_MASS][row] = ft.mass;
+    tab.col[GT_COL_R][row] = ft.r;
+    tab.col[GT_COL_RG][row] = ft.Rg;
+    tab.col[GT_COL_RAW][row] = ft.raw;
+    tab.col[GT_COL_SIGNAL][row] = ft.signal;
+    tab.col[GT_COL_ECC][row] = ft.ecc;
+    tab.col[GT_COL_RAW_MASS][row] = ft.d_raw;
+    tab.col[GT_COL_RAW_BG_MEDIAN][row] = ft.d_bg;
+    tab.col[GT_COL_RAW_MASS_CORRECTED][row] = ft.d_corr;
+    tab.col[GT_COL_MAX_INTENSITY][row] = ft.max_i;
+    tab.col[GT_COL_COUNT][row] = ft.count;
+}
+
+// ------------------------------------------------------------ launch helpers
+size_t bandpass_smem_bytes(int R, int kd, bool cand) {
+    const int k = cand ? kd : 1;
+    const int PH = kLocateTH + k - 1, PW = kLocateTW + k - 1;
+    const int XH = PH + 2 * R, RW = PW + 2 * R;
+    size_t fl = (size_t)XH * RW + 2 * (size_t)XH * PW + (size_t)PH * PW + (cand ? (size_t)kLocateTH * PW : 0);
+    return fl * sizeof(float);
+}
+
+size_t finalize_smem_bytes() {
+    return (size_t)kFinalizeSmemSort * (8 + 4 + 4 + 1) + 32 * 256 * sizeof(uint32_t);
+}
+
+template <typename T>
+cudaError_t launch_bandpass(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c,
+                            int nframes, bool cand, uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap,
+                            uint32_t* flags, cudaStream_t st) {
+    dim3 grid((c.W + kLocateTW - 1) / kLocateTW, (c.H + kLocateTH - 1) / kLocateTH, nframes);
+    size_t smem = bandpass_smem_bytes(c.R, c.kd, cand);
+    if (cand) {
+        cudaFuncSetAttribute(bandpass_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        bandpass_kernel<T, true><<<grid, kLocateThreads, smem, st>>>(frames, frame_stride, processed, c, cand_count,
+                                                                    cand_keys, cand_cap, flags);
+    } else {
+        cudaFuncSetAttribute(bandpass_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        bandpass_kernel<T, false><<<grid, kLocateThreads, smem, st>>>(frames, frame_stride, processed, c, cand_count,
+                                                                     cand_keys, cand_cap, flags);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_stride, const LocateConsts& c,
+                        int nframes, int n_slots, const uint32_t* cand_count, const uint32_t* cand_keys,
+                        uint32_t cand_cap, uint32_t max_cands, const float* radii, const int32_t* angle_off,
+                        const float2* angles, Feature* feats, uint32_t* feat_count, uint32_t feat_cap,
+                        uint32_t* flags, cudaStream_t st) {
+    if (max_cands == 0) return cudaSuccess;
+    dim3 grid((max_cands + 127) / 128, nframes, n_slots);
+    walk_kernel<T><<<grid, 128, 0, st>>>(processed, frames, frame_stride, c, cand_count, cand_keys, cand_cap, radii,
+                                         angle_off, angles, feats, feat_count, feat_cap, flags, n_slots);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_characterize_points(const float* processed, const T* frames, int64_t frame_stride,
+                                       const LocateConsts& c, const float* pts, const int64_t* grp_off,
+                                       const int32_t* grp_frame, int32_t g0, int ngroups, int64_t max_pts,
+                                       const float2* angles, const int32_t* angle_off, int32_t n_angle_tabs,
+                                       int32_t has_r, Feature* feats, uint32_t* feat_count, uint32_t feat_cap,
+                                       cudaStream_t st) {
+    if (max_pts <= 0) return cudaSuccess;
+    dim3 grid((unsigned)((max_pts + 127) / 128), ngroups);
+    characterize_points_kernel<T><<<grid, 128, 0, st>>>(processed, frames, frame_stride, c, pts, grp_off, grp_frame,
+                                                        angles, angle_off, nullptr, n_angle_tabs, has_r, feats,
+                                                        feat_count, feat_cap, g0);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_finalize(const Feature* feats, const uint32_t* feat_count, uint32_t feat_cap, Feature* out,
+                            uint32_t* kept_count, uint8_t* gscratch, const FinalizeConsts& fc, const T* frames,
+                            int64_t frame_stride, const int32_t* frame_index, const short2* dn_inds,
+                            const int4* dn_meta, uint32_t* flags, int ngroups, cudaStream_t st) {
+    size_t smem = finalize_smem_bytes();
+    cudaFuncSetAttribute(finalize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    finalize_kernel<T><<<ngroups, kFinalizeThreads, smem, st>>>(feats, feat_count, feat_cap, out, kept_count,
+                                                                gscratch, fc, frames, frame_stride, frame_index,
+                                                                dn_inds, dn_meta, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const Feature* feats, uint32_t feat_cap, const uint32_t* kept_count,
+                           uint32_t max_kept, const int64_t* row_off, const int64_t* frame_number,
+                           const TableCols& tab, int32_t g0, int ngroups, cudaStream_t st) {
+    if (max_kept == 0) return cudaSuccess;
+    dim3 grid((max_kept + 255) / 256, ngroups);
+    scatter_kernel<<<grid, 256, 0, st>>>(feats, feat_cap, kept_count, row_off, frame_number, tab, g0);
+    return cudaGetLastError();
+}
+
+#define GT_INSTANTIATE(T)                                                                                       \
+    template cudaError_t launch_bandpass<T>(const T*, int64_t, float*, const LocateConsts&, int, bool, uint32_t*, \
+                                            uint32_t*, uint32_t, uint32_t*, cudaStream_t);                        \
+    template cudaError_t launch_walk<T>(const float*, const T*, int64_t, const LocateConsts&, int, int,          \
+                                        const uint32_t*, const uint32_t*, uint32_t, uint32_t, const float*,      \
+                                        const int32_t*, const float2*, Feature*, uint32_t*, uint32_t, uint32_t*, \
+                                        cudaStream_t);                                                           \
+    template cudaError_t launch_characterize_points<T>(const float*, const T*, int64_t, const LocateConsts&,     \
+                                                       const float*, const int64_t*, const int32_t*, int32_t,     \
+                                                       int, int64_t, const float2*, const int32_t*, int32_t,      \
+                                                       int32_t, Feature*, uint32_t*, uint32_t, cudaStream_t);     \
+    template cudaError_t launch_finalize<T>(const Feature*, const uint32_t*, uint32_t, Feature*, uint32_t*,      \
+                                            uint8_t*, const FinalizeConsts&, const T*, int64_t, const int32_t*,  \
+                                            const short2*, const int4*, uint32_t*, int, cudaStream_t);
+
+GT_INSTANTIATE(uint16_t)
+GT_INSTANTIATE(float)
+GT_INSTANTIATE(uint8_t)
+
+}  // namespace gt

@@ -24,6 +24,12 @@
 
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define GT_API __attribute__((visibility("default")))
+#else
+#define GT_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -92,23 +98,23 @@ typedef struct gt_params {
 } gt_params;
 
 /* TrackingParams::default() (src/gpu_setup.rs:61-97). */
-void gt_params_default(gt_params* p);
+GT_API void gt_params_default(gt_params* p);
 
 /* ------------------------------------------------------------- context */
 typedef struct gt_ctx gt_ctx;
 
 /* new_adapter + new_device_queue (src/gpu_setup.rs:582-609): binds a device. */
-gt_status gt_create(int32_t device, gt_ctx** out);
-void gt_destroy(gt_ctx* ctx);
+GT_API gt_status gt_create(int32_t device, gt_ctx** out);
+GT_API void gt_destroy(gt_ctx* ctx);
 /* Human-readable message of the last failing call on this context. */
-const char* gt_last_error(const gt_ctx* ctx);
+GT_API const char* gt_last_error(const gt_ctx* ctx);
 /* Cooperative interrupt (the reference's Arc<AtomicBool>, src/execute_gpu.rs:1094-1099):
  * a non-zero *flag makes the running call return GT_ERR_INTERRUPTED between
  * frame chunks.  Pass NULL to clear. */
-gt_status gt_set_interrupt(gt_ctx* ctx, const volatile int32_t* flag);
+GT_API gt_status gt_set_interrupt(gt_ctx* ctx, const volatile int32_t* flag);
 /* Progress of the running/last call: (frames done, frames total), the
  * reference's Arc<Mutex<(usize, Option<usize>)>> (src/execute_gpu.rs:972-975). */
-gt_status gt_progress(const gt_ctx* ctx, int64_t* done, int64_t* total);
+GT_API gt_status gt_progress(const gt_ctx* ctx, int64_t* done, int64_t* total);
 
 /* ------------------------------------------------------------ result table */
 typedef struct gt_table gt_table;
@@ -124,16 +130,16 @@ typedef enum gt_column {
     GT_NUM_COLUMNS
 } gt_column;
 
-int64_t gt_table_nrows(const gt_table* t);
+GT_API int64_t gt_table_nrows(const gt_table* t);
 /* Copy one column to host memory as float32 (all value columns, and the
  * integer columns converted the way the reference stores them). */
-gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst);
+GT_API gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst);
 /* Copy an integer column (frame / particle / duration) as int64. */
-gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst);
+GT_API gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst);
 /* 1 if the column was computed for this table (e.g. GT_COL_PARTICLE only
  * when linking ran). */
-int32_t gt_table_has_column(const gt_table* t, int32_t column);
-void gt_table_free(gt_table* t);
+GT_API int32_t gt_table_has_column(const gt_table* t, int32_t column);
+GT_API void gt_table_free(gt_table* t);
 
 /* ---------------------------------------------------------------- entry points */
 /*
@@ -148,7 +154,7 @@ void gt_table_free(gt_table* t);
  * linker_reset_points (nullable, length n_reset) mirrors
  * TrackingParams::linker_reset_points (src/execute_gpu.rs:792-798).
  */
-gt_status gt_batch(gt_ctx* ctx, const gt_params* params,
+GT_API gt_status gt_batch(gt_ctx* ctx, const gt_params* params,
                    const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
                    const int64_t* frame_numbers,
                    const int64_t* linker_reset_points, int64_t n_reset,
@@ -161,7 +167,7 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params,
  * src/linking.rs:97-196).  points is row-major (n_points, ncols) float32 with
  * columns [frame,] y, x [, r] according to has_frames / has_r.
  */
-gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params,
+GT_API gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params,
                                  const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
                                  const float* points, int64_t n_points,
                                  int32_t has_frames, int32_t has_r,
@@ -172,7 +178,7 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params,
  * -> linker_all (src/linking.rs:818-831).  frame_y_x is row-major (n, 3)
  * float32, sorted by frame.  particle_out receives one id per row.
  */
-gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n,
+GT_API gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n,
                   float search_range, uint32_t memory, int64_t* particle_out);
 
 /*
@@ -180,7 +186,7 @@ gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n,
  * (gpu_tracking_python/src/python_bindings.rs:293-312) -> connect_all
  * (src/linking.rs:960-1020).
  */
-gt_status gt_connect(gt_ctx* ctx, const float* frame_y_x1, int64_t n1,
+GT_API gt_status gt_connect(gt_ctx* ctx, const float* frame_y_x1, int64_t n1,
                      const float* frame_y_x2, int64_t n2, float search_range,
                      int64_t* out1, int64_t* out2);
 
@@ -188,11 +194,20 @@ gt_status gt_connect(gt_ctx* ctx, const float* frame_y_x1, int64_t n1,
  * Mean frame of a video (src/execute_gpu.rs:819-847, mean_from_file_rust
  * gpu_tracking_python/src/python_bindings.rs:361-371), out is (H, W) float32.
  */
-gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype,
+GT_API gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype,
                         int64_t T, int32_t H, int32_t W, float* out);
 
 /* Library version string. */
-const char* gt_version(void);
+GT_API const char* gt_version(void);
+
+/* ------------------------------------------------------------ diagnostics */
+/* Per-kernel timing with CUDA events on the engine's compute stream (no
+ * counterpart in the reference): enable, run calls, then read the launch
+ * count and summed milliseconds of a kernel class ("bandpass_localmax",
+ * "walk_characterize", "finalize", "bandpass", "laplace", "logspace_max",
+ * "link_sort", "link_lists", "link_video"). */
+GT_API gt_status gt_profile_enable(gt_ctx* ctx, int32_t enable);
+GT_API gt_status gt_profile_read(gt_ctx* ctx, const char* name, int64_t* launches, double* total_ms);
 
 #ifdef __cplusplus
 }
