@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Headline benchmark of the B200 particle locate + link engine.
+
+Workload (one step = one pass of the hot path over one synthetic video):
+2000 frames of 2048x2048 uint16, 2000 Gaussian spots per frame (sigma uniform
+1.2-2.5 px, peak SNR log-normal in 3-20 over a background of 100 with
+Poisson noise), Brownian motion D = 1.0 px^2/frame with 2 % births/deaths per
+frame; trackpy-style locate with diameter 11, full characterization and the
+doughnut correction (the Python defaults), minmass 220 (the configuration
+names none; 220 separates the noise maxima, mass <= 190, from the dimmest
+true spots, mass >= 260, on this generator), linking with search_range 7 and
+memory 3.  The video is generated on the device and stays in HBM (16.8 GB,
+larger than L2, so no flush is needed between steps).
+
+  value  frames/s over all ranks, inputs resident in HBM, device-timed with
+         CUDA events (max over ranks)
+  e2e    the same through the public Python API (gt.batch on a pinned host
+         array, host->device copies and the DataFrame read-back included)
+
+Multi-GPU (torchrun): weak scaling, every rank tracks its own video (frames
+and videos are independent; no data-path collective).
+
+`--impl reference` times the CPU restatement of the reference's path (the
+oracle; the reference's own Rust/wgpu build is unavailable here) on the host
+cores with every thread, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s + features/s at 2048²: plain vs learned-proposal; % HBM roofline"
+CONFIG = dict(workload="plain batch locate+characterize+link, 2000 frames 2048x2048 uint16, 2000 spots/frame",
+              frames=2000, height=2048, width=2048, spots_per_frame=2000, diameter=11, minmass=220.0,
+              separation=12, characterize=True, doughnut_correction=True, search_range=7.0, memory=3,
+              sigma_px=[1.2, 2.5], snr=[3, 20], background=100, D=1.0, births_deaths=0.02,
+              l2="inputs (16.8 GB) larger than L2; no flush", style="trackpy")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=CONFIG["frames"])
+    ap.add_argument("--size", type=int, default=CONFIG["height"])
+    ap.add_argument("--cpu-sample", type=int, default=0, help="frames in the CPU-baseline sample (0: auto)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def params():
+    from gpu_tracking_b200._params import trackpy_params
+    return trackpy_params(CONFIG["diameter"], minmass=CONFIG["minmass"], search_range=CONFIG["search_range"],
+                          memory=CONFIG["memory"])
+
+
+def make_video(n_frames, size, seed, device):
+    from gpu_tracking_b200.synth import brownian_video
+    return brownian_video(n_frames, size, size, CONFIG["spots_per_frame"], seed=seed, device=device,
+                          sigma_range=tuple(CONFIG["sigma_px"]), snr_range=tuple(CONFIG["snr"]),
+                          bg=CONFIG["background"], D=CONFIG["D"], turnover=CONFIG["births_deaths"])
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-frame DRAM traffic of the dominant kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(frames_u16, p, nthreads):
+    """The oracle on the host cores; returns frames/s and the sample size."""
+    import numpy as np
+    from oracle import loader
+    f32 = frames_u16.astype(np.float32)
+    t = time.perf_counter()
+    tab = loader.batch(p, f32, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    return len(f32) / dt, dt, len(tab)
+
+
+def run_reference(args):
+    import numpy as np
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import torch
+    dev = "cuda:0" if torch.cuda.is_available() else "cpu"
+    cores = os.cpu_count() or 1
+    n = args.cpu_sample or max(8, min(64, 2 * cores))
+    vid = make_video(n, args.size, 2, dev).cpu().numpy()
+    p = params()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        fps, dt, rows = cpu_baseline(vid, p, cores)
+        if i >= args.warmup:
+            vals.append(fps)
+    v = statistics.median(vals)
+    sample = "%d frames of the %dx%d workload (oracle, locate+characterize+doughnut with %d threads, link serial)" % (
+        n, args.size, args.size, cores)
+    line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * n / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": dict(CONFIG, frames=n, height=args.size, width=args.size, parallelism="host threads"),
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    os.environ["GT_DEVICE"] = str(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    import gpu_tracking_b200 as gt
+    from gpu_tracking_b200 import _ffi
+    from gpu_tracking_b200._params import DTYPE_U16
+
+    T, S = args.frames, args.size
+    video = make_video(T, S, 2 + rank, "cuda:%d" % local)
+    torch.cuda.synchronize()
+    p = params()
+    ctx = _ffi.context(local)
+    L = _ffi.lib()
+
+    def step():
+        out = ctypes.c_void_p()
+        ctx.check(L.gt_batch(ctx.handle, ctypes.byref(p), ctypes.c_void_p(video.data_ptr()), DTYPE_U16, T, S, S,
+                             None, None, 0, ctypes.byref(out)))
+        n = L.gt_table_nrows(out)
+        L.gt_table_free(out)
+        return n
+
+    for _ in range(args.warmup):
+        rows = step()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ctx.profile(True)
+    l0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record()
+    rows_total = 0
+    for _ in range(args.steps):
+        rows_total += step()
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count() - l0
+    kernels = {}
+    for name in ("bandpass_localmax", "walk_characterize", "finalize", "scatter", "link_sort", "link_lists",
+                 "link_video", "link_durations", "round_ids"):
+        n, kms = ctx.profile_read(name)
+        if n:
+            kernels[name] = (n, kms)
+    ctx.profile(False)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        r = torch.tensor([rows_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(r)
+        rows_all = float(r.item())
+    else:
+        rows_all = float(rows_total)
+    frames_all = float(T * args.steps * world)
+    value = frames_all / (ms / 1000.0)
+    feats_per_s = rows_all / (ms / 1000.0)
+
+    # end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        try:
+            host = torch.empty(video.shape, dtype=torch.uint16, pin_memory=True)
+            host.copy_(video)
+            host_np = host.numpy()
+            e2e_frames = T
+        except Exception:
+            e2e_frames = min(T, 256)
+            host = torch.empty((e2e_frames, S, S), dtype=torch.uint16, pin_memory=True)
+            host.copy_(video[:e2e_frames])
+            host_np = host.numpy()
+        kw = dict(minmass=CONFIG["minmass"], search_range=CONFIG["search_range"], memory=CONFIG["memory"],
+                  tqdm=False)
+        df = gt.batch(host_np, CONFIG["diameter"], **kw)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            df = gt.batch(host_np, CONFIG["diameter"], **kw)
+            # float columns travel as float32, integer columns as int64
+            d2h += len(df) * sum(8 if df[c].dtype == np.int64 else 4 for c in df.columns)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": e2e_frames * args.steps * world / e2e_s, "unit": "frames/s",
+               "h2d_bytes_per_step": int(host_np.nbytes), "d2h_bytes_per_step": int(d2h // args.steps),
+               "frames_per_step": e2e_frames}
+        del host
+
+    # roofline of the dominant kernel
+    peak, peak_kind = load_peaks()
+    total_k = sum(v[1] for v in kernels.values()) or 1.0
+    dom = max(kernels.items(), key=lambda kv: kv[1][1]) if kernels else ("bandpass_localmax", (1, 1.0))
+    feats_per_frame = rows_all / frames_all
+    bytes_per_frame = S * S * 2 + feats_per_frame * 48.0
+    # frames per launch of the per-chunk kernels: the engine's chunk size
+    frames_per_launch = (T * args.steps) / max(1, kernels.get(dom[0], (1, 1))[0])
+    achieved = None
+    if dom[1][1] > 0:
+        avg_launch_s = dom[1][1] / 1000.0 / dom[1][0]
+        achieved = bytes_per_frame * frames_per_launch / avg_launch_s / 1e9
+    traffic = load_traffic().get(dom[0])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (traffic["dram_bytes_per_frame"] * frames_per_launch) if traffic else None,
+                "kernel": dom[0], "peak_kind": peak_kind,
+                "algorithmic_bytes_per_frame": bytes_per_frame,
+                "kernel_share": {k: round(v[1] / total_k, 4) for k, v in kernels.items()},
+                "whole_step_frac": frames_all * bytes_per_frame / (ms / 1000.0) / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        n = args.cpu_sample or max(8, min(64, 2 * cores))
+        sample = video[:n].cpu().numpy()
+        fps, dt, _ = cpu_baseline(sample, p, cores)
+        cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
+               "sample": "first %d frames of the workload (%.1f s of CPU work)" % (n, dt)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(CONFIG, frames=T, height=S, width=S,
+                               parallelism="dp%d (one video per rank)" % world),
+                "features_per_s": feats_per_s, "features_per_frame": feats_per_frame,
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clk}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -79,6 +79,8 @@ def lib():
         L.gt_mean_frame.argtypes = [vp, vp, i32, i64, i32, i32, P(f32)]
         L.gt_profile_enable.argtypes = [vp, i32]
         L.gt_profile_read.argtypes = [vp, ctypes.c_char_p, P(i64), P(ctypes.c_double)]
+        L.gt_launch_count.argtypes = [vp]
+        L.gt_launch_count.restype = i64
         for name in ("gt_create", "gt_set_interrupt", "gt_progress", "gt_table_column_f32", "gt_table_column_i64",
                      "gt_batch", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
                      "gt_profile_enable", "gt_profile_read"):
@@ -123,6 +125,9 @@ class Context:
         n, ms = ctypes.c_int64(), ctypes.c_double()
         self.check(lib().gt_profile_read(self._h, name.encode(), ctypes.byref(n), ctypes.byref(ms)))
         return n.value, ms.value
+
+    def launch_count(self):
+        return lib().gt_launch_count(self._h)
 
     def close(self):
         if self._h:

@@ -73,6 +73,7 @@ struct gt_ctx {
     // profiling of the main kernels (CUDA events on the compute stream)
     bool profile = false;
     std::map<std::string, KernelStat> stats;
+    std::map<std::string, int64_t> launch_count;
     std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
     std::vector<cudaEvent_t> event_pool;
     // device buffers, grown on demand and kept for the next call
@@ -119,11 +120,14 @@ gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
     } while (0)
 
 // --------------------------------------------------------------- profiling
+// Counts every kernel launch of the engine; with profiling enabled also
+// brackets it with CUDA events on the compute stream.
 struct Prof {
     gt_ctx* ctx;
     const char* name;
     cudaEvent_t a = nullptr, b = nullptr;
     Prof(gt_ctx* c, const char* n) : ctx(c), name(n) {
+        ctx->launch_count[name]++;
         if (!ctx->profile) return;
         a = take();
         b = take();
@@ -502,7 +506,10 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
         CK(cudaMemcpy(counters->data(), out.counter, nvideos * 8, cudaMemcpyDeviceToHost));
     }
     if (row_dur) {
-        CK(link_durations(in, out, row_dur, ctx->st));
+        {
+            Prof pf(ctx, "link_durations");
+            CK(link_durations(in, out, row_dur, ctx->st));
+        }
         CK(cudaMemcpyAsync(flags.data(), out.flags, nvideos * 4, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
         for (auto f : flags)
@@ -540,13 +547,17 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     const bool log_style = (p.style == GT_STYLE_LOG);
     const int nslots = log_style ? (int)lt->radii.size() : 1;
     const uint32_t cand_cap = ctx->cand_cap, feat_cap = ctx->feat_cap;
-    const int nchunks = (int)((NT + F - 1) / F);
+    // super-chunks of SC frames: located chunk by chunk (F frames per launch),
+    // then finalized together (one CTA per frame fills the GPU)
+    const int per_super = std::max(1, (int)std::min<int64_t>(128 / F, (NT + F - 1) / F));
+    const int SC = F * per_super;
+    const int nsuper = (int)((NT + SC - 1) / SC);
     CK(ctx->processed.ensure((size_t)F * npx * 4));
     if (log_style) CK(ctx->planes.ensure((size_t)F * nslots * npx * 4));
     CK(ctx->cand_count.ensure((size_t)F * nslots * 4));
     CK(ctx->cand_keys.ensure((size_t)F * nslots * cand_cap * 4));
-    CK(ctx->feats_raw.ensure((size_t)F * feat_cap * sizeof(Feature)));
-    CK(ctx->feat_count.ensure((size_t)F * 4));
+    CK(ctx->feats_raw.ensure((size_t)SC * feat_cap * sizeof(Feature)));
+    CK(ctx->feat_count.ensure((size_t)SC * 4));
     CK(ctx->feats_out.ensure((size_t)NT * feat_cap * sizeof(Feature)));
     CK(ctx->kept_count.ensure((size_t)NT * 4));
     CK(ctx->flags.ensure(16));
@@ -558,10 +569,10 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         while (np2 < feat_cap) np2 <<= 1;
         fin_per_frame = (np2 * 17 + 255) & ~(size_t)255;
     }
-    CK(ctx->fin_scratch.ensure(std::max<size_t>(fin_per_frame * F, 256)));
+    CK(ctx->fin_scratch.ensure(std::max<size_t>(fin_per_frame * SC, 256)));
     {
-        std::vector<int32_t> ident(F);
-        for (int i = 0; i < F; i++) ident[i] = i;
+        std::vector<int32_t> ident(SC);
+        for (int i = 0; i < SC; i++) ident[i] = i;
         CKS(upload(ctx, ctx->ident, ident));
     }
     // constant tables
@@ -625,15 +636,15 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     lc.n_radii = nslots;
     lc.thr = 0.0f;
 
-    const size_t chunk_bytes = (size_t)F * npx * sizeof(T);
+    const size_t super_bytes = (size_t)SC * npx * sizeof(T);
     if (!on_device) {
-        CK(ctx->stage[0].ensure(chunk_bytes));
-        CK(ctx->stage[1].ensure(chunk_bytes));
+        CK(ctx->stage[0].ensure(super_bytes));
+        CK(ctx->stage[1].ensure(super_bytes));
     }
-    auto issue_copy = [&](int chunk) -> gt_status {
-        int b = chunk & 1;
-        int64_t f0 = (int64_t)chunk * F;
-        int nf = (int)std::min<int64_t>(F, NT - f0);
+    auto issue_copy = [&](int sc) -> gt_status {
+        int b = sc & 1;
+        int64_t f0 = (int64_t)sc * SC;
+        int nf = (int)std::min<int64_t>(SC, NT - f0);
         CK(cudaStreamWaitEvent(ctx->cp, ctx->used[b], 0));
         CK(cudaMemcpyAsync(ctx->stage[b].p, frames + f0 * npx, (size_t)nf * npx * sizeof(T), cudaMemcpyHostToDevice,
                            ctx->cp));
@@ -647,64 +658,69 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         CKS(issue_copy(0));
     }
     uint32_t* flags = ctx->flags.as<uint32_t>();
-    for (int ch = 0; ch < nchunks; ch++) {
+    float* proc = ctx->processed.as<float>();
+    for (int sc = 0; sc < nsuper; sc++) {
         if (interrupted(ctx)) {
             cudaStreamSynchronize(ctx->st);
             cudaStreamSynchronize(ctx->cp);
             return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
         }
-        const int64_t f0 = (int64_t)ch * F;
-        const int nf = (int)std::min<int64_t>(F, NT - f0);
-        const T* src;
+        const int64_t s0 = (int64_t)sc * SC;
+        const int ns = (int)std::min<int64_t>(SC, NT - s0);
+        const T* sbase;
         if (on_device) {
-            src = frames + f0 * npx;
+            sbase = frames + s0 * npx;
         } else {
-            if (ch + 1 < nchunks) CKS(issue_copy(ch + 1));
-            CK(cudaStreamWaitEvent(ctx->st, ctx->filled[ch & 1], 0));
-            src = ctx->stage[ch & 1].as<T>();
+            if (sc + 1 < nsuper) CKS(issue_copy(sc + 1));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->filled[sc & 1], 0));
+            sbase = ctx->stage[sc & 1].as<T>();
         }
-        CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
-        CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)nf * 4, ctx->st));
-        float* proc = ctx->processed.as<float>();
-        if (!log_style) {
-            Prof pf(ctx, "bandpass_localmax");
-            CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
-                                  ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
-        } else {
-            {
-                Prof pf(ctx, "bandpass");
-                CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags, ctx->st));
+        CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)ns * 4, ctx->st));
+        for (int64_t c0f = 0; c0f < ns; c0f += F) {
+            const int nf = (int)std::min<int64_t>(F, ns - c0f);
+            const T* src = sbase + c0f * npx;
+            CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
+            if (!log_style) {
+                Prof pf(ctx, "bandpass_localmax");
+                CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
+                                      ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+            } else {
+                {
+                    Prof pf(ctx, "bandpass");
+                    CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
+                                          ctx->st));
+                }
+                {
+                    Prof pf(ctx, "laplace");
+                    CK(launch_laplace<T>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
+                                         ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
+                                         lnd.as<float>(), lt->max_rint, nf, ctx->st));
+                }
+                {
+                    Prof pf(ctx, "logspace_max");
+                    CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
+                                           ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+                }
             }
             {
-                Prof pf(ctx, "laplace");
-                CK(launch_laplace<T>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
-                                     ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
-                                     lnd.as<float>(), lt->max_rint, nf, ctx->st));
+                Prof pf(ctx, "walk_characterize");
+                CK(launch_walk<T>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
+                                  ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap,
+                                  log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
+                                  ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap,
+                                  ctx->feat_count.as<uint32_t>() + c0f, feat_cap, flags, ctx->st));
             }
-            {
-                Prof pf(ctx, "logspace_max");
-                CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
-                                       ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
-            }
-        }
-        {
-            Prof pf(ctx, "walk_characterize");
-            CK(launch_walk<T>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
-                              ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap,
-                              log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
-                              ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
-                              feat_cap, flags, ctx->st));
         }
         {
             Prof pf(ctx, "finalize");
             CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
-                                  ctx->feats_out.as<Feature>() + (size_t)f0 * feat_cap,
-                                  ctx->kept_count.as<uint32_t>() + f0, ctx->fin_scratch.as<uint8_t>(), fc, src,
+                                  ctx->feats_out.as<Feature>() + (size_t)s0 * feat_cap,
+                                  ctx->kept_count.as<uint32_t>() + s0, ctx->fin_scratch.as<uint8_t>(), fc, sbase,
                                   (int64_t)npx, ctx->ident.as<int32_t>(), ctx->tabs_s.as<short2>(),
-                                  ctx->tabs_m.as<int4>(), flags, nf, ctx->st));
+                                  ctx->tabs_m.as<int4>(), flags, ns, ctx->st));
         }
-        if (!on_device) CK(cudaEventRecord(ctx->used[ch & 1], ctx->st));
-        ctx->done = f0 + nf;
+        if (!on_device) CK(cudaEventRecord(ctx->used[sc & 1], ctx->st));
+        ctx->done = s0 + ns;
     }
     CK(cudaMemcpyAsync(out_flags, flags, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -744,6 +760,7 @@ gt_status assemble_table(gt_ctx* ctx, int64_t NT, const std::vector<int64_t>& fr
     tc.duration = nullptr;
     for (int64_t g0 = 0; g0 < NT; g0 += 65535) {
         int ng = (int)std::min<int64_t>(65535, NT - g0);
+        Prof pf(ctx, "scatter");
         CK(launch_scatter(ctx->feats_out.as<Feature>() + (size_t)g0 * ctx->feat_cap, ctx->feat_cap,
                           ctx->kept_count.as<uint32_t>() + g0, maxk, ctx->row_off.as<int64_t>(),
                           ctx->frame_num.as<int64_t>(), tc, (int32_t)g0, ng, ctx->st));
@@ -813,9 +830,11 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         CK(tab->duration.ensure(n1 * 8));
         CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
                      ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
-        if (tab->n > 0)
+        if (tab->n > 0) {
+            Prof pf(ctx, "round_ids");
             f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
                 ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+        }
         CK(cudaGetLastError());
         tab->has[GT_COL_PARTICLE] = true;
         tab->has[GT_COL_DURATION] = true;
@@ -914,10 +933,14 @@ gt_status mean_impl(gt_ctx* ctx, const T* frames, bool on_device, int64_t NT, in
                                ctx->st));
             src = ctx->stage[0].as<T>();
         }
+        Prof pf(ctx, "mean_frame");
         mean_accumulate_kernel<T><<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(src, nf, npx, acc);
         CK(cudaGetLastError());
     }
-    mean_divide_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(acc, npx, (float)NT);
+    {
+        Prof pf(ctx, "mean_frame");
+        mean_divide_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(acc, npx, (float)NT);
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, acc, npx * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -1029,13 +1052,16 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
             CK(cudaMemcpyAsync(stage + (size_t)g * npx, frames + (size_t)gframe[g0 + g] * npx, npx * sizeof(T),
                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->st));
         CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)ng * 4, ctx->st));
+        Prof pf1(ctx, "bandpass");
         CK(launch_bandpass<T>(stage, (int64_t)npx, ctx->processed.as<float>(), c, ng, false, nullptr, nullptr, 0,
                               ctx->flags.as<uint32_t>(), ctx->st));
+        Prof pf2(ctx, "characterize_points");
         CK(launch_characterize_points<T>(ctx->processed.as<float>(), stage, (int64_t)npx, c, dpts.as<float>(),
                                          dgoff.as<int64_t>(), dgloc.as<int32_t>(), (int32_t)g0, ng, maxg,
                                          ctx->tabs_f.as<float2>(), ctx->tabs_i.as<int32_t>(), (int32_t)aoff.size(),
                                          has_r, ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
                                          feat_cap, ctx->st));
+        Prof pf3(ctx, "finalize");
         CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
                               ctx->feats_out.as<Feature>() + (size_t)g0 * feat_cap,
                               ctx->kept_count.as<uint32_t>() + g0, ctx->fin_scratch.as<uint8_t>(), fc, stage,
@@ -1066,9 +1092,11 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
         CK(tab->duration.ensure(n1 * 8));
         CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
                      ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
-        if (tab->n > 0)
+        if (tab->n > 0) {
+            Prof pf(ctx, "round_ids");
             f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
                 ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+        }
         CK(cudaGetLastError());
         tab->has[GT_COL_PARTICLE] = true;
         tab->has[GT_COL_DURATION] = true;
@@ -1417,6 +1445,7 @@ gt_status gt_profile_enable(gt_ctx* ctx, int32_t enable) {
     if (!ctx) return GT_ERR_INVALID_ARGUMENT;
     ctx->profile = enable != 0;
     ctx->stats.clear();
+    ctx->launch_count.clear();
     return GT_OK;
 }
 
@@ -1432,6 +1461,13 @@ gt_status gt_profile_read(gt_ctx* ctx, const char* name, int64_t* launches, doub
     if (launches) *launches = it->second.launches;
     if (total_ms) *total_ms = it->second.ms;
     return GT_OK;
+}
+
+int64_t gt_launch_count(gt_ctx* ctx) {
+    if (!ctx) return 0;
+    int64_t n = 0;
+    for (auto& kv : ctx->launch_count) n += kv.second;
+    return n;
 }
 
 }  // extern "C"

@@ -47,6 +47,13 @@ cudaError_t launch_bandpass(const T* frames, int64_t frame_stride, float* proces
                             int nframes, bool cand, uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap,
                             uint32_t* flags, cudaStream_t st);
 
+// Streaming strip kernel for the specialised (radius, dilation) pairs; returns
+// false when the pair has no specialisation (the tile kernel is used then).
+template <typename T>
+bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
+                  uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,
+                  cudaError_t* err);
+
 template <typename T>
 cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_stride, const LocateConsts& c,
                         int nframes, int n_slots, const uint32_t* cand_count, const uint32_t* cand_keys,

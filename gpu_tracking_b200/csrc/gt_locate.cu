@@ -729,6 +729,10 @@ cudaError_t launch_bandpass(const T* frames, int64_t frame_stride, float* proces
     dim3 grid((c.W + kLocateTW - 1) / kLocateTW, (c.H + kLocateTH - 1) / kLocateTH, nframes);
     size_t smem = bandpass_smem_bytes(c.R, c.kd, cand);
     if (cand) {
+        cudaError_t e = cudaSuccess;
+        if (launch_strip<T>(frames, frame_stride, processed, c, nframes, cand_count, cand_keys, cand_cap, flags, st,
+                            &e))
+            return e;
         cudaFuncSetAttribute(bandpass_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         bandpass_kernel<T, true><<<grid, kLocateThreads, smem, st>>>(frames, frame_stride, processed, c, cand_count,
                                                                     cand_keys, cand_cap, flags);

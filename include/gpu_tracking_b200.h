@@ -208,6 +208,8 @@ GT_API const char* gt_version(void);
  * "link_sort", "link_lists", "link_video"). */
 GT_API gt_status gt_profile_enable(gt_ctx* ctx, int32_t enable);
 GT_API gt_status gt_profile_read(gt_ctx* ctx, const char* name, int64_t* launches, double* total_ms);
+/* Number of engine kernel launches since the last gt_profile_enable. */
+GT_API int64_t gt_launch_count(gt_ctx* ctx);
 
 #ifdef __cplusplus
 }

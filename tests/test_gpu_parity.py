@@ -249,3 +249,17 @@ def test_errors():
         gt.load("file.avi")
     with pytest.raises(FileNotFoundError):
         gt.load("/nonexistent/file.npy")
+
+
+@pytest.mark.parametrize("diam,sep", [(9, None), (11, None), (9, 9), (7, None), (5, None), (13, None), (9, 30)])
+def test_strip_segments_and_generic_fallback(oracle, diam, sep):
+    """Tall frames split into several row segments, widths that are not a
+    multiple of the strip width, and a dilation size without a specialised
+    kernel (separation 30)."""
+    frames, _ = video(2, 1100, 300, 160, seed=diam * 3 + (sep or 0))
+    kw = dict(minmass=300.0, doughnut_correction=False)
+    if sep is not None:
+        kw["separation"] = sep
+    df = gt.batch(frames, diam, tqdm=False, **kw)
+    tab = oracle.batch(trackpy_params(diam, **kw), frames.astype(np.float32))
+    assert_same(df, tab, ["frame", "y", "x", "mass", "Rg", "raw", "signal", "ecc"])
