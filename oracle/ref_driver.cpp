@@ -34,6 +34,32 @@ struct uvec3 {
     uint32_t operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
 };
 
+// WGSL storage array with robust buffer access.
+template <class T>
+struct RobustArray {
+    T* p = nullptr;
+    int64_t n = 0;
+    T dummy{};
+    RobustArray() = default;
+    RobustArray& operator=(T* q) {
+        p = q;
+        return *this;
+    }
+    T& operator[](int64_t i) {
+        if (i < 0 || i >= n) {
+            dummy = T{};
+            return dummy;
+        }
+        return p[i];
+    }
+};
+
+template <class T>
+void bind(RobustArray<T>& a, T* p, int64_t n) {
+    a.p = p;
+    a.n = n;
+}
+
 inline float wgsl_f32(float x) { return x; }
 inline float wgsl_f32(int32_t x) { return (float)x; }
 inline float wgsl_f32(uint32_t x) { return (float)x; }
@@ -106,18 +132,18 @@ int ref_preprocess(const RefParams* p, int32_t truncate, const float* frame, flo
     const int32_t H = p->pic_nrows, W = p->pic_ncols;
     std::vector<vec2f> temp((size_t)H * W);
     set_params(sh_preprocess_rows::params, p);
-    sh_preprocess_rows::picture = const_cast<float*>(frame);
-    sh_preprocess_rows::temp = temp.data();
+    bind(sh_preprocess_rows::picture, const_cast<float*>(frame), (int64_t)H * W);
+    bind(sh_preprocess_rows::temp, temp.data(), (int64_t)H * W);
     dispatch2d(H, W, [](uvec3 g) { sh_preprocess_rows::main_(g); });
     if (truncate) {
         set_params(sh_preprocess_cols_trunc::params, p);
-        sh_preprocess_cols_trunc::temp = temp.data();
-        sh_preprocess_cols_trunc::processed_buffer = processed;
+        bind(sh_preprocess_cols_trunc::temp, temp.data(), (int64_t)H * W);
+        bind(sh_preprocess_cols_trunc::processed_buffer, processed, (int64_t)H * W);
         dispatch2d(H, W, [](uvec3 g) { sh_preprocess_cols_trunc::main_(g); });
     } else {
         set_params(sh_preprocess_cols_notrunc::params, p);
-        sh_preprocess_cols_notrunc::temp = temp.data();
-        sh_preprocess_cols_notrunc::processed_buffer = processed;
+        bind(sh_preprocess_cols_notrunc::temp, temp.data(), (int64_t)H * W);
+        bind(sh_preprocess_cols_notrunc::processed_buffer, processed, (int64_t)H * W);
         dispatch2d(H, W, [](uvec3 g) { sh_preprocess_cols_notrunc::main_(g); });
     }
     return 0;
@@ -127,17 +153,17 @@ int64_t ref_candidates(const RefParams* p, const float* processed, float pic_std
     const int32_t H = p->pic_nrows, W = p->pic_ncols;
     std::vector<float> mr((size_t)H * W);
     set_params(sh_max_rows::params, p);
-    sh_max_rows::processed_buffer = const_cast<float*>(processed);
-    sh_max_rows::max_rows = mr.data();
+    bind(sh_max_rows::processed_buffer, const_cast<float*>(processed), (int64_t)H * W);
+    bind(sh_max_rows::max_rows, mr.data(), (int64_t)H * W);
     dispatch2d(H, W, [](uvec3 g) { sh_max_rows::main_(g); });
     // every pixel may be a candidate; the reference's own buffer holds H*W/4
     // entries and drops the rest, which the callers treat as an error case
     std::vector<sh_extract_max::ParticleLocation> pts((size_t)H * W + 1);
     set_params(sh_extract_max::params, p);
-    sh_extract_max::processed_buffer = const_cast<float*>(processed);
-    sh_extract_max::max_rows = mr.data();
+    bind(sh_extract_max::processed_buffer, const_cast<float*>(processed), (int64_t)H * W);
+    bind(sh_extract_max::max_rows, mr.data(), (int64_t)H * W);
     sh_extract_max::n_particles = 0;
-    sh_extract_max::max_points = pts.data();
+    bind(sh_extract_max::max_points, pts.data(), (int64_t)pts.size());
     sh_extract_max::pic_std = pic_std;
     sh_extract_max::wg_size = {};
     dispatch2d(H, W, [](uvec3 g) { sh_extract_max::main_(g); });
@@ -157,12 +183,12 @@ int64_t ref_walk(const RefParams* p, const float* processed, const float* raw, c
     for (int64_t i = 0; i < n; i++) parts[i] = {uv[2 * i], uv[2 * i + 1], r, -1.0f};
     std::vector<sh_walk::ResultRow> res((size_t)n + 1);
     set_params(sh_walk::params, p);
-    sh_walk::processed_buffer = const_cast<float*>(processed);
-    sh_walk::particles = parts.data();
+    bind(sh_walk::processed_buffer, const_cast<float*>(processed), (int64_t)p->pic_nrows * p->pic_ncols);
+    bind(sh_walk::particles, parts.data(), (int64_t)parts.size());
     sh_walk::n_particles = (uint32_t)n;
     sh_walk::n_particles_filtered = 0;
-    sh_walk::results = res.data();
-    sh_walk::raw_frame = const_cast<float*>(raw);
+    bind(sh_walk::results, res.data(), (int64_t)res.size());
+    bind(sh_walk::raw_frame, const_cast<float*>(raw), (int64_t)p->pic_nrows * p->pic_ncols);
     sh_walk::image_std = pic_std;
     sh_walk::next_dispatch = {};
     for (int64_t i = 0; i < n; i++) sh_walk::main_(uvec3{(uint32_t)i, 0u, 0u});
@@ -172,10 +198,10 @@ int64_t ref_walk(const RefParams* p, const float* processed, const float* raw, c
         std::vector<sh_characterize::ResultRow> cr((size_t)nk + 1);
         std::memcpy(cr.data(), res.data(), (size_t)nk * sizeof(sh_walk::ResultRow));
         set_params(sh_characterize::params, p);
-        sh_characterize::processed_buffer = const_cast<float*>(processed);
-        sh_characterize::raw_frame = const_cast<float*>(raw);
+        bind(sh_characterize::processed_buffer, const_cast<float*>(processed), (int64_t)p->pic_nrows * p->pic_ncols);
+        bind(sh_characterize::raw_frame, const_cast<float*>(raw), (int64_t)p->pic_nrows * p->pic_ncols);
         sh_characterize::n_particles = (uint32_t)nk;
-        sh_characterize::results = cr.data();
+        bind(sh_characterize::results, cr.data(), (int64_t)cr.size());
         for (int64_t i = 0; i < nk; i++) sh_characterize::main_(uvec3{(uint32_t)i, 0u, 0u});
         std::memcpy(res.data(), cr.data(), (size_t)nk * sizeof(sh_walk::ResultRow));
     }
@@ -189,10 +215,10 @@ int ref_characterize_points(const RefParams* p, const float* processed, const fl
     std::vector<sh_characterize_points::ResultRow> cr((size_t)n + 1);
     std::memcpy(cr.data(), rows_inout, (size_t)n * 10 * sizeof(float));
     set_params(sh_characterize_points::params, p);
-    sh_characterize_points::processed_buffer = const_cast<float*>(processed);
-    sh_characterize_points::raw_frame = const_cast<float*>(raw);
+    bind(sh_characterize_points::processed_buffer, const_cast<float*>(processed), (int64_t)p->pic_nrows * p->pic_ncols);
+    bind(sh_characterize_points::raw_frame, const_cast<float*>(raw), (int64_t)p->pic_nrows * p->pic_ncols);
     sh_characterize_points::n_particles = (uint32_t)n;
-    sh_characterize_points::results = cr.data();
+    bind(sh_characterize_points::results, cr.data(), (int64_t)cr.size());
     for (int64_t i = 0; i < n; i++) sh_characterize_points::main_(uvec3{(uint32_t)i, 0u, 0u});
     std::memcpy(rows_inout, cr.data(), (size_t)n * 10 * sizeof(float));
     return 0;
@@ -204,15 +230,15 @@ int ref_laplace(const RefParams* p, const float* frame, float sigma, float* fina
     const int32_t H = p->pic_nrows, W = p->pic_ncols;
     std::vector<float> temp2((size_t)H * W), temp1((size_t)H * W);
     set_params(sh_separable_log::params, p);
-    sh_separable_log::final_output = final_out;
+    bind(sh_separable_log::final_output, final_out, (int64_t)H * W);
     for (uint32_t diff_dim = 0; diff_dim < 2; diff_dim++) {
         sh_separable_log::pc = {0u, diff_dim, sigma};
-        sh_separable_log::input = const_cast<float*>(frame);
-        sh_separable_log::output = temp2.data();
+        bind(sh_separable_log::input, const_cast<float*>(frame), (int64_t)H * W);
+        bind(sh_separable_log::output, temp2.data(), (int64_t)H * W);
         dispatch2d(H, W, [](uvec3 g) { sh_separable_log::main_(g); });
         sh_separable_log::pc = {1u, diff_dim, sigma};
-        sh_separable_log::input = temp2.data();
-        sh_separable_log::output = temp1.data();
+        bind(sh_separable_log::input, temp2.data(), (int64_t)H * W);
+        bind(sh_separable_log::output, temp1.data(), (int64_t)H * W);
         dispatch2d(H, W, [](uvec3 g) { sh_separable_log::main_(g); });
     }
     return 0;
@@ -224,14 +250,14 @@ int64_t ref_logspace_max(const RefParams* p, const float* bottom, const float* m
     const int32_t H = p->pic_nrows, W = p->pic_ncols;
     std::vector<sh_logspace_max::ParticleLocation> pts((size_t)H * W + 1);
     set_params(sh_logspace_max::params, p);
-    sh_logspace_max::bottom = const_cast<float*>(bottom);
-    sh_logspace_max::middle = const_cast<float*>(middle);
-    sh_logspace_max::top = const_cast<float*>(top);
+    bind(sh_logspace_max::bottom, const_cast<float*>(bottom), (int64_t)H * W);
+    bind(sh_logspace_max::middle, const_cast<float*>(middle), (int64_t)H * W);
+    bind(sh_logspace_max::top, const_cast<float*>(top), (int64_t)H * W);
     sh_logspace_max::n_particles = 0;
-    sh_logspace_max::particles = pts.data();
+    bind(sh_logspace_max::particles, pts.data(), (int64_t)pts.size());
     sh_logspace_max::wg_size = {};
     sh_logspace_max::std_pic = pic_std;
-    sh_logspace_max::processed = const_cast<float*>(processed);
+    bind(sh_logspace_max::processed, const_cast<float*>(processed), (int64_t)H * W);
     sh_logspace_max::pc = {edge, radius};
     dispatch2d(H, W, [](uvec3 g) { sh_logspace_max::main_(g); });
     int64_t n = sh_logspace_max::n_particles;

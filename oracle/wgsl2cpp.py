@@ -21,7 +21,9 @@ Translation rules (the WGSL subset used by these shaders):
     compiled with -ffp-contract=off).
   * Storage/uniform/push-constant bindings become namespace-scope variables
     the driver sets; atomics become plain sequential increments (the driver
-    dispatches invocations serially in row-major order).
+    dispatches invocations serially in row-major order); storage arrays are
+    bounds-checked (WGSL robust buffer access: reads outside the buffer give
+    zero, writes outside it are dropped).
 
 Usage: wgsl2cpp.py <reference_root> <out_dir>
 """
@@ -60,7 +62,9 @@ def ctype(t):
         return TYPE_MAP[t]
     m = re.fullmatch(r"array<(.+)>", t)
     if m:
-        return ctype(m.group(1)) + "*"
+        # storage arrays keep WGSL's robust buffer access: out-of-range reads
+        # return zero, out-of-range writes are dropped
+        return "RobustArray<%s>" % ctype(m.group(1))
     return t  # user struct
 
 
