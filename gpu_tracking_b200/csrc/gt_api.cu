@@ -1110,6 +1110,11 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
 // =================================================================== C ABI
 extern "C" {
 
+// internal accessors for the other translation units (not exported)
+int gt__ctx_device(const gt_ctx* ctx) { return ctx->device; }
+cudaStream_t gt__ctx_stream(const gt_ctx* ctx) { return ctx->st; }
+void gt__ctx_set_error(gt_ctx* ctx, const char* msg) { ctx->err = msg; }
+
 const char* gt_version(void) { return "gpu_tracking_b200 0.1 (sm_100a)"; }
 
 void gt_params_default(gt_params* p) {

@@ -197,6 +197,23 @@ GT_API gt_status gt_connect(gt_ctx* ctx, const float* frame_y_x1, int64_t n1,
 GT_API gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype,
                         int64_t T, int32_t H, int32_t W, float* out);
 
+/*
+ * Link detections that are already in device memory without allocating any
+ * device memory.  No counterpart in the reference: it exists for callers that
+ * cannot allocate while they run — a live acquisition loop linking each batch
+ * of detections as frames arrive (cudaMalloc/cudaFree synchronise the device
+ * and would stall it), or a process whose device memory belongs to another
+ * allocator.  d_frame_y_x is (n, 3) float32 [frame, y, x] rows sorted by frame
+ * on the context's device; d_particle_out receives n int64 ids on that device;
+ * the ids equal gt_link's.  Working memory is one static device array shared
+ * by all calls (limits: n <= 32768, <= 4096 detections per frame, memory <= 3;
+ * larger inputs return GT_ERR_CAPACITY_EXCEEDED), so calls whose GPU work
+ * overlaps race on it.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture.
+ */
+GT_API gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_frame_y_x, int64_t n, float search_range,
+                                 uint32_t memory, int64_t* d_particle_out);
+
 /* Library version string. */
 GT_API const char* gt_version(void);
 
