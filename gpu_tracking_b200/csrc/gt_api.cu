@@ -14,11 +14,14 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -54,6 +57,61 @@ struct DBuf {
     }
 };
 
+// Result tables come and go with every call: their columns are stream-ordered
+// allocations from one pool per device that keeps its memory, so a call
+// neither maps fresh device memory nor synchronises the device to free it.
+cudaMemPool_t table_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = pool;
+    return pool;
+}
+
+struct TBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;   // the call's compute stream
+    TBuf() = default;
+    TBuf(const TBuf&) = delete;
+    TBuf& operator=(const TBuf&) = delete;
+    // a table is freed only when no work on it is pending
+    ~TBuf() {
+        if (p) cudaFreeAsync(p, cudaStreamPerThread);
+    }
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n && p) return cudaSuccess;
+        if (p) cudaFreeAsync(p, stream);
+        p = nullptr;
+        n = 0;
+        const size_t want = std::max<size_t>(bytes, 256);
+        cudaMemPool_t pool = table_pool(device);
+        if (!pool) return cudaErrorMemoryAllocation;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, stream);
+        if (e == cudaSuccess) n = want;
+        return e;
+    }
+    template <class T>
+    T* as() const {
+        return (T*)p;
+    }
+};
+
 struct KernelStat {
     int64_t launches = 0;
     double ms = 0.0;
@@ -65,6 +123,8 @@ struct gt_ctx {
     int device = 0;
     cudaStream_t st = nullptr;   // compute
     cudaStream_t cp = nullptr;   // host -> device copies
+    cudaStream_t lk = nullptr;   // linking of located frames, overlapped with locating
+    cudaEvent_t located = nullptr, linked = nullptr;
     cudaEvent_t used[2] = {nullptr, nullptr};    // compute finished with staging buffer b
     cudaEvent_t filled[2] = {nullptr, nullptr};  // staging buffer b holds its chunk
     std::string err;
@@ -81,6 +141,11 @@ struct gt_ctx {
         fin_scratch, flags, ident, tabs_f, tabs_i, tabs_s, tabs_m, row_off, frame_num;
     DBuf l_srt, l_sortscr, l_fcnt, l_bcnt, l_foff, l_boff, l_fpts, l_bpts, l_bdist, l_scan, l_scratch, l_ids, l_cnt,
         l_dur, l_flags, l_goff, l_pgroup, l_vgrp, l_reset, l_vpoff, l_px, l_py, l_ge, l_rowdur, l_part;
+    // windowed linking inside gt_batch (slot mode)
+    DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
+        w_cnt, w_flags, w_vgrp, w_reset;
+    int64_t w_list_cap = 0;   // entries of each window neighbour-list buffer (0 = not sized yet)
+    int64_t w_edge_cap = 0;   // backward edges per frame the window scratch holds
     uint32_t cand_cap = 16384;
     uint32_t feat_cap = 4096;
 };
@@ -88,9 +153,19 @@ struct gt_ctx {
 struct gt_table {
     int device = 0;
     int64_t n = 0;
-    DBuf frame, particle, duration;
-    DBuf col[GT_NUM_COLUMNS];
+    TBuf frame, particle, duration;
+    TBuf col[GT_NUM_COLUMNS];
     bool has[GT_NUM_COLUMNS] = {};
+    gt_table(int dev, cudaStream_t st) : device(dev) {
+        for (TBuf* b : {&frame, &particle, &duration}) {
+            b->device = dev;
+            b->stream = st;
+        }
+        for (auto& b : col) {
+            b.device = dev;
+            b.stream = st;
+        }
+    }
 };
 
 namespace {
@@ -125,13 +200,14 @@ gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
 struct Prof {
     gt_ctx* ctx;
     const char* name;
+    cudaStream_t stream;
     cudaEvent_t a = nullptr, b = nullptr;
-    Prof(gt_ctx* c, const char* n) : ctx(c), name(n) {
+    Prof(gt_ctx* c, const char* n, cudaStream_t s = nullptr) : ctx(c), name(n), stream(s ? s : c->st) {
         ctx->launch_count[name]++;
         if (!ctx->profile) return;
         a = take();
         b = take();
-        cudaEventRecord(a, ctx->st);
+        cudaEventRecord(a, stream);
     }
     cudaEvent_t take() {
         if (!ctx->event_pool.empty()) {
@@ -145,15 +221,40 @@ struct Prof {
     }
     ~Prof() {
         if (!ctx->profile) return;
-        cudaEventRecord(b, ctx->st);
+        cudaEventRecord(b, stream);
         ctx->pending.push_back({name, {a, b}});
     }
 };
 
-void drain_profile(gt_ctx* ctx) {
-    for (auto& p : ctx->pending) {
+// Host wall-clock of one phase of a call, accumulated under `name` next to
+// the kernels' device times when profiling is on (gaps between kernels are
+// host work: allocation, uploads, read-backs).
+struct HostSpan {
+    gt_ctx* ctx;
+    const char* name;
+    std::chrono::steady_clock::time_point t0;
+    HostSpan(gt_ctx* c, const char* n) : ctx(c), name(n), t0(std::chrono::steady_clock::now()) {}
+    ~HostSpan() {
+        if (!ctx->profile) return;
+        auto& s = ctx->stats[name];
+        s.launches++;
+        s.ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+// Folds finished launches into the statistics; with block, waits for all.
+void drain_profile(gt_ctx* ctx, bool block = true) {
+    size_t keep = 0;
+    for (size_t i = 0; i < ctx->pending.size(); i++) {
+        auto& p = ctx->pending[i];
+        if (block) {
+            cudaEventSynchronize(p.second.second);
+        } else if (cudaEventQuery(p.second.second) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->pending[keep++] = p;
+            continue;
+        }
         float ms = 0.0f;
-        cudaEventSynchronize(p.second.second);
         cudaEventElapsedTime(&ms, p.second.first, p.second.second);
         auto& s = ctx->stats[p.first];
         s.launches++;
@@ -161,7 +262,7 @@ void drain_profile(gt_ctx* ctx) {
         ctx->event_pool.push_back(p.second.first);
         ctx->event_pool.push_back(p.second.second);
     }
-    ctx->pending.clear();
+    ctx->pending.resize(keep);
 }
 
 // ------------------------------------------------------- derived parameters
@@ -388,6 +489,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     const int nvideos = (int)job.vgrp.size() - 1;
     const int64_t N = job.goff.back();
     const int K = job.memory + 1;
+    std::unique_ptr<HostSpan> hs(new HostSpan(ctx, "host_link_prep"));
     int max_group = 0;
     for (int g = 0; g < ngroups; g++) max_group = std::max<int64_t>(max_group, job.goff[g + 1] - job.goff[g]);
     std::vector<int32_t> pgroup(N);
@@ -440,6 +542,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
                                      (int64_t)NK + 1, ctx->st));
     CK(cub::DeviceScan::ExclusiveSum(ctx->l_scan.p, tmp_bytes, ctx->l_bcnt.as<int64_t>(), ctx->l_boff.as<int64_t>(),
                                      (int64_t)NK + 1, ctx->st));
+    hs.reset(new HostSpan(ctx, "host_link_counts"));
     int64_t ftot = 0, btot = 0;
     CK(cudaMemcpyAsync(&ftot, ctx->l_foff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&btot, ctx->l_boff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -450,6 +553,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
         CK(cudaMemcpyAsync(&boff_at[g], ctx->l_boff.as<int64_t>() + job.goff[g] * K, 8, cudaMemcpyDeviceToHost,
                            ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    hs.reset(new HostSpan(ctx, "host_link_run"));
     int64_t max_edges = 1;
     for (int g = 0; g < ngroups; g++) max_edges = std::max(max_edges, boff_at[g + 1] - boff_at[g]);
     CK(ctx->l_fpts.ensure(std::max<int64_t>(ftot, 1) * 4));
@@ -473,6 +577,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     S.max_group = std::max(max_group, 1);
     S.max_edges = max_edges;
     S.bytes_per_video = link_scratch_bytes(S.max_group, S.max_edges, max_np, job.memory);
+    S.max_points = max_np;
     CK(ctx->l_scratch.ensure(S.bytes_per_video * nvideos));
     S.base = ctx->l_scratch.as<uint8_t>();
     LinkOutput out;
@@ -505,6 +610,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
         counters->resize(nvideos);
         CK(cudaMemcpy(counters->data(), out.counter, nvideos * 8, cudaMemcpyDeviceToHost));
     }
+    hs.reset(new HostSpan(ctx, "host_link_durations"));
     if (row_dur) {
         {
             Prof pf(ctx, "link_durations");
@@ -526,6 +632,154 @@ __global__ void f32_round_ids_kernel(const int64_t* ids, int64_t* out, int64_t n
     if (i < n) out[i] = (int64_t)(float)ids[i];
 }
 
+// Windowed linking inside gt_batch.  Every super-chunk of located frames is
+// linked on the link stream while the next super-chunk is being located, so
+// the linker's sequential frame loop runs beside the locate kernels instead
+// of after them.  The detections are read in place from their per-frame
+// slots (feats_out / kept_count, slot stride = feat_cap); each window builds
+// the neighbour lists of its frames and of the memory+1 frames before it, and
+// the linker's state (memory ring, stamps, id counter) carries over in its
+// scratch from one window to the next, so ids and durations are those of the
+// whole-video linker.  A window whose list or edge buffers are too small
+// stops the video (kFlagListOverflow / kFlagEdgeOverflow); the call then
+// links the finished table with the whole-video linker and the buffers grow
+// for the next call.
+struct PipeLink {
+    gt_ctx* ctx = nullptr;
+    LinkInput in;
+    LinkScratch S;
+    LinkOutput out;
+    int K = 1;
+    int64_t C = 0, list_cap = 0, max_items = 0;
+    size_t scan_bytes = 0;
+
+    gt_status setup(gt_ctx* c, int64_t NT, uint32_t feat_cap, int SC, float radius, int memory,
+                    const std::vector<uint8_t>& reset) {
+        ctx = c;
+        C = feat_cap;
+        K = memory + 1;
+        const int64_t NS = NT * C;
+        max_items = (int64_t)(SC + K) * C * K + 1;
+        if (ctx->w_list_cap <= 0) ctx->w_list_cap = std::max<int64_t>(max_items, 1 << 20);
+        if (ctx->w_edge_cap <= 0) ctx->w_edge_cap = std::max<int64_t>(C * 16, 1 << 16);
+        list_cap = ctx->w_list_cap;
+        CK(ctx->w_srt.ensure(NS * 4));
+        CK(ctx->w_fcnt.ensure(max_items * 8));
+        CK(ctx->w_bcnt.ensure(max_items * 8));
+        CK(ctx->w_foff.ensure(max_items * 8));
+        CK(ctx->w_boff.ensure(max_items * 8));
+        CK(ctx->w_fpts.ensure(list_cap * 4));
+        CK(ctx->w_bpts.ensure(list_cap * 4));
+        CK(ctx->w_bdist.ensure(list_cap * 4));
+        CK(ctx->w_ids.ensure(NS * 8));
+        CK(ctx->w_dur.ensure(NS * 8));
+        CK(ctx->w_state.ensure(sizeof(LinkState)));
+        CK(ctx->w_cnt.ensure(8));
+        CK(ctx->w_flags.ensure(4));
+        CK(ctx->w_vgrp.ensure(8));
+        CK(ctx->w_reset.ensure(std::max<int64_t>(NT, 1)));
+        S.max_group = (int32_t)C;
+        S.max_edges = ctx->w_edge_cap;
+        S.max_points = NS;
+        S.bytes_per_video = link_scratch_bytes(S.max_group, S.max_edges, NS, memory);
+        CK(ctx->w_scratch.ensure(S.bytes_per_video));
+        S.base = ctx->w_scratch.as<uint8_t>();
+        scan_bytes = 0;
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, ctx->w_fcnt.as<int64_t>(), ctx->w_foff.as<int64_t>(),
+                                         max_items, ctx->lk));
+        CK(ctx->w_scan.ensure(scan_bytes));
+
+        const int32_t vg[2] = {0, (int32_t)NT};
+        CK(cudaMemcpyAsync(ctx->w_vgrp.p, vg, sizeof(vg), cudaMemcpyHostToDevice, ctx->lk));
+        CK(cudaMemcpyAsync(ctx->w_reset.p, reset.data(), NT, cudaMemcpyHostToDevice, ctx->lk));
+        // the per-point linker arrays start cleared: stamps -1, first positions 0
+        size_t o_id, o_src, o_first;
+        link_scratch_point_arrays(S.max_group, S.max_edges, NS, memory, &o_id, &o_src, &o_first);
+        CK(cudaMemsetAsync(S.base + o_id, 0xFF, NS * 4, ctx->lk));
+        CK(cudaMemsetAsync(S.base + o_src, 0xFF, NS * 4, ctx->lk));
+        CK(cudaMemsetAsync(S.base + o_first, 0, NS * 8, ctx->lk));
+        CK(cudaMemsetAsync(ctx->w_flags.p, 0, 4, ctx->lk));
+        CK(cudaMemsetAsync(ctx->w_cnt.p, 0, 8, ctx->lk));
+        // the host buffers above are read before the call returns
+        CK(cudaStreamSynchronize(ctx->lk));
+
+        in = LinkInput();
+        const float* f = (const float*)ctx->feats_out.p;
+        in.px = f + offsetof(Feature, x) / 4;
+        in.py = f + offsetof(Feature, y) / 4;
+        in.xy_stride = (int32_t)(sizeof(Feature) / 4);
+        in.gcount = ctx->kept_count.as<uint32_t>();
+        in.slot_stride = C;
+        in.vgrp = ctx->w_vgrp.as<int32_t>();
+        in.reset = ctx->w_reset.as<uint8_t>();
+        in.ngroups = (int32_t)NT;
+        in.nvideos = 1;
+        in.npoints = NS;
+        in.radius = radius;
+        in.memory = memory;
+        out.ids = ctx->w_ids.as<int64_t>();
+        out.counter = ctx->w_cnt.as<int64_t>();
+        out.dur = ctx->w_dur.as<int64_t>();
+        out.vpoff = nullptr;
+        out.flags = ctx->w_flags.as<uint32_t>();
+        return GT_OK;
+    }
+
+    // frames [s0, s1) have been located on the compute stream
+    gt_status window(int s0, int s1, bool first, bool last) {
+        const int LA = std::max(0, s0 - K);
+        const int64_t p0 = (int64_t)LA * C, p1 = (int64_t)s1 * C;
+        const int64_t items = (p1 - p0) * K + 1;
+        if (items > max_items) return set_err(ctx, GT_ERR_INTERNAL, "link window larger than its buffers");
+        CK(cudaEventRecord(ctx->located, ctx->st));
+        CK(cudaStreamWaitEvent(ctx->lk, ctx->located, 0));
+        in.groups_ready = s1;
+        uint32_t* srt = ctx->w_srt.as<uint32_t>();
+        {
+            Prof pf(ctx, "link_sort", ctx->lk);
+            CK(link_sort_groups_range(in, srt, s0, s1, ctx->lk));
+        }
+        CK(cudaMemsetAsync(ctx->w_fcnt.p, 0, items * 8, ctx->lk));
+        CK(cudaMemsetAsync(ctx->w_bcnt.p, 0, items * 8, ctx->lk));
+        {
+            Prof pf(ctx, "link_lists", ctx->lk);
+            CK(link_count_lists_range(in, srt, p0, p1, ctx->w_fcnt.as<int64_t>(), ctx->w_bcnt.as<int64_t>(),
+                                      out.flags, ctx->lk));
+        }
+        size_t tb = scan_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, ctx->w_fcnt.as<int64_t>(), ctx->w_foff.as<int64_t>(),
+                                         items, ctx->lk));
+        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, ctx->w_bcnt.as<int64_t>(), ctx->w_boff.as<int64_t>(),
+                                         items, ctx->lk));
+        LinkLists L;
+        L.f_off = ctx->w_foff.as<int64_t>();
+        L.b_off = ctx->w_boff.as<int64_t>();
+        L.f_pts = ctx->w_fpts.as<int32_t>();
+        L.b_pts = ctx->w_bpts.as<int32_t>();
+        L.b_dist = ctx->w_bdist.as<float>();
+        L.srt = srt;
+        L.pbase = p0;
+        L.f_cap = list_cap;
+        L.b_cap = list_cap;
+        {
+            Prof pf(ctx, "link_lists", ctx->lk);
+            CK(link_fill_lists_range(in, L, p1, out.flags, ctx->lk));
+        }
+        LinkWindow w;
+        w.g0 = s0;
+        w.g1 = s1;
+        w.first = first ? 1 : 0;
+        w.last = last ? 1 : 0;
+        w.init_points = 0;
+        w.state = (LinkState*)ctx->w_state.p;
+        {
+            Prof pf(ctx, "link_video", ctx->lk);
+            CK(link_run_window(in, L, S, out, w, ctx->lk));
+        }
+        return GT_OK;
+    }
+};
+
 // --------------------------------------------------------------- locate
 struct Chunking {
     int F;
@@ -542,7 +796,8 @@ int pick_chunk(int64_t T, int32_t H, int32_t W, int n_planes) {
 
 template <typename T>
 gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
-                      int32_t W, const LocateConsts& c, const LogTables* lt, int F, uint32_t* out_flags) {
+                      int32_t W, const LocateConsts& c, const LogTables* lt, int F, uint32_t* out_flags,
+                      PipeLink* pl, const std::vector<uint8_t>* reset) {
     const size_t npx = (size_t)H * W;
     const bool log_style = (p.style == GT_STYLE_LOG);
     const int nslots = log_style ? (int)lt->radii.size() : 1;
@@ -562,6 +817,7 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     CK(ctx->kept_count.ensure((size_t)NT * 4));
     CK(ctx->flags.ensure(16));
     CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
+    if (pl) CKS(pl->setup(ctx, NT, feat_cap, SC, p.search_range, (int)p.memory, *reset));
     // finalize scratch for frames with more detections than shared memory sorts
     size_t fin_per_frame = 0;
     if (feat_cap > (uint32_t)kFinalizeSmemSort) {
@@ -663,6 +919,7 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         if (interrupted(ctx)) {
             cudaStreamSynchronize(ctx->st);
             cudaStreamSynchronize(ctx->cp);
+            cudaStreamSynchronize(ctx->lk);
             return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
         }
         const int64_t s0 = (int64_t)sc * SC;
@@ -720,11 +977,12 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                                   ctx->tabs_m.as<int4>(), flags, ns, ctx->st));
         }
         if (!on_device) CK(cudaEventRecord(ctx->used[sc & 1], ctx->st));
+        if (pl) CKS(pl->window((int)s0, (int)(s0 + ns), sc == 0, sc == nsuper - 1));
         ctx->done = s0 + ns;
     }
     CK(cudaMemcpyAsync(out_flags, flags, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    drain_profile(ctx);
+    drain_profile(ctx, false);
     return GT_OK;
 }
 
@@ -791,10 +1049,28 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
     const int F = pick_chunk(NT, H, W, log_style ? (int)lt.radii.size() : 0);
     ctx->total = NT;
     ctx->done = 0;
+    std::vector<int64_t> fnum(NT);
+    for (int64_t t = 0; t < NT; t++) fnum[t] = frame_numbers ? frame_numbers[t] : t;
+    std::vector<uint8_t> reset(NT, 0);
+    for (int64_t t = 0; t < NT; t++)
+        for (int64_t k = 0; k < n_reset; k++)
+            if (reset_points[k] == fnum[t]) reset[t] = 1;
+    PipeLink pl;
+    bool windowed = false;
     for (int attempt = 0;; attempt++) {
         uint32_t fl = 0;
-        CKS(locate_pass<T>(ctx, p, frames, on_device, NT, H, W, c, log_style ? &lt : nullptr, F, &fl));
+        HostSpan hs(ctx, "host_locate");
+        // frames link while later frames are located when every frame's
+        // detections sort in shared memory (the group sort's limit)
+        windowed = p.has_search_range && ctx->feat_cap <= 4096u;
+        gt_status st = locate_pass<T>(ctx, p, frames, on_device, NT, H, W, c, log_style ? &lt : nullptr, F, &fl,
+                                      windowed ? &pl : nullptr, &reset);
+        if (st != GT_OK) {
+            cudaStreamSynchronize(ctx->lk);
+            return st;
+        }
         if (!(fl & (kFlagCandOverflow | kFlagFeatOverflow))) break;
+        CK(cudaStreamSynchronize(ctx->lk));
         const uint64_t npx = (uint64_t)H * W;
         if (attempt > 8) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame capacity exceeded");
         if (fl & kFlagCandOverflow) {
@@ -810,39 +1086,77 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
             ctx->feat_cap = (uint32_t)nf;
         }
     }
-    std::vector<int64_t> fnum(NT);
-    for (int64_t t = 0; t < NT; t++) fnum[t] = frame_numbers ? frame_numbers[t] : t;
     std::vector<int64_t> row_off;
-    CKS(assemble_table(ctx, NT, fnum, log_style, tab, row_off));
+    {
+        HostSpan hs(ctx, "host_assemble");
+        gt_status st = assemble_table(ctx, NT, fnum, log_style, tab, row_off);
+        if (st != GT_OK) {
+            cudaStreamSynchronize(ctx->lk);
+            return st;
+        }
+    }
     if (p.has_search_range) {
-        LinkJob job;
-        job.goff = row_off;
-        job.vgrp = {0, (int32_t)NT};
-        job.reset.assign(NT, 0);
-        for (int64_t t = 0; t < NT; t++)
-            for (int64_t k = 0; k < n_reset; k++)
-                if (reset_points[k] == fnum[t]) job.reset[t] = 1;
-        job.radius = p.search_range;
-        job.memory = (int32_t)p.memory;
+        HostSpan hs(ctx, "host_link");
         const size_t n1 = std::max<int64_t>(tab->n, 1);
-        CK(ctx->l_ids.ensure(n1 * 8));
         CK(tab->particle.ensure(n1 * 8));
         CK(tab->duration.ensure(n1 * 8));
-        CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
-                     ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
-        if (tab->n > 0) {
-            Prof pf(ctx, "round_ids");
-            f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
-                ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+        bool whole = !windowed;
+        if (windowed) {
+            // the table rows take the windowed linker's ids and durations
+            CK(cudaEventRecord(ctx->linked, ctx->lk));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->linked, 0));
+            {
+                Prof pf(ctx, "link_rows");
+                CK(link_slot_rows(pl.in, pl.out, ctx->row_off.as<int64_t>(), tab->particle.as<int64_t>(),
+                                  tab->duration.as<int64_t>(), ctx->st));
+            }
+            uint32_t lf = 0;
+            CK(cudaMemcpyAsync(&lf, pl.out.flags, 4, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            if (lf & kFlagTooDense)
+                return set_err(ctx, GT_ERR_TOO_DENSE_TO_LINK,
+                               "computational load during linking is abnormally high. try setting a smaller search "
+                               "range or track with settings that give fewer detections.");
+            if (lf & kFlagSubnetBudget)
+                return set_err(ctx, GT_ERR_SUBNET_TOO_EXPENSIVE, "a linking subnet exceeded the device search budget");
+            if (lf & (kFlagListOverflow | kFlagEdgeOverflow)) {
+                // buffers too small for this video: grow them for the next
+                // call and link this one with the whole-video linker
+                if (lf & kFlagListOverflow) ctx->w_list_cap *= 4;
+                if (lf & kFlagEdgeOverflow) ctx->w_edge_cap *= 4;
+                whole = true;
+            } else if (lf & kFlagScratch) {
+                return set_err(ctx, GT_ERR_INTERNAL,
+                               "a particle id has no duration entry after a linker reset (the reference panics here)");
+            }
         }
-        CK(cudaGetLastError());
+        if (whole) {
+            LinkJob job;
+            job.goff = row_off;
+            job.vgrp = {0, (int32_t)NT};
+            job.reset = reset;
+            job.radius = p.search_range;
+            job.memory = (int32_t)p.memory;
+            CK(ctx->l_ids.ensure(n1 * 8));
+            CKS(run_link(ctx, job, tab->col[GT_COL_Y].as<float>(), tab->col[GT_COL_X].as<float>(),
+                         ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
+            if (tab->n > 0) {
+                Prof pf(ctx, "round_ids");
+                f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
+                    ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+            }
+            CK(cudaGetLastError());
+        }
         tab->has[GT_COL_PARTICLE] = true;
         tab->has[GT_COL_DURATION] = true;
     }
     if (!p.doughnut_correction) {
         tab->has[GT_COL_RAW_MASS] = tab->has[GT_COL_RAW_BG_MEDIAN] = tab->has[GT_COL_RAW_MASS_CORRECTED] = false;
     }
-    CK(cudaStreamSynchronize(ctx->st));
+    {
+        HostSpan hs(ctx, "host_tail_sync");
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     drain_profile(ctx);
     return GT_OK;
 }
@@ -1115,6 +1429,17 @@ int gt__ctx_device(const gt_ctx* ctx) { return ctx->device; }
 cudaStream_t gt__ctx_stream(const gt_ctx* ctx) { return ctx->st; }
 void gt__ctx_set_error(gt_ctx* ctx, const char* msg) { ctx->err = msg; }
 
+// Test hook (exported, not part of the public header): the entries of each
+// windowed-linking neighbour-list buffer and the backward edges per frame its
+// scratch holds; values <= 0 restore the defaults.  Small values make gt_batch
+// take its fallback to the whole-video linker.
+GT_API gt_status gt__set_link_window_caps(gt_ctx* ctx, int64_t list_entries, int64_t edges_per_frame) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    ctx->w_list_cap = list_entries;
+    ctx->w_edge_cap = edges_per_frame;
+    return GT_OK;
+}
+
 const char* gt_version(void) { return "gpu_tracking_b200 0.1 (sm_100a)"; }
 
 void gt_params_default(gt_params* p) {
@@ -1147,7 +1472,10 @@ gt_status gt_create(int32_t device, gt_ctx** out) {
     gt_ctx* ctx = new gt_ctx();
     ctx->device = device;
     if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->lk, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->located, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->linked, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
         return GT_ERR_CUDA;
     }
@@ -1164,14 +1492,18 @@ void gt_destroy(gt_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->st);
     cudaStreamSynchronize(ctx->cp);
+    cudaStreamSynchronize(ctx->lk);
     drain_profile(ctx);
     for (auto e : ctx->event_pool) cudaEventDestroy(e);
     for (int i = 0; i < 2; i++) {
         cudaEventDestroy(ctx->used[i]);
         cudaEventDestroy(ctx->filled[i]);
     }
+    cudaEventDestroy(ctx->located);
+    cudaEventDestroy(ctx->linked);
     cudaStreamDestroy(ctx->st);
     cudaStreamDestroy(ctx->cp);
+    cudaStreamDestroy(ctx->lk);
     delete ctx;
 }
 
@@ -1204,7 +1536,7 @@ gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst) {
     cudaSetDevice(t->device);
     if (column == GT_COL_FRAME || column == GT_COL_PARTICLE || column == GT_COL_DURATION) {
         std::vector<int64_t> v(t->n);
-        const DBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
+        const TBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
         if (cudaMemcpy(v.data(), b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
         for (int64_t i = 0; i < t->n; i++) dst[i] = (float)v[i];
         return GT_OK;
@@ -1220,7 +1552,7 @@ gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst) {
     if (!t->has[column]) return GT_ERR_INVALID_ARGUMENT;
     if (t->n == 0) return GT_OK;
     cudaSetDevice(t->device);
-    const DBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
+    const TBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
     if (cudaMemcpy(dst, b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
     return GT_OK;
 }
@@ -1239,8 +1571,7 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
     CKS(validate(ctx, params, frames, dtype, T, H, W));
     bool on_device = false;
     CKS(check_frames_ptr(ctx, frames, &on_device));
-    std::unique_ptr<gt_table> tab(new gt_table());
-    tab->device = ctx->device;
+    std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
     gt_status st;
     if (dtype == GT_DTYPE_U16)
         st = batch_impl<uint16_t>(ctx, *params, (const uint16_t*)frames, on_device, T, H, W, frame_numbers,
@@ -1251,7 +1582,12 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
     else
         st = batch_impl<uint8_t>(ctx, *params, (const uint8_t*)frames, on_device, T, H, W, frame_numbers,
                                  linker_reset_points, n_reset, tab.get());
-    if (st != GT_OK) return st;
+    if (st != GT_OK) {
+        // no kernel may still write the table when its columns go back to the pool
+        cudaStreamSynchronize(ctx->st);
+        cudaStreamSynchronize(ctx->lk);
+        return st;
+    }
     *out = tab.release();
     return GT_OK;
 }
@@ -1265,8 +1601,7 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const voi
     if (n_points > 0 && !points) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null points");
     bool on_device = false;
     CKS(check_frames_ptr(ctx, frames, &on_device));
-    std::unique_ptr<gt_table> tab(new gt_table());
-    tab->device = ctx->device;
+    std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
     gt_status st;
     if (dtype == GT_DTYPE_U16)
         st = charpoints_impl<uint16_t>(ctx, *params, (const uint16_t*)frames, on_device, T, H, W, points, n_points,
@@ -1277,7 +1612,12 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const voi
     else
         st = charpoints_impl<uint8_t>(ctx, *params, (const uint8_t*)frames, on_device, T, H, W, points, n_points,
                                       has_frames, has_r, tab.get());
-    if (st != GT_OK) return st;
+    if (st != GT_OK) {
+        // no kernel may still write the table when its columns go back to the pool
+        cudaStreamSynchronize(ctx->st);
+        cudaStreamSynchronize(ctx->lk);
+        return st;
+    }
     *out = tab.release();
     return GT_OK;
 }

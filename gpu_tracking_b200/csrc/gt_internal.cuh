@@ -31,7 +31,11 @@ enum : uint32_t {
     kFlagTooDense = 4u,
     kFlagSubnetBudget = 8u,
     kFlagScratch = 16u,
+    kFlagListOverflow = 32u,   // windowed linking: a neighbour list buffer is full
+    kFlagEdgeOverflow = 64u,   // windowed linking: a frame has more edges than the scratch holds
 };
+// Linker flags after which the remaining frames of a video are not linked.
+constexpr uint32_t kLinkStopFlags = 4u | 8u | 16u | 32u | 64u;
 
 // Derived parameters of the trackpy locate pipeline
 // (gpuparams_from_tracking_params, src/gpu_setup.rs:528-580).

@@ -94,28 +94,41 @@ template <typename T>
 cudaError_t launch_mean_frame(const T* frames, int64_t T_, int64_t npix, float* out, cudaStream_t st);
 
 // Linking --------------------------------------------------------------
+// Points are addressed in one of two ways:
+//   compact   point p of group g is p in [goff[g], goff[g+1]) and its
+//             coordinates are px[p], py[p] (table columns);
+//   slot      point j of group g is p = g*slot_stride + j, j < gcount[g], and
+//             its coordinates are px[p*xy_stride] (per-frame result slots,
+//             read in place while later frames are still being located).
 struct LinkInput {
-    const float* px;          // row coordinate of every point ("y" column)
-    const float* py;          // column coordinate ("x" column)
-    const int64_t* goff;      // group offsets, ngroups+1
-    const int32_t* pgroup;    // group of every point
-    const int32_t* vgrp;      // group range of every video, nvideos+1
-    const uint8_t* reset;     // reset flag per group (linker_reset_points)
-    int32_t ngroups, nvideos;
-    int64_t npoints;
-    float radius;
-    int32_t memory;
+    const float* px = nullptr;          // row coordinate of every point ("y" column)
+    const float* py = nullptr;          // column coordinate ("x" column)
+    int32_t xy_stride = 1;              // floats between consecutive points
+    const int64_t* goff = nullptr;      // compact: group offsets, ngroups+1
+    const int32_t* pgroup = nullptr;    // compact: group of every point
+    const uint32_t* gcount = nullptr;   // slot: points per group
+    int64_t slot_stride = 0;            // slot: slots per group (0 = compact)
+    const int32_t* vgrp = nullptr;      // group range of every video, nvideos+1
+    const uint8_t* reset = nullptr;     // reset flag per group (linker_reset_points)
+    int32_t ngroups = 0, nvideos = 0;
+    int32_t groups_ready = 0;           // groups whose points exist (forward lists stop there)
+    int64_t npoints = 0;                // compact: points; slot: ngroups*slot_stride
+    float radius = 0.0f;
+    int32_t memory = 0;
 };
 
 struct LinkLists {
-    // per point and k in 1..K: forward (dests in group+k) and backward
-    // (sources in group-k) neighbour lists, ascending point index
-    int64_t* f_off;   // npoints*K + 1
-    int64_t* b_off;   // npoints*K + 1
-    int32_t* f_pts;
-    int32_t* b_pts;
-    float* b_dist;    // squared distances of the backward lists
-    uint32_t* srt;    // per group: points sorted by row key
+    // per point p and k in 1..K: forward (dests in group+k) and backward
+    // (sources in group-k) neighbour lists, ascending point index; the
+    // offsets of (p, k) are at [(p - pbase)*K + k - 1] and the next entry
+    int64_t* f_off = nullptr;
+    int64_t* b_off = nullptr;
+    int32_t* f_pts = nullptr;
+    int32_t* b_pts = nullptr;
+    float* b_dist = nullptr;      // squared distances of the backward lists
+    uint32_t* srt = nullptr;      // per group: points sorted by row key
+    int64_t pbase = 0;            // first point the offset arrays cover
+    int64_t f_cap = -1, b_cap = -1;  // entries f_pts / b_pts hold (-1: sized exactly)
 };
 
 struct LinkScratch {
@@ -123,6 +136,21 @@ struct LinkScratch {
     size_t bytes_per_video;
     int32_t max_group;
     int64_t max_edges;   // max over groups of the per-step backward-edge total
+    int64_t max_points;  // per-video point space (compact: points of the video)
+};
+
+// Linker state carried from one window of frames to the next (slot mode).
+struct LinkState {
+    long long counter, frame;
+    int32_t prevg, head;
+};
+
+// Frames [g0, g1) of video 0 linked by one launch; g0 < 0 = every video whole.
+struct LinkWindow {
+    int32_t g0 = -1, g1 = -1;
+    int32_t first = 1, last = 1;   // initialise state / run Linker::finish
+    int32_t init_points = 1;       // clear the per-point arrays in the kernel
+    LinkState* state = nullptr;
 };
 
 struct LinkOutput {
@@ -135,12 +163,29 @@ struct LinkOutput {
 
 cudaError_t link_sort_groups(const LinkInput& in, uint32_t* srt, uint8_t* scratch, size_t scratch_per_group,
                              int max_group, cudaStream_t st);
+// groups [g0, g1) only
+cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, cudaStream_t st);
 cudaError_t link_count_lists(const LinkInput& in, const uint32_t* srt, int64_t* f_cnt, int64_t* b_cnt,
                              cudaStream_t st);
 cudaError_t link_fill_lists(const LinkInput& in, const LinkLists& L, cudaStream_t st);
+// points [p0, p1) only; f_cnt/b_cnt and L's offsets are relative to p0 (L.pbase == p0)
+cudaError_t link_count_lists_range(const LinkInput& in, const uint32_t* srt, int64_t p0, int64_t p1,
+                                   int64_t* f_cnt, int64_t* b_cnt, uint32_t* flags, cudaStream_t st);
+cudaError_t link_fill_lists_range(const LinkInput& in, const LinkLists& L, int64_t p1, uint32_t* flags,
+                                  cudaStream_t st);
 size_t link_scratch_bytes(int32_t max_group, int64_t max_edges, int64_t npoints_video, int32_t memory);
+// byte offsets of the per-point arrays the host may clear itself (LinkWindow::init_points == 0):
+// idstamp and srcstamp to 0xFF bytes, firstpos to zero
+void link_scratch_point_arrays(int32_t max_group, int64_t max_edges, int64_t npoints_video, int32_t memory,
+                               size_t* idstamp, size_t* srcstamp, size_t* firstpos);
 cudaError_t link_run(const LinkInput& in, const LinkLists& L, const LinkScratch& S, const LinkOutput& out,
                      cudaStream_t st);
+cudaError_t link_run_window(const LinkInput& in, const LinkLists& L, const LinkScratch& S, const LinkOutput& out,
+                            const LinkWindow& w, cudaStream_t st);
 cudaError_t link_durations(const LinkInput& in, const LinkOutput& out, int64_t* row_dur, cudaStream_t st);
+// slot mode: particle ids (through the f32 round trip) and durations of every
+// point written to table rows row_off[g] + j
+cudaError_t link_slot_rows(const LinkInput& in, const LinkOutput& out, const int64_t* row_off, int64_t* particle,
+                           int64_t* row_dur, cudaStream_t st);
 
 }  // namespace gt

@@ -26,18 +26,36 @@ constexpr int kLinkThreads = 1024;
 constexpr int kSortSmem = 4096;
 constexpr long long kSubnetBudget = 1ll << 28;
 
+// ------------------------------------------------------- point addressing
+__device__ __forceinline__ int64_t gbase(const LinkInput& in, int g) {
+    return in.slot_stride ? (int64_t)g * in.slot_stride : in.goff[g];
+}
+__device__ __forceinline__ int64_t gsize(const LinkInput& in, int g) {
+    return in.slot_stride ? (int64_t)in.gcount[g] : in.goff[g + 1] - in.goff[g];
+}
+__device__ __forceinline__ int ggroup(const LinkInput& in, int64_t p) {
+    return in.slot_stride ? (int)(p / in.slot_stride) : in.pgroup[p];
+}
+__device__ __forceinline__ float prow(const LinkInput& in, int64_t p) { return in.px[p * in.xy_stride]; }
+__device__ __forceinline__ float pcol(const LinkInput& in, int64_t p) { return in.py[p * in.xy_stride]; }
+// offset-array index of (point p, lag slot k) in 0..K
+__device__ __forceinline__ int64_t lix(const LinkLists& L, int64_t p, int K, int k) {
+    return (p - L.pbase) * K + k;
+}
+
 // ------------------------------------------------------------ group sorting
 __global__ void __launch_bounds__(kLinkThreads)
-sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restrict__ scratch, size_t per_group) {
+sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restrict__ scratch, size_t per_group,
+                   int g0) {
     __shared__ uint64_t sk[kSortSmem];
-    const int g = blockIdx.x;
-    const int64_t a = in.goff[g], n = in.goff[g + 1] - a;
+    const int g = g0 + blockIdx.x;
+    const int64_t a = gbase(in, g), n = gsize(in, g);
     if (n == 0) return;
     int np2 = 1;
     while (np2 < n) np2 <<= 1;
-    uint64_t* keys = (np2 <= kSortSmem) ? sk : scratch + (size_t)g * per_group;
+    uint64_t* keys = (np2 <= kSortSmem) ? sk : scratch + (size_t)blockIdx.x * per_group;
     for (int i = threadIdx.x; i < np2; i += blockDim.x)
-        keys[i] = (i < n) ? (((uint64_t)float_order_key(in.px[a + i]) << 32) | (uint64_t)i) : ~0ull;
+        keys[i] = (i < n) ? (((uint64_t)float_order_key(prow(in, a + i)) << 32) | (uint64_t)i) : ~0ull;
     __syncthreads();
     block_sort_u64(keys, np2);
     for (int i = threadIdx.x; i < n; i += blockDim.x) srt[a + i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
@@ -46,18 +64,18 @@ sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restric
 // First sorted position of group t whose row key is >= klo, and first > khi.
 __device__ __forceinline__ void row_range(const LinkInput& in, const uint32_t* srt, int t, float lo, float hi,
                                           int64_t* p0, int64_t* p1) {
-    const int64_t a = in.goff[t], n = in.goff[t + 1] - a;
+    const int64_t a = gbase(in, t), n = gsize(in, t);
     const uint32_t klo = float_order_key(lo), khi = float_order_key(hi);
     int64_t x = 0, y = n;
     while (x < y) {
         int64_t m = (x + y) >> 1;
-        if (float_order_key(in.px[a + srt[a + m]]) < klo) x = m + 1; else y = m;
+        if (float_order_key(prow(in, a + srt[a + m])) < klo) x = m + 1; else y = m;
     }
     *p0 = x;
     y = n;
     while (x < y) {
         int64_t m = (x + y) >> 1;
-        if (float_order_key(in.px[a + srt[a + m]]) <= khi) x = m + 1; else y = m;
+        if (float_order_key(prow(in, a + srt[a + m])) <= khi) x = m + 1; else y = m;
     }
     *p1 = x;
 }
@@ -79,16 +97,21 @@ __device__ __forceinline__ void group_video_range(const LinkInput& in, int h, in
     *ve = in.vgrp[x + 1];
 }
 
-// mode 0: count, mode 1: fill (and sort ascending)
+// mode 0: count, mode 1: fill (and sort ascending); points [p0, p1), offsets
+// relative to L.pbase.  A fill whose list would pass the end of its buffer
+// (f_cap / b_cap) writes nothing and raises kFlagListOverflow.
 template <int kMode>
-__global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t* b_cnt) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= in.npoints) return;
+__global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t* b_cnt, int64_t p0, int64_t p1,
+                             uint32_t* flags) {
+    const int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= p1) return;
     const int K = in.memory + 1;
-    const int h = in.pgroup[p];
+    const int h = ggroup(in, p);
+    if (in.slot_stride && p - gbase(in, h) >= gsize(in, h)) return;  // empty slot
     int vb, ve;
     group_video_range(in, h, &vb, &ve);
-    const float qx = in.px[p], qy = in.py[p];
+    const int ready = in.groups_ready > 0 ? in.groups_ready : in.ngroups;
+    const float qx = prow(in, p), qy = pcol(in, p);
     const float R = in.radius;
     float lo, hi;
     search_bounds(qx, R, &lo, &hi);
@@ -97,15 +120,20 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
         // forward: p is a source, dests in group h + k
         int t = h + k;
         int64_t cnt = 0;
-        if (t < ve && !qnan) {
+        bool skip = false;
+        if (kMode && t < ve && t < ready && L.f_cap >= 0 && L.f_off[lix(L, p, K, k)] > L.f_cap) {
+            atomicOr(flags, kFlagListOverflow);
+            skip = true;
+        }
+        if (t < ve && t < ready && !qnan && !skip) {
             int64_t s0, s1;
             row_range(in, L.srt, t, lo, hi, &s0, &s1);
-            const int64_t a = in.goff[t];
-            int32_t* out = kMode ? L.f_pts + L.f_off[p * K + (k - 1)] : nullptr;
+            const int64_t a = gbase(in, t);
+            int32_t* out = kMode ? L.f_pts + L.f_off[lix(L, p, K, k - 1)] : nullptr;
             for (int64_t m = s0; m < s1; m++) {
                 int64_t d = a + L.srt[a + m];
                 float dist;
-                if (within_rd2(in.px[d], in.py[d], qx, qy, R, &dist)) {
+                if (within_rd2(prow(in, d), pcol(in, d), qx, qy, R, &dist)) {
                     if (kMode) out[cnt] = (int32_t)(d - a);
                     cnt++;
                 }
@@ -119,20 +147,25 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
                 }
             }
         }
-        if (!kMode) f_cnt[p * K + (k - 1)] = cnt;
+        if (!kMode) f_cnt[lix(L, p, K, k - 1)] = cnt;
         // backward: p is a dest, sources in group h - k
         t = h - k;
         cnt = 0;
-        if (t >= vb && !qnan) {
+        skip = false;
+        if (kMode && t >= vb && L.b_cap >= 0 && L.b_off[lix(L, p, K, k)] > L.b_cap) {
+            atomicOr(flags, kFlagListOverflow);
+            skip = true;
+        }
+        if (t >= vb && !qnan && !skip) {
             int64_t s0, s1;
             row_range(in, L.srt, t, lo, hi, &s0, &s1);
-            const int64_t a = in.goff[t];
-            int32_t* out = kMode ? L.b_pts + L.b_off[p * K + (k - 1)] : nullptr;
-            float* outd = kMode ? L.b_dist + L.b_off[p * K + (k - 1)] : nullptr;
+            const int64_t a = gbase(in, t);
+            int32_t* out = kMode ? L.b_pts + L.b_off[lix(L, p, K, k - 1)] : nullptr;
+            float* outd = kMode ? L.b_dist + L.b_off[lix(L, p, K, k - 1)] : nullptr;
             for (int64_t m = s0; m < s1; m++) {
                 int64_t s = a + L.srt[a + m];
                 float dist;
-                if (within_rd2(qx, qy, in.px[s], in.py[s], R, &dist)) {
+                if (within_rd2(qx, qy, prow(in, s), pcol(in, s), R, &dist)) {
                     if (kMode) {
                         out[cnt] = (int32_t)(s - a);
                         outd[cnt] = dist;
@@ -151,7 +184,7 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
                 }
             }
         }
-        if (!kMode) b_cnt[p * K + (k - 1)] = cnt;
+        if (!kMode) b_cnt[lix(L, p, K, k - 1)] = cnt;
     }
 }
 
@@ -207,6 +240,14 @@ size_t link_scratch_bytes(int32_t max_group, int64_t max_edges, int64_t npoints_
     return make_lay(max_group, max_edges, npoints_video, memory).total;
 }
 
+void link_scratch_point_arrays(int32_t max_group, int64_t max_edges, int64_t npoints_video, int32_t memory,
+                               size_t* idstamp, size_t* srcstamp, size_t* firstpos) {
+    const Lay l = make_lay(max_group, max_edges, npoints_video, memory);
+    *idstamp = l.idstamp;
+    *srcstamp = l.srcstamp;
+    *firstpos = l.firstpos;
+}
+
 // union-find over the destinations of one frame; roots are minimal indices
 __device__ __forceinline__ int uf_find(volatile int* parent, int x) {
     while (true) {
@@ -229,17 +270,19 @@ __device__ __forceinline__ void uf_union(volatile int* parent, int a, int b) {
 }
 
 __global__ void __launch_bounds__(kLinkThreads)
-link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
+link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, LinkWindow W) {
     __shared__ int wsum[33];
     __shared__ long long sh_counter, sh_frame, sh_load;
     __shared__ int sh_prevg, sh_head, sh_nroots, sh_ringtot;
     const int v = blockIdx.x;
     const int gb = in.vgrp[v], ge = in.vgrp[v + 1];
-    const int64_t P0 = in.goff[gb];
-    const int64_t NP = in.goff[ge] - P0;
+    const int g_lo = (W.g0 < 0) ? gb : W.g0, g_hi = (W.g0 < 0) ? ge : W.g1;
+    if (out.flags[v] & kLinkStopFlags) return;  // an earlier window stopped this video
+    const int64_t P0 = gbase(in, gb);
+    const int64_t NP = in.slot_stride ? (int64_t)(ge - gb) * in.slot_stride : in.goff[ge] - P0;
     const int M = in.memory, K = M + 1;
     const int G = S.max_group;
-    const Lay lay = make_lay(G, S.max_edges, NP, M);
+    const Lay lay = make_lay(G, S.max_edges, S.max_points, M);
     uint8_t* base = S.base + (size_t)v * S.bytes_per_video;
     int64_t* start = (int64_t*)(base + lay.start);
     int32_t* idstamp = (int32_t*)(base + lay.idstamp);
@@ -279,23 +322,33 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
     const float R2 = __fmul_rn(R, R);
     const int tid = threadIdx.x, nth = blockDim.x;
 
-    for (int64_t i = tid; i < NP; i += nth) {
-        idstamp[i] = -1;
-        srcstamp[i] = -1;
-        firstpos[i] = 0ull;
-    }
-    for (int i = tid; i < Smax; i += nth) vis_s[i] = -1;
-    for (int i = tid; i < G; i += nth) vis_d[i] = -1;
-    for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
-    if (tid == 0) {
-        sh_counter = 0;
-        sh_frame = 0;
-        sh_prevg = -1;
-        sh_head = 0;
+    if (W.first) {
+        if (W.init_points) {
+            for (int64_t i = tid; i < NP; i += nth) {
+                idstamp[i] = -1;
+                srcstamp[i] = -1;
+                firstpos[i] = 0ull;
+            }
+        }
+        for (int i = tid; i < Smax; i += nth) vis_s[i] = -1;
+        for (int i = tid; i < G; i += nth) vis_d[i] = -1;
+        for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
+        if (tid == 0) {
+            sh_counter = 0;
+            sh_frame = 0;
+            sh_prevg = -1;
+            sh_head = 0;
+        }
+    } else if (tid == 0) {
+        const LinkState st = W.state[v];
+        sh_counter = st.counter;
+        sh_frame = st.frame;
+        sh_prevg = st.prevg;
+        sh_head = st.head;
     }
     __syncthreads();
 
-    for (int g = gb; g < ge; g++) {
+    for (int g = g_lo; g < g_hi; g++) {
         const int step = g - gb;
         if (in.reset[g]) {
             // Linker::reset (src/linking.rs:401-403, src/execute_gpu.rs:792-798)
@@ -308,11 +361,11 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
             for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
             __syncthreads();
         }
-        const int64_t a = in.goff[g];
-        const int D = (int)(in.goff[g + 1] - a);
+        const int64_t a = gbase(in, g);
+        const int D = (int)gsize(in, g);
         const int prevg = sh_prevg;
-        const int S0 = (prevg == g - 1 && prevg >= gb) ? (int)(in.goff[g] - in.goff[g - 1]) : 0;
-        const int64_t pa = (S0 > 0) ? in.goff[g - 1] : 0;
+        const int S0 = (prevg == g - 1 && prevg >= gb) ? (int)gsize(in, g - 1) : 0;
+        const int64_t pa = (S0 > 0) ? gbase(in, g - 1) : 0;
         // ---- P1: sources = previous frame + memory entries not already present
         for (int i = tid; i < S0; i += nth) {
             int64_t pt = pa + i;
@@ -377,12 +430,12 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
             int deg = 0;
             if (j < D) {
                 int64_t pt = a + j;
-                if (S0 > 0) deg += (int)(L.b_off[pt * K + 1] - L.b_off[pt * K + 0]);
+                if (S0 > 0) deg += (int)(L.b_off[lix(L, pt, K, 1)] - L.b_off[lix(L, pt, K, 0)]);
                 for (int k = K; k >= 2; k--) {
                     int t = g - k;
                     if (t < gb) continue;
-                    int64_t o0 = L.b_off[pt * K + (k - 1)], o1 = L.b_off[pt * K + k];
-                    int64_t ta = in.goff[t] - P0;
+                    int64_t o0 = L.b_off[lix(L, pt, K, k - 1)], o1 = L.b_off[lix(L, pt, K, k)];
+                    int64_t ta = gbase(in, t) - P0;
                     for (int64_t e = o0; e < o1; e++)
                         if (srcstamp[ta + L.b_pts[e]] == step) deg++;
                 }
@@ -395,14 +448,14 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
         if (tid == 0) d_off[D] = etot;
         __syncthreads();
         if (etot > S.max_edges) {
-            if (tid == 0) atomicOr(out.flags + v, kFlagScratch);
+            if (tid == 0) atomicOr(out.flags + v, in.slot_stride ? kFlagEdgeOverflow : kFlagScratch);
             break;
         }
         for (int j = tid; j < D; j += nth) {
             int64_t pt = a + j;
             int w = d_off[j];
             if (S0 > 0) {
-                int64_t o0 = L.b_off[pt * K + 0], o1 = L.b_off[pt * K + 1];
+                int64_t o0 = L.b_off[lix(L, pt, K, 0)], o1 = L.b_off[lix(L, pt, K, 1)];
                 for (int64_t e = o0; e < o1; e++) {
                     e_src[w] = L.b_pts[e];  // index within group g-1 == source index
                     e_dist[w] = L.b_dist[e];
@@ -412,8 +465,8 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
             for (int k = K; k >= 2; k--) {
                 int t = g - k;
                 if (t < gb) continue;
-                int64_t o0 = L.b_off[pt * K + (k - 1)], o1 = L.b_off[pt * K + k];
-                int64_t ta = in.goff[t] - P0;
+                int64_t o0 = L.b_off[lix(L, pt, K, k - 1)], o1 = L.b_off[lix(L, pt, K, k)];
+                int64_t ta = gbase(in, t) - P0;
                 for (int64_t e = o0; e < o1; e++) {
                     int64_t lp = ta + L.b_pts[e];
                     if (srcstamp[lp] == step) {
@@ -435,9 +488,9 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
         auto fwd = [&](int s, int64_t* f0, int64_t* f1) {
             int64_t lp = src_pt[s];
             int64_t pt = P0 + lp;
-            int k = g - in.pgroup[pt];
-            *f0 = L.f_off[pt * K + (k - 1)];
-            *f1 = L.f_off[pt * K + k];
+            int k = g - ggroup(in, pt);
+            *f0 = L.f_off[lix(L, pt, K, k - 1)];
+            *f1 = L.f_off[lix(L, pt, K, k)];
         };
         for (int j = tid; j < D; j += nth) {
             int deg = d_off[j + 1] - d_off[j];
@@ -707,8 +760,19 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
         }
     }
     __syncthreads();
+    if (!W.last) {
+        if (tid == 0 && !(out.flags[v] & kLinkStopFlags)) {
+            LinkState st;
+            st.counter = sh_counter;
+            st.frame = sh_frame;
+            st.prevg = sh_prevg;
+            st.head = sh_head;
+            W.state[v] = st;
+        }
+        return;
+    }
     // ---- Linker::finish (src/linking.rs:505-520)
-    if (!(out.flags[v] & (kFlagTooDense | kFlagSubnetBudget | kFlagScratch))) {
+    if (!(out.flags[v] & kLinkStopFlags)) {
         const long long frame = sh_frame;
         if (M > 0) {
             for (int q = 0; q < M; q++) {
@@ -723,7 +787,8 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out) {
         }
         if (sh_prevg >= gb) {
             const int pg = sh_prevg;
-            for (int64_t p = in.goff[pg] + tid; p < in.goff[pg + 1]; p += nth) {
+            const int64_t pb = gbase(in, pg), pe = pb + gsize(in, pg);
+            for (int64_t p = pb + tid; p < pe; p += nth) {
                 int64_t id = ids[p];
                 dur[id] = frame - start[id];
             }
@@ -754,40 +819,96 @@ __global__ void durations_kernel(LinkInput in, LinkOutput out, int64_t* row_dur)
     row_dur[p] = out.dur[P0 + id];
 }
 
+// Slot mode: the table rows of every point (row_off[g] + j) receive the
+// particle id after the reference's f32 round trip and its duration
+// (src/execute_gpu.rs:812-815, 1165-1181).  One video.
+__global__ void slot_rows_kernel(LinkInput in, LinkOutput out, const int64_t* __restrict__ row_off,
+                                 int64_t* __restrict__ particle, int64_t* __restrict__ row_dur) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= in.npoints) return;
+    const int g = (int)(p / in.slot_stride);
+    const int64_t j = p - (int64_t)g * in.slot_stride;
+    if (j >= (int64_t)in.gcount[g]) return;
+    const int64_t row = row_off[g] + j;
+    const int64_t id = (int64_t)(float)out.ids[p];
+    particle[row] = id;
+    if (id >= out.counter[0]) {
+        atomicOr(out.flags, kFlagScratch);
+        row_dur[row] = -1;
+        return;
+    }
+    row_dur[row] = out.dur[id];
+}
+
 // --------------------------------------------------------------- launchers
 cudaError_t link_sort_groups(const LinkInput& in, uint32_t* srt, uint8_t* scratch, size_t scratch_per_group,
                              int max_group, cudaStream_t st) {
     (void)max_group;
     if (in.ngroups == 0) return cudaSuccess;
-    sort_groups_kernel<<<in.ngroups, kLinkThreads, 0, st>>>(in, srt, (uint64_t*)scratch, scratch_per_group / 8);
+    sort_groups_kernel<<<in.ngroups, kLinkThreads, 0, st>>>(in, srt, (uint64_t*)scratch, scratch_per_group / 8, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, cudaStream_t st) {
+    if (g1 <= g0) return cudaSuccess;
+    // groups of at most kSortSmem points sort in shared memory; no scratch
+    if (in.slot_stride > kSortSmem) return cudaErrorInvalidValue;
+    sort_groups_kernel<<<g1 - g0, kLinkThreads, 0, st>>>(in, srt, nullptr, 0, g0);
     return cudaGetLastError();
 }
 
 cudaError_t link_count_lists(const LinkInput& in, const uint32_t* srt, int64_t* f_cnt, int64_t* b_cnt,
                              cudaStream_t st) {
-    if (in.npoints == 0) return cudaSuccess;
-    LinkLists L = {};
+    return link_count_lists_range(in, srt, 0, in.npoints, f_cnt, b_cnt, nullptr, st);
+}
+
+cudaError_t link_count_lists_range(const LinkInput& in, const uint32_t* srt, int64_t p0, int64_t p1,
+                                   int64_t* f_cnt, int64_t* b_cnt, uint32_t* flags, cudaStream_t st) {
+    if (p1 <= p0) return cudaSuccess;
+    LinkLists L;
     L.srt = (uint32_t*)srt;
-    lists_kernel<0><<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, L, f_cnt, b_cnt);
+    L.pbase = p0;
+    lists_kernel<0><<<(unsigned)((p1 - p0 + 255) / 256), 256, 0, st>>>(in, L, f_cnt, b_cnt, p0, p1, flags);
     return cudaGetLastError();
 }
 
 cudaError_t link_fill_lists(const LinkInput& in, const LinkLists& L, cudaStream_t st) {
-    if (in.npoints == 0) return cudaSuccess;
-    lists_kernel<1><<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, L, nullptr, nullptr);
+    return link_fill_lists_range(in, L, in.npoints, nullptr, st);
+}
+
+cudaError_t link_fill_lists_range(const LinkInput& in, const LinkLists& L, int64_t p1, uint32_t* flags,
+                                  cudaStream_t st) {
+    const int64_t p0 = L.pbase;
+    if (p1 <= p0) return cudaSuccess;
+    if ((L.f_cap >= 0 || L.b_cap >= 0) && !flags) return cudaErrorInvalidValue;
+    lists_kernel<1><<<(unsigned)((p1 - p0 + 255) / 256), 256, 0, st>>>(in, L, nullptr, nullptr, p0, p1, flags);
     return cudaGetLastError();
 }
 
 cudaError_t link_run(const LinkInput& in, const LinkLists& L, const LinkScratch& S, const LinkOutput& out,
                      cudaStream_t st) {
+    return link_run_window(in, L, S, out, LinkWindow(), st);
+}
+
+cudaError_t link_run_window(const LinkInput& in, const LinkLists& L, const LinkScratch& S, const LinkOutput& out,
+                            const LinkWindow& w, cudaStream_t st) {
     if (in.nvideos == 0) return cudaSuccess;
-    link_video_kernel<<<in.nvideos, kLinkThreads, 0, st>>>(in, L, S, out);
+    if (w.g0 >= 0 && (in.nvideos != 1 || !w.state)) return cudaErrorInvalidValue;
+    link_video_kernel<<<in.nvideos, kLinkThreads, 0, st>>>(in, L, S, out, w);
     return cudaGetLastError();
 }
 
 cudaError_t link_durations(const LinkInput& in, const LinkOutput& out, int64_t* row_dur, cudaStream_t st) {
     if (in.npoints == 0) return cudaSuccess;
     durations_kernel<<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, out, row_dur);
+    return cudaGetLastError();
+}
+
+cudaError_t link_slot_rows(const LinkInput& in, const LinkOutput& out, const int64_t* row_off, int64_t* particle,
+                           int64_t* row_dur, cudaStream_t st) {
+    if (in.npoints == 0) return cudaSuccess;
+    if (!in.slot_stride || in.nvideos != 1) return cudaErrorInvalidValue;
+    slot_rows_kernel<<<(unsigned)((in.npoints + 255) / 256), 256, 0, st>>>(in, out, row_off, particle, row_dur);
     return cudaGetLastError();
 }
 

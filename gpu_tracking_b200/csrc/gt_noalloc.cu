@@ -319,6 +319,7 @@ extern "C" gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_fyx, int64_t n,
     S.max_group = kNoAllocMaxGroup;
     S.max_edges = kNoAllocMaxEdges;
     S.bytes_per_video = link_scratch_bytes(S.max_group, S.max_edges, n, (int32_t)memory);
+    S.max_points = n;
     LinkOutput out;
     out.ids = d_out;
     out.counter = (int64_t*)(base + L.counter);
