@@ -327,6 +327,46 @@ gt_status make_locate_consts(gt_ctx* ctx, const gt_params& p, int32_t H, int32_t
     return GT_OK;
 }
 
+// Division by gnorm and kk in the strip kernel as fma(x, zh, x*zl), zh + zl
+// the two-float reciprocal, when that is IEEE division for every dividend the
+// pipeline can produce: integer pixels 0..65535 and positive taps bound the
+// row-pass sums, the column-pass sums and the boxcar sums away from zero and
+// infinity, and inside those bounds (x*zl and the quotient normal) the
+// identity checked for every mantissa of [1, 2) holds at every exponent.
+template <typename T>
+void set_fast_div(gt_ctx* ctx, LocateConsts& c) {
+    c.fast_div = 0;
+    if (std::is_same<T, float>::value) return;
+    auto split = [](float d, float* zh, float* zl) {
+        const double r = 1.0 / (double)d;
+        *zh = (float)r;
+        *zl = (float)(r - (double)*zh);
+    };
+    split(c.gnorm, &c.zh_g, &c.zl_g);
+    split(c.kk, &c.zh_k, &c.zl_k);
+    double tmin = INFINITY, tsum = 0.0;
+    for (int i = 0; i <= 2 * c.R; i++) {
+        if (!(c.taps[i] > 0.0f)) return;
+        tmin = std::min(tmin, (double)c.taps[i]);
+        tsum += c.taps[i];
+    }
+    const double gn = c.gnorm, kk = c.kk;
+    const double row_lo = tmin, row_hi = 65535.0 * tsum;
+    const double col_lo = tmin * (row_lo / gn), col_hi = tsum * (row_hi / gn);
+    const double g_lo = 0.5 * std::min(row_lo, col_lo), g_hi = 2.0 * std::max(row_hi, col_hi);
+    const double k_lo = 0.5, k_hi = 2.0 * 65535.0 * kk;
+    auto safe = [](double lo, double hi, double d, double zh, double zl) {
+        const double tiny = std::ldexp(1.0, -120), big = std::ldexp(1.0, 100);
+        if (zl != 0.0 && lo * std::fabs(zl) < tiny) return false;
+        if (lo / d < tiny || hi * zh > big || hi / d > big) return false;
+        return true;
+    };
+    if (!safe(g_lo, g_hi, gn, c.zh_g, c.zl_g) || !safe(k_lo, k_hi, kk, c.zh_k, c.zl_k)) return;
+    if (!const_div_proven(c.gnorm, c.zh_g, c.zl_g, ctx->st) || !const_div_proven(c.kk, c.zh_k, c.zl_k, ctx->st))
+        return;
+    c.fast_div = 1;
+}
+
 // (sin 2θ, cos 2θ) tables per integer radius 0..max_rint (characterize.wgsl:120-124)
 void angle_tables(int max_rint, std::vector<float2>& tab, std::vector<int32_t>& off) {
     tab.clear();
@@ -1032,6 +1072,7 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
                      gt_table* tab) {
     LocateConsts c;
     CKS(make_locate_consts(ctx, p, H, W, c));
+    set_fast_div<T>(ctx, c);
     LogTables lt;
     const bool log_style = (p.style == GT_STYLE_LOG);
     if (log_style) {

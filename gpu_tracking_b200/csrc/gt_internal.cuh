@@ -57,6 +57,13 @@ struct LocateConsts {
     float image_std;
     float rough;
     int32_t characterize;
+    // Division by the call's constant divisors gnorm and kk as
+    // fma(x, zh, x*zl) with zh + zl a two-float reciprocal; set only when
+    // that equals IEEE x/d for every mantissa (checked on the device) and
+    // every dividend the pipeline can produce lies in the exponent range
+    // where the check carries over (integer pixel types).
+    int32_t fast_div;
+    float zh_g, zl_g, zh_k, zl_k;
     float taps[kMaxTaps];
 };
 

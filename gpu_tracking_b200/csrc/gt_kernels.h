@@ -54,6 +54,10 @@ bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const
                   uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,
                   cudaError_t* err);
 
+// True when fma(x, zh, x*zl) equals IEEE x/d for every x in [1, 2) (checked
+// on the device once per (d, zh, zl) and remembered).
+bool const_div_proven(float d, float zh, float zl, cudaStream_t st);
+
 template <typename T>
 cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_stride, const LocateConsts& c,
                         int nframes, int n_slots, const uint32_t* cand_count, const uint32_t* cand_keys,

@@ -2,18 +2,30 @@
 //
 // Same results as bandpass_kernel<T, true> (preprocess_rows.wgsl,
 // preprocess_cols.wgsl, max_rows.wgsl, extract_max.wgsl), organised for
-// throughput: a CTA owns a strip of 128 output columns and walks down a
-// segment of rows eight rows per step.  The row-pass results (g/gauss_norm,
-// boxcar) and the processed rows live in shared-memory ring buffers, so the
-// vertical halo is computed once per strip instead of once per tile; the tap
-// loops are unrolled for the compile-time radius (taps come from the constant
-// bank); each thread computes four outputs per pass from registers; the
-// dilation maximum of a 4-output run is built from one shared middle block
-// plus prefix/suffix maxima.  The floating-point operation sequence of every
-// output is the oracle's: sequential fused multiply-adds over the taps,
-// sequential boxcar sums (a sliding sum for integer inputs, where every
-// partial sum is an exactly representable integer), IEEE division.
+// instruction throughput.  A CTA owns a strip of 128 output columns and walks
+// down a segment of rows eight rows per step:
+//   A  the step's raw rows are staged in shared memory (4 pixels per load,
+//      converted exactly to float), the next step's are prefetched;
+//   B  row pass: each thread makes 4 adjacent columns from float4 loads;
+//   C  column pass: each thread makes 4 rows of one column;
+//   D  vertical dilation maximum, 4 rows per thread;
+//   E  horizontal dilation maximum and the candidate test, 4 columns per
+//      thread, slots reserved once per warp.
+// The row-pass rows and the processed rows live in ring buffers that hold
+// every row twice (at r and r + ring), so any window of consecutive rows is
+// contiguous and every read in the tap loops is a constant offset from one
+// base address.  The tap loops are unrolled for the compile-time radius.
+// The floating-point operation sequence of every output is the oracle's:
+// sequential fused multiply-adds over the taps, sequential boxcar sums (a
+// sliding sum for integer inputs, where every partial sum is an exactly
+// representable integer), and division by the constants gnorm and kk either
+// as IEEE division or, where proven equal to it (LocateConsts::fast_div), as
+// fma(x, zh, x*zl).
 #include <math.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "gt_internal.cuh"
 #include "gt_kernels.h"
@@ -28,14 +40,28 @@ template <int R, int KD>
 struct StripGeom {
     static constexpr int O = (int)((float)KD / 2.0f - 0.5f);
     static constexpr int E = KD - 1 - O;
-    static constexpr int PW = kStripTW + KD - 1;   // processed / row-pass columns
-    static constexpr int RW = PW + 2 * R;          // raw columns
-    static constexpr int XR = ((kStepRows + 2 * R + 7) / 8) * 8;   // row-pass ring rows
-    static constexpr int PR = ((kStepRows + KD - 1 + 7) / 8) * 8;  // processed ring rows
-    static constexpr int RAWN = kStepRows * RW;
+    static constexpr int PW = kStripTW + KD - 1;          // processed columns a strip needs
+    // raw column origin rc0 = c0 - O - R is rounded down to a multiple of 4
+    // (c0 is a multiple of 128): the row-pass columns start SH4 early
+    static constexpr int SH4 = (4 - (O + R) % 4) % 4;
+    static constexpr int NG = (PW + SH4 + 3) / 4;         // 4-column groups of the row pass
+    static constexpr int PWp = 4 * NG;                    // row stride of row-pass / processed rows
+    static constexpr int NX4 = (4 + 2 * R + 3) / 4;       // float4 loads per row-pass group
+    static constexpr int RWp = PWp + 4 * (NX4 - 1);       // staged raw columns (>= PWp + 2R)
+    static constexpr int RW4 = RWp / 4;
+    static constexpr int XR = kStepRows + 2 * R;          // row-pass ring rows
+    static constexpr int PR = kStepRows + KD - 1;         // processed ring rows
+    static constexpr int NV4 = (KD + 3 + 3) / 4;          // float4 loads per dilation group
+    static constexpr int RAWV = kStepRows * RW4;          // 4-pixel loads per step
+    static constexpr int RAWVPT = (RAWV + kStripThreads - 1) / kStripThreads;
+    static constexpr int RAWN = kStepRows * RWp;
     static constexpr int RAWPT = (RAWN + kStripThreads - 1) / kStripThreads;
-    static constexpr size_t smem_floats = (size_t)kStepRows * RW + 2 * (size_t)XR * PW + (size_t)PR * PW +
-                                          (size_t)kStepRows * PW;
+    static constexpr size_t smem_floats = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp +
+                                          (size_t)(2 * PR) * PWp + (size_t)kStepRows * PWp;
+    static constexpr int min_blocks = (smem_floats * 4 + 1024) * 3 <= 227 * 1024 ? 3 : 2;
+    static_assert(RWp % 4 == 0 && RWp >= PWp + 2 * R, "staged raw row");
+    static_assert(4 * 31 + 4 * NV4 <= PWp, "dilation row reads stay in the row");
+    static_assert(4 * 31 + KD + 2 <= PW - 1 && SH4 + O + kStripTW <= PWp, "dilation windows inside the row");
 };
 
 template <typename T>
@@ -43,49 +69,109 @@ struct IsIntPix {
     static constexpr bool value = !std::is_same<T, float>::value;
 };
 
-template <typename T, int R, int KD>
-__global__ void __launch_bounds__(kStripThreads, 3)
+// Four raw pixels of one aligned load, exactly as floats (u8/u16 through the
+// 2^23 bias: the integer's bits under the exponent of 2^23, minus 2^23).
+__device__ __forceinline__ float bias_to_f32(uint32_t bits) { return __fsub_rn(__uint_as_float(bits), 8388608.0f); }
+
+template <typename T>
+struct Quad;
+template <>
+struct Quad<uint16_t> {
+    using V = uint2;
+    __device__ static V load(const uint16_t* p) { return __ldg((const uint2*)p); }
+    __device__ static float4 cvt(V v) {
+        return make_float4(bias_to_f32(__byte_perm(v.x, 0x4B00u, 0x5410)), bias_to_f32(__byte_perm(v.x, 0x4B00u, 0x5432)),
+                           bias_to_f32(__byte_perm(v.y, 0x4B00u, 0x5410)), bias_to_f32(__byte_perm(v.y, 0x4B00u, 0x5432)));
+    }
+};
+template <>
+struct Quad<uint8_t> {
+    using V = uint32_t;
+    __device__ static V load(const uint8_t* p) { return __ldg((const uint32_t*)p); }
+    __device__ static float4 cvt(V v) {
+        return make_float4(bias_to_f32(__byte_perm(v, 0x4B000000u, 0x7440)),
+                           bias_to_f32(__byte_perm(v, 0x4B000000u, 0x7441)),
+                           bias_to_f32(__byte_perm(v, 0x4B000000u, 0x7442)),
+                           bias_to_f32(__byte_perm(v, 0x4B000000u, 0x7443)));
+    }
+};
+template <>
+struct Quad<float> {
+    using V = float4;
+    __device__ static V load(const float* p) { return __ldg((const float4*)p); }
+    __device__ static float4 cvt(V v) { return v; }
+};
+
+template <bool FAST>
+__device__ __forceinline__ float div_gnorm(float x, const LocateConsts& c) {
+    return FAST ? __fmaf_rn(x, c.zh_g, __fmul_rn(x, c.zl_g)) : __fdiv_rn(x, c.gnorm);
+}
+template <bool FAST>
+__device__ __forceinline__ float div_kk(float x, const LocateConsts& c) {
+    return FAST ? __fmaf_rn(x, c.zh_k, __fmul_rn(x, c.zl_k)) : __fdiv_rn(x, c.kk);
+}
+
+template <typename T, int R, int KD, bool FAST>
+__global__ void __launch_bounds__(kStripThreads, StripGeom<R, KD>::min_blocks)
 strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restrict__ processed, const LocateConsts c,
-             int SH, uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys, uint32_t cand_cap,
-             uint32_t* __restrict__ flags) {
+             int SH, int vec_ok, uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys,
+             uint32_t cand_cap, uint32_t* __restrict__ flags) {
     using G = StripGeom<R, KD>;
-    constexpr int O = G::O, E = G::E, PW = G::PW, RW = G::RW, XR = G::XR, PR = G::PR;
+    constexpr int O = G::O, E = G::E, PWp = G::PWp, RWp = G::RWp, XR = G::XR, PR = G::PR, SH4 = G::SH4;
     constexpr bool kInt = IsIntPix<T>::value;
-    extern __shared__ float sm[];
-    float* stage = sm;                          // [8][RW]
-    float* xg = stage + kStepRows * RW;         // [XR][PW]
-    float* xb = xg + XR * PW;                   // [XR][PW]
-    float* pr = xb + XR * PW;                   // [PR][PW]
-    float* vb = pr + PR * PW;                   // [8][PW]
+    extern __shared__ float4 sm4[];
+    float* sm = (float*)sm4;
+    float* stage = sm;                          // [8][RWp]      raw columns xa .. xa+RWp
+    float* xg = stage + kStepRows * RWp;        // [2XR][PWp]    row pass g / gnorm, rows stored twice
+    float* xb = xg + 2 * XR * PWp;              // [2XR][PWp]    row pass boxcar
+    float* pr = xb + 2 * XR * PWp;              // [2PR][PWp]    processed rows, stored twice
+    float* vb = pr + 2 * PR * PWp;              // [8][PWp]      vertical maxima (pc0-relative columns)
 
     const int H = c.H, W = c.W;
     const int f = blockIdx.z;
     const int c0 = blockIdx.x * kStripTW;
     const int R0 = blockIdx.y * SH;
     const int R1 = min(R0 + SH, H);
-    const int x0 = R0 - O - R;          // first raw/row-pass row
-    const int pc0 = c0 - O;             // first processed column
-    const int rc0 = pc0 - R;            // first raw column
+    const int x0 = R0 - O - R;          // first raw / row-pass row
+    const int pc0 = c0 - O;             // first processed column of the strip's dilation windows
+    const int xa = pc0 - R - SH4;       // first staged raw column (a multiple of 4)
+    const int ps = xa + R;              // processed column of row-pass index 0 (= pc0 - SH4)
     const T* img = frames + (size_t)f * frame_stride;
     float* proc = processed + (size_t)f * H * W;
     const int tid = threadIdx.x;
-    const bool edge_cols = (rc0 < 0) || (rc0 + RW > W);
+    const bool edge_cols = (xa < 0) || (xa + RWp > W);
+    const bool vec = vec_ok && !edge_cols;
     // steps until the dilation rows reach R1: x0 + 8s - R - E + 8 >= R1
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
-    float pre[G::RAWPT];
+    // ---- A: staging of raw rows (registers hold the next step's pixels)
+    typename Quad<T>::V pv[G::RAWVPT];
+    float ps_[G::RAWPT];
     auto load_raw = [&](int s) {
+        const int rbase = x0 + kStepRows * s;
+        if (vec) {
 #pragma unroll
-        for (int q = 0; q < G::RAWPT; q++) {
-            int idx = tid + q * kStripThreads;
-            float v = 0.0f;
-            if (idx < G::RAWN) {
-                int j = idx / RW, k = idx - j * RW;
-                int gr = min(max(x0 + kStepRows * s + j, 0), H - 1);
-                int gc = min(max(rc0 + k, 0), W - 1);
-                v = load_px<T>(img, (size_t)gr * W + gc);
+            for (int q = 0; q < G::RAWVPT; q++) {
+                const int v = tid + q * kStripThreads;
+                if (v < G::RAWV) {
+                    const int j = v / G::RW4, k4 = v - j * G::RW4;
+                    const int gr = min(max(rbase + j, 0), H - 1);
+                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
+                }
             }
-            pre[q] = v;
+        } else {
+#pragma unroll
+            for (int q = 0; q < G::RAWPT; q++) {
+                const int idx = tid + q * kStripThreads;
+                float v = 0.0f;
+                if (idx < G::RAWN) {
+                    const int j = idx / RWp, k = idx - j * RWp;
+                    const int gr = min(max(rbase + j, 0), H - 1);
+                    const int gc = min(max(xa + k, 0), W - 1);
+                    v = load_px<T>(img, (size_t)gr * W + gc);
+                }
+                ps_[q] = v;
+            }
         }
     };
     load_raw(0);
@@ -93,39 +179,54 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     uint32_t* cout = cand_keys + (size_t)f * cand_cap;
 
     for (int s = 0; s < nsteps; s++) {
-        // ---- A: raw rows of this step into shared memory; prefetch the next step
+        if (vec) {
 #pragma unroll
-        for (int q = 0; q < G::RAWPT; q++) {
-            int idx = tid + q * kStripThreads;
-            if (idx < G::RAWN) stage[idx] = pre[q];
+            for (int q = 0; q < G::RAWVPT; q++) {
+                const int v = tid + q * kStripThreads;
+                if (v < G::RAWV) {
+                    const int j = v / G::RW4, k4 = v - j * G::RW4;
+                    *(float4*)(stage + j * RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < G::RAWPT; q++) {
+                const int idx = tid + q * kStripThreads;
+                if (idx < G::RAWN) stage[idx] = ps_[q];
+            }
         }
         __syncthreads();
         if (s + 1 < nsteps) load_raw(s + 1);
 
-        // ---- B: row pass (preprocess_rows.wgsl) for 8 rows x PW columns, 4 per thread
+        // ---- B: row pass (preprocess_rows.wgsl), 8 rows x PWp columns, 4 per thread
         {
-            constexpr int NG = (PW + 3) / 4;
-            for (int t = tid; t < kStepRows * NG; t += kStripThreads) {
-                const int j = t / NG, gq = t - j * NG;
+            for (int t = tid; t < kStepRows * G::NG; t += kStripThreads) {
+                const int j = t / G::NG, gq = t - j * G::NG;
                 const int col = 4 * gq;
-                const float* src = stage + j * RW + col;
-                float x[4 + 2 * R];
+                const float4* src = (const float4*)(stage + j * RWp + col);
+                float x[4 * G::NX4];
 #pragma unroll
-                for (int i = 0; i < 4 + 2 * R; i++) x[i] = (col + i < RW) ? src[i] : 0.0f;
-                const int xrow = (kStepRows * s + j) % XR;
+                for (int i = 0; i < G::NX4; i++) {
+                    const float4 v = src[i];
+                    x[4 * i] = v.x;
+                    x[4 * i + 1] = v.y;
+                    x[4 * i + 2] = v.z;
+                    x[4 * i + 3] = v.w;
+                }
+                float og[4], ob[4];
                 float cs = 0.0f;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    if (col + k >= PW) break;
                     float gs = 0.0f;
                     if (!edge_cols) {
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
                     } else {
-                        const int gcol = pc0 + col + k;
+                        // Gaussian taps outside the frame are skipped
+                        const int gcol = ps + col + k;
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) {
-                            int gc = gcol + i - R;
+                            const int gc = gcol + i - R;
                             if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
                         }
                     }
@@ -141,9 +242,16 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, x[k + i]);
                     }
-                    xg[xrow * PW + col + k] = __fdiv_rn(gs, c.gnorm);
-                    xb[xrow * PW + col + k] = cs;
+                    og[k] = div_gnorm<FAST>(gs, c);
+                    ob[k] = cs;
                 }
+                const int xrow = (kStepRows * s + j) % XR;
+                const float4 g4 = make_float4(og[0], og[1], og[2], og[3]);
+                const float4 b4 = make_float4(ob[0], ob[1], ob[2], ob[3]);
+                *(float4*)(xg + xrow * PWp + col) = g4;
+                *(float4*)(xg + (xrow + XR) * PWp + col) = g4;
+                *(float4*)(xb + xrow * PWp + col) = b4;
+                *(float4*)(xb + (xrow + XR) * PWp + col) = b4;
             }
         }
         __syncthreads();
@@ -151,32 +259,35 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
         // ---- C: column pass (preprocess_cols.wgsl) for processed rows q = x0 + 8s - R + jj
         {
             const int qbase = x0 + kStepRows * s - R;
-            for (int t = tid; t < 2 * PW; t += kStripThreads) {
-                const int h = t / PW, pc = t - h * PW;
-                const int q0 = qbase + 4 * h;        // first of 4 processed rows
-                const int gcol = pc0 + pc;
+            for (int t = tid; t < 2 * PWp; t += kStripThreads) {
+                const int h = t / PWp, pc = t - h * PWp;
+                const int q0 = qbase + 4 * h;       // first of 4 processed rows
+                const int gcol = ps + pc;
+                // row-pass rows q0 - R .. q0 + 3 + R: relative index 8s - 2R + 4h + i
+                const int w0 = (kStepRows * s + 4 * h + (XR - 2 * R)) % XR;
+                const float* pg = xg + w0 * PWp + pc;
+                const float* pb = xb + w0 * PWp + pc;
                 float vg[4 + 2 * R], vbx[4 + 2 * R];
 #pragma unroll
                 for (int i = 0; i < 4 + 2 * R; i++) {
-                    // X row q0 - R + i lives at ring row (q0 - R + i - x0) mod XR
-                    int rr = (q0 - R + i - x0 + 8 * XR) % XR;
-                    vg[i] = xg[rr * PW + pc];
-                    vbx[i] = xb[rr * PW + pc];
+                    vg[i] = pg[i * PWp];
+                    vbx[i] = pb[i * PWp];
                 }
                 const bool col_in = (gcol >= 0 && gcol < W);
+                const bool rows_in = (q0 >= R && q0 + 3 < H - R);
                 float cs = 0.0f;
+                float res[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int q = q0 + k;
-                    float res;
                     float gs = 0.0f;
-                    if (q >= R && q < H - R) {
+                    if (rows_in) {
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
                     } else {
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) {
-                            int gr = q + i - R;
+                            const int gr = q + i - R;
                             if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
                         }
                     }
@@ -192,13 +303,24 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
 #pragma unroll
                         for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[k + i]);
                     }
-                    res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
-                    if (c.truncate && res < trunc_thr) res = 0.0f;
+                    float r = __fsub_rn(div_gnorm<FAST>(gs, c), div_kk<FAST>(cs, c));
+                    if (c.truncate && r < trunc_thr) r = 0.0f;
+                    res[k] = r;
+                }
+                // processed row q has relative index q - (x0 - R) = 8s + 4h + k
+                const int p0 = (kStepRows * s + 4 * h) % PR;
+                const int vcol = pc - SH4;   // pc0-relative column
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int q = q0 + k;
                     const bool in = col_in && q >= 0 && q < H;
-                    const int prow = (q - x0 + R + 8 * PR) % PR;
-                    pr[prow * PW + pc] = in ? res : -INFINITY;
+                    const float v = in ? res[k] : -INFINITY;
+                    int pp = p0 + k;
+                    if (pp >= PR) pp -= PR;
+                    pr[pp * PWp + pc] = v;
+                    pr[(pp + PR) * PWp + pc] = v;
                     // the segment's own rows and the strip's own columns go to HBM
-                    if (in && q >= R0 && q < R1 && pc >= O && pc < O + kStripTW) proc[(size_t)q * W + gcol] = res;
+                    if (in && q >= R0 && q < R1 && vcol >= O && vcol < O + kStripTW) proc[(size_t)q * W + gcol] = v;
                 }
             }
         }
@@ -207,16 +329,17 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
         // ---- D: vertical maximum over KD processed rows for dilation rows d = x0 + 8s - R - E + jj
         const int dbase = x0 + kStepRows * s - R - E;
         {
-            for (int t = tid; t < 2 * PW; t += kStripThreads) {
-                const int h = t / PW, pc = t - h * PW;
-                const int d0 = dbase + 4 * h;
-                // window of output k: rows d0 + k - O .. d0 + k + E
+            for (int t = tid; t < 2 * PWp; t += kStripThreads) {
+                const int h = t / PWp, pc = t - h * PWp;
+                const int vcol = pc - SH4;
+                if (vcol < 0) continue;
+                // output k of this thread: processed rows d0 + k - O .. d0 + k + E,
+                // relative index 8s - (KD - 1) + 4h + k + i
+                const int w0 = (kStepRows * s + 4 * h + (2 * PR - (KD - 1))) % PR;
+                const float* pp = pr + w0 * PWp + pc;
                 float a[KD + 3];
 #pragma unroll
-                for (int i = 0; i < KD + 3; i++) {
-                    int rr = (d0 - O + i - x0 + R + 8 * PR) % PR;
-                    a[i] = pr[rr * PW + pc];
-                }
+                for (int i = 0; i < KD + 3; i++) a[i] = pp[i * PWp];
                 float mid = a[3];
 #pragma unroll
                 for (int i = 4; i < KD; i++) mid = fmaxf(mid, a[i]);
@@ -224,10 +347,10 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                 float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
                 float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
                 const int vr = 4 * h;
-                vb[(vr + 0) * PW + pc] = fmaxf(s0, mid);
-                vb[(vr + 1) * PW + pc] = fmaxf(fmaxf(s1, mid), p1);
-                vb[(vr + 2) * PW + pc] = fmaxf(fmaxf(s2, mid), p2);
-                vb[(vr + 3) * PW + pc] = fmaxf(mid, p3);
+                vb[(vr + 0) * PWp + vcol] = fmaxf(s0, mid);
+                vb[(vr + 1) * PWp + vcol] = fmaxf(fmaxf(s1, mid), p1);
+                vb[(vr + 2) * PWp + vcol] = fmaxf(fmaxf(s2, mid), p2);
+                vb[(vr + 3) * PWp + vcol] = fmaxf(mid, p3);
             }
         }
         __syncthreads();
@@ -241,11 +364,18 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
             if (t < kStepRows * (kStripTW / 4)) {
                 const int jj = t / (kStripTW / 4), cg = t - jj * (kStripTW / 4);
                 const int d = dbase + jj;
-                const int cc = 4 * cg;  // interior column offset; processed column = cc + O
+                const int cc = 4 * cg;  // interior column offset; processed column = cc + O (pc0-relative)
                 if (d >= R0 && d < R1) {
-                    float a[KD + 3];
+                    const float4* src = (const float4*)(vb + jj * PWp + cc);
+                    float a[4 * G::NV4];
 #pragma unroll
-                    for (int i = 0; i < KD + 3; i++) a[i] = vb[jj * PW + cc + i];
+                    for (int i = 0; i < G::NV4; i++) {
+                        const float4 v = src[i];
+                        a[4 * i] = v.x;
+                        a[4 * i + 1] = v.y;
+                        a[4 * i + 2] = v.z;
+                        a[4 * i + 3] = v.w;
+                    }
                     float mid = a[3];
 #pragma unroll
                     for (int i = 4; i < KD; i++) mid = fmaxf(mid, a[i]);
@@ -253,13 +383,15 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                     float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
                     float m[4] = {fmaxf(s0, mid), fmaxf(fmaxf(s1, mid), p1), fmaxf(fmaxf(s2, mid), p2),
                                   fmaxf(mid, p3)};
-                    const int prow = (d - x0 + R + 8 * PR) % PR;
+                    int prow = (kStepRows * s + jj + (PR - E)) % PR;   // relative index of row d: 8s + jj - E
+                    const float* cen = pr + prow * PWp + SH4 + O + cc;
+                    const bool rows_ok = d >= c.margin && d < H - c.margin;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
                         const int gc = c0 + cc + k;
                         if (gc >= W) continue;
-                        if (d < c.margin || d >= H - c.margin || gc < c.margin || gc >= W - c.margin) continue;
-                        const float center = pr[prow * PW + cc + k + O];
+                        if (!rows_ok || gc < c.margin || gc >= W - c.margin) continue;
+                        const float center = cen[k];
                         if (center < c.thr) continue;
                         if (m[k] > center) continue;
                         cmask |= 1u << k;
@@ -301,16 +433,19 @@ size_t strip_smem() {
     return StripGeom<R, KD>::smem_floats * sizeof(float);
 }
 
-template <typename T, int R, int KD>
+template <typename T, int R, int KD, bool FAST>
 cudaError_t strip_launch(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                          uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags,
                          cudaStream_t st) {
     const int SH = c.H > 1024 ? 512 : c.H;
     dim3 grid((c.W + kStripTW - 1) / kStripTW, (c.H + SH - 1) / SH, nframes);
     const size_t smem = strip_smem<R, KD>();
-    cudaFuncSetAttribute(strip_kernel<T, R, KD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    strip_kernel<T, R, KD><<<grid, kStripThreads, smem, st>>>(frames, frame_stride, processed, c, SH, cand_count,
-                                                               cand_keys, cand_cap, flags);
+    // 4-pixel loads need every row start (and the frames) aligned to 4 pixels
+    const int vec_ok = (c.W % 4 == 0) && (frame_stride % 4 == 0) &&
+                       ((uintptr_t)frames % (4 * sizeof(T)) == 0) ? 1 : 0;
+    cudaFuncSetAttribute(strip_kernel<T, R, KD, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    strip_kernel<T, R, KD, FAST><<<grid, kStripThreads, smem, st>>>(frames, frame_stride, processed, c, SH, vec_ok,
+                                                                     cand_count, cand_keys, cand_cap, flags);
     return cudaGetLastError();
 }
 
@@ -320,15 +455,19 @@ cudaError_t strip_launch(const T* frames, int64_t frame_stride, float* processed
 #define GT_STRIP_CASES(X) \
     X(2, 8) X(3, 11) X(4, 12) X(4, 14) X(5, 15) X(5, 16) X(6, 18) X(6, 19) X(7, 21) X(7, 22)
 
+// Integer pixels use the proven constant division (fast_div) and fall back to
+// the tile kernel when it is not proven; float pixels use IEEE division.
 template <typename T>
 bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                   uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,
                   cudaError_t* err) {
-#define GT_STRIP_TRY(RR, KK)                                                                                \
-    if (c.R == RR && c.kd == KK) {                                                                         \
-        *err = strip_launch<T, RR, KK>(frames, frame_stride, processed, c, nframes, cand_count, cand_keys, \
-                                       cand_cap, flags, st);                                               \
-        return true;                                                                                       \
+    constexpr bool kInt = IsIntPix<T>::value;
+    if (kInt && !c.fast_div) return false;
+#define GT_STRIP_TRY(RR, KK)                                                                              \
+    if (c.R == RR && c.kd == KK) {                                                                       \
+        *err = strip_launch<T, RR, KK, kInt>(frames, frame_stride, processed, c, nframes, cand_count,     \
+                                             cand_keys, cand_cap, flags, st);                             \
+        return true;                                                                                     \
     }
     GT_STRIP_CASES(GT_STRIP_TRY)
 #undef GT_STRIP_TRY
@@ -341,5 +480,52 @@ template bool launch_strip<float>(const float*, int64_t, float*, const LocateCon
                                   uint32_t, uint32_t*, cudaStream_t, cudaError_t*);
 template bool launch_strip<uint8_t>(const uint8_t*, int64_t, float*, const LocateConsts&, int, uint32_t*, uint32_t*,
                                     uint32_t, uint32_t*, cudaStream_t, cudaError_t*);
+
+// ------------------------------------------------ constant-divisor proof
+// Counts the mantissas x in [1, 2) where fma(x, zh, x*zl) != x / d.  Both
+// sides scale exactly with x by powers of two while x*zl and the quotient
+// stay normal, so zero mismatches prove the identity for every dividend in
+// that exponent range (and for zero).
+__global__ void const_div_check_kernel(float d, float zh, float zl, unsigned int* bad) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= (1u << 23)) return;
+    const float x = __uint_as_float(0x3F800000u | m);
+    const float want = __fdiv_rn(x, d);
+    const float got = __fmaf_rn(x, zh, __fmul_rn(x, zl));
+    const bool ok = __float_as_uint(got) == __float_as_uint(want);
+    const unsigned int nbad = __popc(__ballot_sync(0xffffffffu, !ok));
+    if (nbad && (threadIdx.x & 31) == 0) atomicAdd(bad, nbad);
+}
+
+__device__ unsigned int g_const_div_bad;
+
+bool const_div_proven(float d, float zh, float zl, cudaStream_t st) {
+    static std::mutex mu;
+    static std::map<std::tuple<uint32_t, uint32_t, uint32_t>, bool> cache;
+    uint32_t kd, kh, kl;
+    memcpy(&kd, &d, 4);
+    memcpy(&kh, &zh, 4);
+    memcpy(&kl, &zl, 4);
+    const auto key = std::make_tuple(kd, kh, kl);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    unsigned int* bad = nullptr;
+    if (cudaGetSymbolAddress((void**)&bad, g_const_div_bad) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    unsigned int nbad = 1;
+    if (cudaMemsetAsync(bad, 0, sizeof(unsigned int), st) != cudaSuccess) return false;
+    const_div_check_kernel<<<(1u << 23) / 256, 256, 0, st>>>(d, zh, zl, bad);
+    if (cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const bool ok = (nbad == 0);
+    cache[key] = ok;
+    return ok;
+}
 
 }  // namespace gt

@@ -263,3 +263,18 @@ def test_strip_segments_and_generic_fallback(oracle, diam, sep):
     df = gt.batch(frames, diam, tqdm=False, **kw)
     tab = oracle.batch(trackpy_params(diam, **kw), frames.astype(np.float32))
     assert_same(df, tab, ["frame", "y", "x", "mass", "Rg", "raw", "signal", "ecc"])
+
+
+@pytest.mark.parametrize("dtype,width", [(np.uint16, 520), (np.uint16, 522), (np.uint8, 520), (np.float32, 520),
+                                         (np.uint16, 1030)])
+def test_strip_interior_strips_and_pixel_types(oracle, dtype, width):
+    """Frames wide enough for interior strips (4-pixel staging loads), a width
+    that is not a multiple of 4 (per-pixel staging), and every pixel type."""
+    kw = dict(bg=40.0, amp_mu=np.log(120.0)) if dtype == np.uint8 else {}
+    if dtype == np.float32:
+        kw = dict(read_noise=4.0, bg=50.0)
+    frames, _ = video(2, 260, width, 150, seed=width + 7, dtype=dtype, **kw)
+    mm = 60.0 if dtype == np.uint8 else 300.0
+    df = gt.batch(frames, 11, minmass=mm, tqdm=False)
+    tab = oracle.batch(trackpy_params(11, minmass=mm), frames.astype(np.float32))
+    assert_same(df, tab, ALL_TP)
