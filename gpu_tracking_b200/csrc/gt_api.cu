@@ -324,6 +324,13 @@ gt_status make_locate_consts(gt_ctx* ctx, const gt_params& p, int32_t H, int32_t
     c.image_std = 0.0f;
     c.rough = p.has_adaptive_background ? 0.5f : 1.0f;
     c.characterize = p.characterize ? 1 : 0;
+    {
+        const int rint = std::max(0, (c.circle - 1) / 2);
+        c.skip_zero = (p.style == GT_STYLE_TRACKPY && c.truncate && p.minmass > 0.0f && c.o >= rint &&
+                       c.kd - 1 - c.o >= rint)
+                          ? 1
+                          : 0;
+    }
     return GT_OK;
 }
 
@@ -828,7 +835,7 @@ struct Chunking {
 int pick_chunk(int64_t T, int32_t H, int32_t W, int n_planes) {
     const size_t px = (size_t)H * W;
     size_t per_frame = px * 4 * (1 + n_planes);
-    int F = (int)std::max<size_t>(1, (size_t)(256u << 20) / per_frame);
+    int F = (int)std::max<size_t>(1, (size_t)(1024u << 20) / per_frame);
     F = std::min<int>(F, 64);
     F = (int)std::min<int64_t>(F, T);
     return std::max(F, 1);

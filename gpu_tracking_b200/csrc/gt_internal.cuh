@@ -64,6 +64,12 @@ struct LocateConsts {
     // where the check carries over (integer pixel types).
     int32_t fast_div;
     float zh_g, zl_g, zh_k, zl_k;
+    // Candidates at a processed value of exactly 0 may be left out: with
+    // truncation every processed value is 0 or >= 1/255, so such a pixel's
+    // whole dilation window is 0; when that window covers the walk circle the
+    // walk ends where it started with mass 0 (0/0 centroid moves nothing),
+    // and minmass > 0 rejects it (walk_keep, walk.wgsl).
+    int32_t skip_zero;
     float taps[kMaxTaps];
 };
 

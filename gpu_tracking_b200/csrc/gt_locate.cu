@@ -125,6 +125,7 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
         if (gr < c.margin || gr >= H - c.margin || gc < c.margin || gc >= W - c.margin) continue;
         float center = sp[(r + o) * PW + cc + o];
         if (center < c.thr) continue;
+        if (c.skip_zero && center == 0.0f) continue;
         float m = -INFINITY;
         for (int j = 0; j < kd; j++) m = fmaxf(m, sv[r * PW + cc + j]);
         if (m > center) continue;

@@ -56,10 +56,12 @@ struct StripGeom {
     static constexpr int RAWVPT = (RAWV + kStripThreads - 1) / kStripThreads;
     static constexpr int RAWN = kStepRows * RWp;
     static constexpr int RAWPT = (RAWN + kStripThreads - 1) / kStripThreads;
+    // the vertical maxima (stages D-E) reuse the staged raw rows (stages A-B)
     static constexpr size_t smem_floats = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp +
-                                          (size_t)(2 * PR) * PWp + (size_t)kStepRows * PWp;
+                                          (size_t)(2 * PR) * PWp;
     static constexpr int min_blocks = (smem_floats * 4 + 1024) * 3 <= 227 * 1024 ? 3 : 2;
     static_assert(RWp % 4 == 0 && RWp >= PWp + 2 * R, "staged raw row");
+    static_assert(RWp >= PWp, "vertical maxima fit in the staging rows");
     static_assert(4 * 31 + 4 * NV4 <= PWp, "dilation row reads stay in the row");
     static_assert(4 * 31 + KD + 2 <= PW - 1 && SH4 + O + kStripTW <= PWp, "dilation windows inside the row");
 };
@@ -125,7 +127,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     float* xg = stage + kStepRows * RWp;        // [2XR][PWp]    row pass g / gnorm, rows stored twice
     float* xb = xg + 2 * XR * PWp;              // [2XR][PWp]    row pass boxcar
     float* pr = xb + 2 * XR * PWp;              // [2PR][PWp]    processed rows, stored twice
-    float* vb = pr + 2 * PR * PWp;              // [8][PWp]      vertical maxima (pc0-relative columns)
+    float* vb = stage;                          // [8][PWp]      vertical maxima (pc0-relative columns)
 
     const int H = c.H, W = c.W;
     const int f = blockIdx.z;
@@ -393,6 +395,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                         if (!rows_ok || gc < c.margin || gc >= W - c.margin) continue;
                         const float center = cen[k];
                         if (center < c.thr) continue;
+                        if (c.skip_zero && center == 0.0f) continue;
                         if (m[k] > center) continue;
                         cmask |= 1u << k;
                         cnt++;
@@ -402,6 +405,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                 }
             }
             // warp-aggregated reservation of output slots
+            if (__any_sync(0xffffffffu, cnt != 0)) {
             const int lane = tid & 31;
             int incl = cnt;
 #pragma unroll
@@ -422,6 +426,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                 if (pos < cand_cap) cout[pos] = (uint32_t)cd * (uint32_t)W + (uint32_t)(ccol + k);
                 else atomicOr(flags, kFlagCandOverflow);
                 pos++;
+            }
             }
         }
         __syncthreads();
@@ -444,6 +449,8 @@ cudaError_t strip_launch(const T* frames, int64_t frame_stride, float* processed
     const int vec_ok = (c.W % 4 == 0) && (frame_stride % 4 == 0) &&
                        ((uintptr_t)frames % (4 * sizeof(T)) == 0) ? 1 : 0;
     cudaFuncSetAttribute(strip_kernel<T, R, KD, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(strip_kernel<T, R, KD, FAST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     strip_kernel<T, R, KD, FAST><<<grid, kStripThreads, smem, st>>>(frames, frame_stride, processed, c, SH, vec_ok,
                                                                      cand_count, cand_keys, cand_cap, flags);
     return cudaGetLastError();

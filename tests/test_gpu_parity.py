@@ -278,3 +278,30 @@ def test_strip_interior_strips_and_pixel_types(oracle, dtype, width):
     df = gt.batch(frames, 11, minmass=mm, tqdm=False)
     tab = oracle.batch(trackpy_params(11, minmass=mm), frames.astype(np.float32))
     assert_same(df, tab, ALL_TP)
+
+
+def plateau_video():
+    """Noise-free background with a few spots: the processed image is exactly
+    0 on wide plateaus, whose pixels are all local maxima."""
+    rng = np.random.default_rng(3)
+    fr = np.full((2, 96, 100), 100.0)
+    yy, xx = np.mgrid[0:96, 0:100]
+    for t in range(2):
+        for _ in range(6):
+            y, x = rng.uniform(10, 86), rng.uniform(10, 90)
+            fr[t] += 600 * np.exp(-((yy - y) ** 2 + (xx - x) ** 2) / (2 * 1.5 ** 2))
+    return np.round(fr).astype(np.uint16)
+
+
+@pytest.mark.parametrize("minmass", [0.0, 100.0])
+def test_zero_plateau_candidates(oracle, minmass):
+    """minmass = 0 keeps the walks of zero-valued local maxima (mass 0 >= 0),
+    so none may be left out; with minmass > 0 they are all rejected and the
+    kernels skip them."""
+    frames = plateau_video()
+    kw = dict(minmass=minmass, separation=14)
+    df = gt.batch(frames, 9, tqdm=False, **kw)
+    tab = oracle.batch(trackpy_params(9, **kw), frames.astype(np.float32))
+    if minmass == 0.0:
+        assert (df["mass"] == 0).sum() > 1000
+    assert_same(df, tab, ALL_TP)
