@@ -183,4 +183,30 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total, int* wsum) {
     return wsum[wid] + incl - v;
 }
 
+// Block-wide exclusive scan of one 64-bit value per thread (blockDim <= 1024).
+__device__ __forceinline__ long long block_excl_scan64(long long v, long long* total, long long* wsum) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    long long incl = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        long long t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        long long x = (lane < nw) ? wsum[lane] : 0;
+        long long s = x;
+        for (int d = 1; d < 32; d <<= 1) {
+            long long t = __shfl_up_sync(0xffffffffu, s, d);
+            if (lane >= d) s += t;
+        }
+        if (lane < nw) wsum[lane] = s - x;
+        if (lane == 31) wsum[32] = s;
+    }
+    __syncthreads();
+    *total = wsum[32];
+    return wsum[wid] + incl - v;
+}
+
 }  // namespace gt

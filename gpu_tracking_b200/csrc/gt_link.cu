@@ -25,6 +25,8 @@ namespace gt {
 constexpr int kLinkThreads = 1024;
 constexpr int kSortSmem = 4096;
 constexpr long long kSubnetBudget = 1ll << 28;
+constexpr int kLagRegs = 4;     // backward-list offsets of up to 4 lags held in registers
+constexpr int kRingSmem = 64;   // memory ring bookkeeping in shared memory up to memory = 64
 
 // ------------------------------------------------------- point addressing
 __device__ __forceinline__ int64_t gbase(const LinkInput& in, int g) {
@@ -190,7 +192,8 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
 
 // ---------------------------------------------------------- scratch layout
 struct Lay {
-    size_t start, idstamp, firstpos, srcidx, srcstamp, src_pt, ring_pt, ring_n, ringpre, d_off, e_src, e_dist,
+    size_t start, idstamp, firstpos, srcidx, srcstamp, src_pt, ring_pt, ring_n, ringpre, d_off, d_end, sf0, sf1,
+        e_src, e_dist,
         out_src, parent, comp_nd, comp_ns, comp_off, comp_soff, roots, pathD, pathS, srcLocal, srcUsed, vis_d,
         vis_s, stack, r2a, r2b, r2c, r2used, tmp, total;
 };
@@ -211,6 +214,9 @@ __host__ __device__ inline Lay make_lay(int64_t G, int64_t E, int64_t NP, int64_
     l.ring_n = o; o = al(o + 4 * (M + 1));
     l.ringpre = o; o = al(o + 4 * (M + 2));
     l.d_off = o; o = al(o + 4 * (G + 1));
+    l.d_end = o; o = al(o + 4 * (G + 1));
+    l.sf0 = o; o = al(o + 8 * Smax);
+    l.sf1 = o; o = al(o + 8 * Smax);
     l.e_src = o; o = al(o + 4 * (E + 1));
     l.e_dist = o; o = al(o + 4 * (E + 1));
     l.out_src = o; o = al(o + 4 * G);
@@ -272,6 +278,8 @@ __device__ __forceinline__ void uf_union(volatile int* parent, int a, int b) {
 __global__ void __launch_bounds__(kLinkThreads)
 link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, LinkWindow W) {
     __shared__ int wsum[33];
+    __shared__ long long wsum64[33];
+    __shared__ int sh_ring_n[kRingSmem + 1], sh_ringpre[kRingSmem + 2];
     __shared__ long long sh_counter, sh_frame, sh_load;
     __shared__ int sh_prevg, sh_head, sh_nroots, sh_ringtot;
     const int v = blockIdx.x;
@@ -294,6 +302,9 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
     int32_t* ring_n = (int32_t*)(base + lay.ring_n);
     int32_t* ringpre = (int32_t*)(base + lay.ringpre);
     int32_t* d_off = (int32_t*)(base + lay.d_off);
+    int32_t* d_end = (int32_t*)(base + lay.d_end);
+    int64_t* sf0 = (int64_t*)(base + lay.sf0);
+    int64_t* sf1 = (int64_t*)(base + lay.sf1);
     int32_t* e_src = (int32_t*)(base + lay.e_src);
     float* e_dist = (float*)(base + lay.e_dist);
     int32_t* out_src = (int32_t*)(base + lay.out_src);
@@ -322,6 +333,10 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
     const float R2 = __fmul_rn(R, R);
     const int tid = threadIdx.x, nth = blockDim.x;
 
+    // ring sizes and their prefix live in shared memory for memory <= kRingSmem
+    const bool ring_smem = M <= kRingSmem;
+    int32_t* ringN = ring_smem ? sh_ring_n : ring_n;
+    int32_t* ringP = ring_smem ? sh_ringpre : ringpre;
     if (W.first) {
         if (W.init_points) {
             for (int64_t i = tid; i < NP; i += nth) {
@@ -332,14 +347,18 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         }
         for (int i = tid; i < Smax; i += nth) vis_s[i] = -1;
         for (int i = tid; i < G; i += nth) vis_d[i] = -1;
-        for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
+        for (int i = tid; i <= M; i += nth) ringN[i] = 0;
         if (tid == 0) {
             sh_counter = 0;
             sh_frame = 0;
             sh_prevg = -1;
             sh_head = 0;
         }
-    } else if (tid == 0) {
+    } else {
+        if (ring_smem)
+            for (int i = tid; i <= M; i += nth) ringN[i] = ring_n[i];
+    }
+    if (!W.first && tid == 0) {
         const LinkState st = W.state[v];
         sh_counter = st.counter;
         sh_frame = st.frame;
@@ -358,7 +377,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
                 sh_prevg = -1;
                 sh_head = 0;
             }
-            for (int i = tid; i <= M; i += nth) ring_n[i] = 0;
+            for (int i = tid; i <= M; i += nth) ringN[i] = 0;
             __syncthreads();
         }
         const int64_t a = gbase(in, g);
@@ -367,154 +386,158 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         const int S0 = (prevg == g - 1 && prevg >= gb) ? (int)gsize(in, g - 1) : 0;
         const int64_t pa = (S0 > 0) ? gbase(in, g - 1) : 0;
         // ---- P1: sources = previous frame + memory entries not already present
-        for (int i = tid; i < S0; i += nth) {
-            int64_t pt = pa + i;
-            int64_t id = ids[pt];
-            idstamp[id] = step;
-            src_pt[i] = (int32_t)(pt - P0);
-            srcidx[pt - P0] = i;
-            srcstamp[pt - P0] = step;
+        for (int i0 = 2 * tid; i0 < S0; i0 += 2 * nth) {
+            const int n2 = min(2, S0 - i0);
+            int64_t idv[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+                if (u < n2) idv[u] = ids[pa + i0 + u];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                if (u >= n2) break;
+                const int i = i0 + u;
+                const int64_t lp = pa + i - P0;
+                idstamp[idv[u]] = step;
+                src_pt[i] = (int32_t)lp;
+                srcidx[lp] = i;
+                srcstamp[lp] = step;
+            }
         }
         if (tid == 0) {
             int tot = 0;
             for (int q = 0; q < M; q++) {
-                ringpre[q] = tot;
-                tot += ring_n[(sh_head + q) % M];
+                ringP[q] = tot;
+                tot += ringN[(sh_head + q) % M];
             }
-            ringpre[M] = tot;
+            ringP[M] = tot;
             sh_ringtot = tot;
         }
         __syncthreads();
         const int RT = (M > 0) ? sh_ringtot : 0;
         // ring entries in ring order: position r -> (slot q, entry e)
-        for (int r = tid; r < RT; r += nth) {
+        auto ring_lp = [&](int r) -> int32_t {
             int q = 0;
-            while (ringpre[q + 1] <= r) q++;
-            int slot = (sh_head + q) % M;
-            int32_t lp = ring_pt[slot * G + (r - ringpre[q])];
-            int64_t id = ids[P0 + lp];
+            while (ringP[q + 1] <= r) q++;
+            const int slot = (sh_head + q) % M;
+            return ring_pt[slot * G + (r - ringP[q])];
+        };
+        for (int r = tid; r < RT; r += nth) {
+            const int64_t id = ids[P0 + ring_lp(r)];
             if (idstamp[id] != step)
                 atomicMax(&firstpos[id], ((unsigned long long)(uint32_t)step << 32) | (0xFFFFFFFFull - (uint32_t)r));
         }
         __syncthreads();
         int kept_tot = 0;
-        for (int base0 = 0; base0 < RT; base0 += nth) {
-            int r = base0 + tid;
-            int keep = 0;
-            int32_t lp = 0;
-            if (r < RT) {
-                int q = 0;
-                while (ringpre[q + 1] <= r) q++;
-                int slot = (sh_head + q) % M;
-                lp = ring_pt[slot * G + (r - ringpre[q])];
-                int64_t id = ids[P0 + lp];
-                keep = (idstamp[id] != step) &&
-                       firstpos[id] == (((unsigned long long)(uint32_t)step << 32) | (0xFFFFFFFFull - (uint32_t)r));
+        for (int base0 = 0; base0 < RT; base0 += 2 * nth) {
+            int keep[2] = {0, 0};
+            int32_t lpv[2] = {0, 0};
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int r = base0 + 2 * tid + u;
+                if (r < RT) {
+                    lpv[u] = ring_lp(r);
+                    const int64_t id = ids[P0 + lpv[u]];
+                    keep[u] = (idstamp[id] != step) &&
+                              firstpos[id] ==
+                                  (((unsigned long long)(uint32_t)step << 32) | (0xFFFFFFFFull - (uint32_t)r));
+                }
             }
             int tot;
-            int pos = block_excl_scan(keep, &tot, wsum);
-            if (keep) {
-                int si = S0 + kept_tot + pos;
-                src_pt[si] = lp;
-                srcidx[lp] = si;
-                srcstamp[lp] = step;
+            const int pos = block_excl_scan(keep[0] + keep[1], &tot, wsum);
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                if (!keep[u]) continue;
+                const int si = S0 + kept_tot + pos + (u ? keep[0] : 0);
+                src_pt[si] = lpv[u];
+                srcidx[lpv[u]] = si;
+                srcstamp[lpv[u]] = step;
             }
             kept_tot += tot;
         }
         const int Sn = S0 + kept_tot;
         __syncthreads();
-        // ---- P2: destination -> source lists (ascending source index)
-        int etot = 0;
-        for (int base0 = 0; base0 < D; base0 += nth) {
-            int j = base0 + tid;
-            int deg = 0;
-            if (j < D) {
-                int64_t pt = a + j;
-                if (S0 > 0) deg += (int)(L.b_off[lix(L, pt, K, 1)] - L.b_off[lix(L, pt, K, 0)]);
-                for (int k = K; k >= 2; k--) {
-                    int t = g - k;
-                    if (t < gb) continue;
-                    int64_t o0 = L.b_off[lix(L, pt, K, k - 1)], o1 = L.b_off[lix(L, pt, K, k)];
-                    int64_t ta = gbase(in, t) - P0;
-                    for (int64_t e = o0; e < o1; e++)
-                        if (srcstamp[ta + L.b_pts[e]] == step) deg++;
-                }
-            }
-            int tot;
-            int pos = block_excl_scan(deg, &tot, wsum);
-            if (j < D) d_off[j] = etot + pos;
-            etot += tot;
-        }
-        if (tid == 0) d_off[D] = etot;
-        __syncthreads();
-        if (etot > S.max_edges) {
+        // ---- P2: destination -> source lists (ascending source index).  The
+        // edges of destination j go to its own range of the frame's backward
+        // lists, whose size bounds the kept edges: [d_off[j], d_end[j]).
+        const int64_t fb = L.b_off[lix(L, a, K, 0)];
+        if (L.b_off[lix(L, a + D, K, 0)] - fb > S.max_edges) {
             if (tid == 0) atomicOr(out.flags + v, in.slot_stride ? kFlagEdgeOverflow : kFlagScratch);
             break;
         }
         for (int j = tid; j < D; j += nth) {
-            int64_t pt = a + j;
-            int w = d_off[j];
+            const int64_t pt = a + j;
+            const int64_t lb = lix(L, pt, K, 0);
+            int64_t bo[kLagRegs + 1];
+            const bool regs = K <= kLagRegs;
+#pragma unroll
+            for (int i = 0; i <= kLagRegs; i++)
+                if (regs && i <= K) bo[i] = L.b_off[lb + i];
+            const int64_t b0 = regs ? bo[0] : L.b_off[lb];
+            int w = (int)(b0 - fb);
+            d_off[j] = w;
             if (S0 > 0) {
-                int64_t o0 = L.b_off[lix(L, pt, K, 0)], o1 = L.b_off[lix(L, pt, K, 1)];
-                for (int64_t e = o0; e < o1; e++) {
+                const int64_t o1 = regs ? bo[1] : L.b_off[lb + 1];
+                for (int64_t e = b0; e < o1; e++) {
                     e_src[w] = L.b_pts[e];  // index within group g-1 == source index
                     e_dist[w] = L.b_dist[e];
                     w++;
                 }
             }
-            for (int k = K; k >= 2; k--) {
-                int t = g - k;
-                if (t < gb) continue;
-                int64_t o0 = L.b_off[lix(L, pt, K, k - 1)], o1 = L.b_off[lix(L, pt, K, k)];
-                int64_t ta = gbase(in, t) - P0;
+            // lags K..2: only sources that are in this step's source list
+            auto lag = [&](int k, int64_t o0, int64_t o1) {
+                const int t = g - k;
+                if (t < gb) return;
+                const int64_t ta = gbase(in, t) - P0;
                 for (int64_t e = o0; e < o1; e++) {
-                    int64_t lp = ta + L.b_pts[e];
+                    const int64_t lp = ta + L.b_pts[e];
                     if (srcstamp[lp] == step) {
                         e_src[w] = srcidx[lp];
                         e_dist[w] = L.b_dist[e];
                         w++;
                     }
                 }
+            };
+            if (regs) {
+#pragma unroll
+                for (int k = kLagRegs; k >= 2; k--)
+                    if (k <= K) lag(k, bo[k - 1], bo[k]);
+            } else {
+                for (int k = K; k >= 2; k--) lag(k, L.b_off[lb + k - 1], L.b_off[lb + k]);
             }
+            d_end[j] = w;
             parent[j] = j;
             out_src[j] = -2;
         }
+        // ---- P3: trivial links and subnets (connected components)
+        // forward range of every source toward this frame, read once
         for (int s = tid; s < Sn; s += nth) {
+            const int64_t pt = P0 + src_pt[s];
+            const int64_t l = lix(L, pt, K, g - ggroup(in, pt) - 1);
+            const int64_t f0 = L.f_off[l], f1 = L.f_off[l + 1];
+            sf0[s] = f0;
+            sf1[s] = f1;
             srcUsed[s] = 0;
         }
         __syncthreads();
-        // ---- P3: trivial links and subnets (connected components)
-        // forward list of source s toward this frame
-        auto fwd = [&](int s, int64_t* f0, int64_t* f1) {
-            int64_t lp = src_pt[s];
-            int64_t pt = P0 + lp;
-            int k = g - ggroup(in, pt);
-            *f0 = L.f_off[lix(L, pt, K, k - 1)];
-            *f1 = L.f_off[lix(L, pt, K, k)];
-        };
+        for (int s = tid; s < Sn; s += nth) {
+            const int64_t f0 = sf0[s], f1 = sf1[s];
+            if (f1 - f0 >= 2) {
+                const int j0 = L.f_pts[f0];
+                for (int64_t e = f0 + 1; e < f1; e++) uf_union(parent, j0, L.f_pts[e]);
+            }
+        }
         for (int j = tid; j < D; j += nth) {
-            int deg = d_off[j + 1] - d_off[j];
+            const int e0 = d_off[j], deg = d_end[j] - e0;
             if (deg == 0) {
                 out_src[j] = -1;
             } else if (deg == 1) {
-                int s = e_src[d_off[j]];
-                int64_t f0, f1;
-                fwd(s, &f0, &f1);
-                if (f1 - f0 == 1) out_src[j] = s;
-            }
-        }
-        for (int s = tid; s < Sn; s += nth) {
-            int64_t f0, f1;
-            fwd(s, &f0, &f1);
-            if (f1 - f0 >= 2) {
-                int j0 = L.f_pts[f0];
-                for (int64_t e = f0 + 1; e < f1; e++) uf_union(parent, j0, L.f_pts[e]);
+                const int s = e_src[e0];
+                if (sf1[s] - sf0[s] == 1) out_src[j] = s;
             }
         }
         __syncthreads();
         for (int j = tid; j < D; j += nth) {
-            int r = uf_find(parent, j);
-            tmp[j] = r;
+            tmp[j] = uf_find(parent, j);
             comp_nd[j] = 0;
             comp_ns[j] = 0;
         }
@@ -522,36 +545,47 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         for (int j = tid; j < D; j += nth)
             if (out_src[j] == -2) atomicAdd(&comp_nd[tmp[j]], 1);
         for (int s = tid; s < Sn; s += nth) {
-            int64_t f0, f1;
-            fwd(s, &f0, &f1);
-            if (f1 > f0) {
-                int j0 = L.f_pts[f0];
+            const int64_t f0 = sf0[s];
+            if (sf1[s] > f0) {
+                const int j0 = L.f_pts[f0];
                 if (out_src[j0] == -2) atomicAdd(&comp_ns[tmp[j0]], 1);
             }
         }
         __syncthreads();
         {
-            int nr = 0, offd = 0, offs = 0;
-            for (int base0 = 0; base0 < D; base0 += nth) {
-                int j = base0 + tid;
-                int isroot = (j < D && out_src[j] == -2 && tmp[j] == j) ? 1 : 0;
-                int nd = isroot ? comp_nd[j] : 0;
-                int ns = isroot ? comp_ns[j] : 0;
-                int t1, t2, t3;
-                int p1 = block_excl_scan(isroot, &t1, wsum);
-                int p2 = block_excl_scan(nd, &t2, wsum);
-                int p3 = block_excl_scan(ns, &t3, wsum);
-                if (isroot) {
-                    roots[nr + p1] = j;
-                    comp_off[j] = offd + p2;
-                    comp_soff[j] = offs + p3;
+            // one 64-bit scan of (roots, destinations) and one of sources, two
+            // destinations per thread in destination order
+            long long acc_rd = 0;
+            int offs = 0;
+            for (int base0 = 0; base0 < D; base0 += 2 * nth) {
+                int isroot[2], nd[2], ns[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int j = base0 + 2 * tid + u;
+                    isroot[u] = (j < D && out_src[j] == -2 && tmp[j] == j) ? 1 : 0;
+                    nd[u] = isroot[u] ? comp_nd[j] : 0;
+                    ns[u] = isroot[u] ? comp_ns[j] : 0;
                 }
-                nr += t1;
-                offd += t2;
-                offs += t3;
+                const long long rd0 = (long long)isroot[0] + ((long long)nd[0] << 32);
+                const long long rd1 = (long long)isroot[1] + ((long long)nd[1] << 32);
+                long long trd;
+                int ts;
+                const long long prd = block_excl_scan64(rd0 + rd1, &trd, wsum64);
+                const int ps = block_excl_scan(ns[0] + ns[1], &ts, wsum);
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    if (!isroot[u]) continue;
+                    const int j = base0 + 2 * tid + u;
+                    const long long pr_ = acc_rd + prd + (u ? rd0 : 0);
+                    roots[(int)(pr_ & 0xFFFFFFFFll)] = j;
+                    comp_off[j] = (int)(pr_ >> 32);
+                    comp_soff[j] = offs + ps + (u ? ns[0] : 0);
+                }
+                acc_rd += trd;
+                offs += ts;
             }
             if (tid == 0) {
-                sh_nroots = nr;
+                sh_nroots = (int)(acc_rd & 0xFFFFFFFFll);
                 sh_load = 0;
             }
         }
@@ -571,7 +605,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
                 int2& top = stk[sp - 1];
                 if (top.x >= 0) {  // destination: its sources in list order
                     const int j = top.x;
-                    const int e0 = d_off[j], e1 = d_off[j + 1];
+                    const int e0 = d_off[j], e1 = d_end[j];
                     bool pushed = false;
                     while (e0 + top.y < e1) {
                         int s = e_src[e0 + top.y];
@@ -588,8 +622,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
                     if (!pushed) sp--;
                 } else {  // source: its destinations in list order
                     const int s = -top.x - 1;
-                    int64_t f0, f1;
-                    fwd(s, &f0, &f1);
+                    const int64_t f0 = sf0[s], f1 = sf1[s];
                     bool pushed = false;
                     while (f0 + top.y < f1) {
                         int j = L.f_pts[f0 + top.y];
@@ -633,7 +666,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
                 if (++budget > kSubnetBudget) { over = true; break; }
                 const int j = pathD[od + level];
                 const int e0 = d_off[j];
-                const int deg = d_off[j + 1] - e0;
+                const int deg = d_end[j] - e0;
                 const int o = opt[level];
                 bool ascend = false;
                 if (o > deg) {
@@ -675,7 +708,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
                     if (level < 0) break;
                     const int jp = pathD[od + level];
                     const int ep = d_off[jp];
-                    const int degp = d_off[jp + 1] - ep;
+                    const int degp = d_end[jp] - ep;
                     const int op = opt[level];
                     const bool nullp = (op == degp);
                     const float cp = nullp ? R2 : e_dist[ep + op];
@@ -697,19 +730,27 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
             int newtot = 0;
             const long long counter = sh_counter;
             const long long frame = sh_frame;
-            for (int base0 = 0; base0 < D; base0 += nth) {
-                int j = base0 + tid;
-                int isnew = (j < D && out_src[j] < 0) ? 1 : 0;
+            for (int base0 = 0; base0 < D; base0 += 2 * nth) {
+                int osrc[2], isnew[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int j = base0 + 2 * tid + u;
+                    osrc[u] = (j < D) ? out_src[j] : 0;
+                    isnew[u] = (j < D && osrc[u] < 0) ? 1 : 0;
+                }
                 int tot;
-                int pos = block_excl_scan(isnew, &tot, wsum);
-                if (j < D) {
-                    int64_t pt = a + j;
-                    if (isnew) {
-                        long long id = counter + newtot + pos;
+                const int pos = block_excl_scan(isnew[0] + isnew[1], &tot, wsum);
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int j = base0 + 2 * tid + u;
+                    if (j >= D) break;
+                    const int64_t pt = a + j;
+                    if (isnew[u]) {
+                        const long long id = counter + newtot + pos + (u ? isnew[0] : 0);
                         ids[pt] = id;
                         start[id] = frame;
                     } else {
-                        int s = out_src[j];
+                        const int s = osrc[u];
                         ids[pt] = ids[P0 + src_pt[s]];
                         srcUsed[s] = 1;
                     }
@@ -724,23 +765,29 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
             const long long frame = sh_frame;
             if (M > 0) {
                 const int hs = sh_head;
-                const int nleave = ring_n[hs];
+                const int nleave = ringN[hs];
                 for (int e = tid; e < nleave; e += nth) {
                     int64_t id = ids[P0 + ring_pt[hs * G + e]];
                     dur[id] = (frame - start[id]) - M;
                 }
                 __syncthreads();
                 int ut = 0;
-                for (int base0 = 0; base0 < S0; base0 += nth) {
-                    int s = base0 + tid;
-                    int un = (s < S0 && !srcUsed[s]) ? 1 : 0;
+                for (int base0 = 0; base0 < S0; base0 += 2 * nth) {
+                    int un[2];
+#pragma unroll
+                    for (int u = 0; u < 2; u++) {
+                        const int s = base0 + 2 * tid + u;
+                        un[u] = (s < S0 && !srcUsed[s]) ? 1 : 0;
+                    }
                     int tot;
-                    int pos = block_excl_scan(un, &tot, wsum);
-                    if (un) ring_pt[hs * G + ut + pos] = src_pt[s];
+                    const int pos = block_excl_scan(un[0] + un[1], &tot, wsum);
+#pragma unroll
+                    for (int u = 0; u < 2; u++)
+                        if (un[u]) ring_pt[hs * G + ut + pos + (u ? un[0] : 0)] = src_pt[base0 + 2 * tid + u];
                     ut += tot;
                 }
                 if (tid == 0) {
-                    ring_n[hs] = ut;
+                    ringN[hs] = ut;
                     sh_head = (hs + 1) % M;
                 }
             } else {
@@ -761,6 +808,8 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
     }
     __syncthreads();
     if (!W.last) {
+        if (ring_smem)
+            for (int i = tid; i <= M; i += nth) ring_n[i] = ringN[i];
         if (tid == 0 && !(out.flags[v] & kLinkStopFlags)) {
             LinkState st;
             st.counter = sh_counter;
@@ -777,7 +826,7 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         if (M > 0) {
             for (int q = 0; q < M; q++) {
                 int slot = (sh_head + q) % M;
-                int n = ring_n[slot];
+                int n = ringN[slot];
                 for (int e = tid; e < n; e += nth) {
                     int64_t id = ids[P0 + ring_pt[slot * G + e]];
                     dur[id] = (frame - start[id]) - (M - q);
