@@ -351,6 +351,153 @@ walk_kernel(const float* __restrict__ processed, const T* __restrict__ frames, i
     else atomicOr(flags, kFlagFeatOverflow);
 }
 
+// ------------------------------------------------ walk for a fixed radius
+// The trackpy circle has integer radius RI = (diameter - 1) / 2: membership
+// of an offset (i*i + j*j <= RI*RI, exact in float) is decided at compile
+// time, the loops unroll completely so every load is independent, and a
+// circle that lies inside the frame skips the bounds tests.  The operation
+// sequence per output is the one of get_center / walk / characterize above.
+template <int RI, bool CHECK>
+__device__ __forceinline__ WalkRes get_center_fixed(const float* __restrict__ p, int H, int W, int u, int v) {
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const float* pc = p + (ptrdiff_t)u * W + v;
+#pragma unroll
+    for (int i = -RI; i <= RI; i++) {
+        const float* prow = pc + (ptrdiff_t)i * W;
+        const bool row_in = !CHECK || (u + i >= 0 && u + i < H);
+#pragma unroll
+        for (int j = -RI; j <= RI; j++) {
+            if (i * i + j * j > RI * RI) continue;
+            if (CHECK && (!row_in || v + j < 0 || v + j >= W)) continue;
+            const float data = __ldg(prow + j);
+            res.x = __fmaf_rn(data, (float)i, res.x);
+            res.y = __fmaf_rn(data, (float)j, res.y);
+            res.mass = __fadd_rn(res.mass, data);
+            res.count = __fadd_rn(res.count, 1.0f);
+            res.max = wgsl_max(res.max, data);
+        }
+    }
+    res.x = __fdiv_rn(res.x, res.mass);
+    res.y = __fdiv_rn(res.y, res.mass);
+    return res;
+}
+
+template <int RI>
+__device__ __forceinline__ WalkRes walk_fixed(const float* __restrict__ p, const LocateConsts& c, int u0, int v0) {
+    int pu = u0, pv = v0;
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const int H = c.H, W = c.W;
+    const float thr = c.shift_thr;
+    for (uint32_t it = 0; it < c.max_iter; it++) {
+        if (pu >= RI && pu + RI < H && pv >= RI && pv + RI < W)
+            res = get_center_fixed<RI, false>(p, H, W, pu, pv);
+        else
+            res = get_center_fixed<RI, true>(p, H, W, pu, pv);
+        bool changed = false;
+        if ((res.x > thr) && (pu < H - 1 - RI)) { pu += 1; changed = true; }
+        else if (res.x < -thr && pu > RI) { pu -= 1; changed = true; }
+        if ((res.y > thr) && (pv < W - 1 - RI)) { pv += 1; changed = true; }
+        else if ((res.y < -thr) && (pv > RI)) { pv -= 1; changed = true; }
+        if (!changed) break;
+    }
+    res.x = __fadd_rn(res.x, (float)pu);
+    res.y = __fadd_rn(res.y, (float)pv);
+    return res;
+}
+
+template <typename T, int RI, bool CHECK>
+__device__ __forceinline__ void characterize_fixed_at(const float* __restrict__ p, const T* __restrict__ raw, int H,
+                                                      int W, int u, int v, const float2* __restrict__ angles,
+                                                      float* Rg_, float* raw_mass_, float* signal_, float* es_,
+                                                      float* ec_) {
+    constexpr int side = 2 * RI + 1;
+    float Rg = 0.0f, raw_mass = 0.0f, signal = 0.0f, es = 0.0f, ec = 0.0f;
+    const ptrdiff_t cidx = (ptrdiff_t)u * W + v;
+#pragma unroll
+    for (int i = -RI; i <= RI; i++) {
+        const bool row_in = !CHECK || (u + i >= 0 && u + i < H);
+#pragma unroll
+        for (int j = -RI; j <= RI; j++) {
+            if (i * i + j * j > RI * RI) continue;
+            if (CHECK && (!row_in || v + j < 0 || v + j >= W)) continue;
+            const ptrdiff_t idx = cidx + (ptrdiff_t)i * W + j;
+            const float data = __ldg(p + idx);
+            Rg = __fmaf_rn(data, (float)(i * i + j * j), Rg);
+            raw_mass = __fadd_rn(raw_mass, load_px<T>(raw, (size_t)idx));
+            signal = wgsl_max(signal, data);
+            if ((i != 0) | (j != 0)) {
+                const float2 sc = __ldg(angles + (i + RI) * side + (j + RI));
+                es = __fmaf_rn(data, sc.x, es);
+                ec = __fmaf_rn(data, sc.y, ec);
+            } else {
+                ec = __fadd_rn(ec, data);
+            }
+        }
+    }
+    *Rg_ = Rg;
+    *raw_mass_ = raw_mass;
+    *signal_ = signal;
+    *es_ = es;
+    *ec_ = ec;
+}
+
+template <typename T, int RI>
+__global__ void __launch_bounds__(128)
+walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ frames, int64_t frame_stride,
+                  const LocateConsts c, const uint32_t* __restrict__ cand_count,
+                  const uint32_t* __restrict__ cand_keys, uint32_t cand_cap, const int32_t* __restrict__ angle_off,
+                  const float2* __restrict__ angles, Feature* __restrict__ feats, uint32_t* __restrict__ feat_count,
+                  uint32_t feat_cap, uint32_t* __restrict__ flags) {
+    const int f = blockIdx.y;
+    const uint32_t n = min(cand_count[f], cand_cap);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t key = cand_keys[(size_t)f * cand_cap + i];
+    const int u = (int)(key / (uint32_t)c.W), v = (int)(key % (uint32_t)c.W);
+    const int H = c.H, W = c.W;
+    const float* p = processed + (size_t)f * H * W;
+    const WalkRes res = walk_fixed<RI>(p, c, u, v);
+    float minmass;
+    if (c.minmass > 0.0f) minmass = c.minmass;
+    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.image_std), c.rough);
+    if (!(res.mass >= minmass)) return;
+    Feature ft;
+    ft.key_hi = 0;
+    ft.key_lo = key;
+    ft.x = res.x;
+    ft.y = res.y;
+    ft.mass = res.mass;
+    ft.r = 0.0f;
+    ft.max_i = res.max;
+    ft.count = res.count;
+    ft.Rg = ft.raw = ft.signal = ft.ecc = 0.0f;
+    ft.d_raw = ft.d_bg = ft.d_corr = __int_as_float(0x7fc00000);
+    ft.ridx = 0;
+    if (c.characterize) {
+        // characterize.wgsl:61-143 at the rounded position, radius RI
+        const T* raw = frames + (size_t)f * frame_stride;
+        const int cu = sat_f2i(rintf(ft.x)), cv = sat_f2i(rintf(ft.y));
+        const float2* ang = angles + angle_off[RI];
+        float middle = 0.0f;
+        const int64_t middle_idx = (int64_t)cu * W + cv;
+        if (middle_idx >= 0 && middle_idx < (int64_t)H * W) middle = __ldg(p + middle_idx);
+        float Rg, raw_mass, signal, es, ec;
+        if (cu >= RI && cu + RI < H && cv >= RI && cv + RI < W)
+            characterize_fixed_at<T, RI, false>(p, raw, H, W, cu, cv, ang, &Rg, &raw_mass, &signal, &es, &ec);
+        else
+            characterize_fixed_at<T, RI, true>(p, raw, H, W, cu, cv, ang, &Rg, &raw_mass, &signal, &es, &ec);
+        es = __fmul_rn(es, es);
+        ec = __fmul_rn(ec, ec);
+        ft.ecc = __fdiv_rn(__fsqrt_rn(__fadd_rn(es, ec)), __fsub_rn(ft.mass, middle));
+        ft.Rg = __fsqrt_rn(__fdiv_rn(Rg, ft.mass));
+        ft.raw = raw_mass;
+        ft.signal = signal;
+    }
+    uint32_t pos = atomicAdd(feat_count + f, 1u);
+    if (pos < feat_cap) feats[(size_t)f * feat_cap + pos] = ft;
+    else atomicOr(flags, kFlagFeatOverflow);
+}
+
 // characterize_points: characterize.wgsl with _feat_characterize_points (mass
 // recomputed at the rounded position); one thread per given point.
 template <typename T>
@@ -753,6 +900,18 @@ cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_s
                         uint32_t* flags, cudaStream_t st) {
     if (max_cands == 0) return cudaSuccess;
     dim3 grid((max_cands + 127) / 128, nframes, n_slots);
+    if (!radii && n_slots == 1) {
+        const int ri = (c.circle - 1) / 2;
+#define GT_WALK_FIXED(RI)                                                                                          \
+    if (ri == RI) {                                                                                                \
+        walk_kernel_fixed<T, RI><<<grid, 128, 0, st>>>(processed, frames, frame_stride, c, cand_count, cand_keys,  \
+                                                       cand_cap, angle_off, angles, feats, feat_count, feat_cap,   \
+                                                       flags);                                                     \
+        return cudaGetLastError();                                                                                 \
+    }
+        GT_WALK_FIXED(2) GT_WALK_FIXED(3) GT_WALK_FIXED(4) GT_WALK_FIXED(5) GT_WALK_FIXED(6) GT_WALK_FIXED(7)
+#undef GT_WALK_FIXED
+    }
     walk_kernel<T><<<grid, 128, 0, st>>>(processed, frames, frame_stride, c, cand_count, cand_keys, cand_cap, radii,
                                          angle_off, angles, feats, feat_count, feat_cap, flags, n_slots);
     return cudaGetLastError();
