@@ -1507,6 +1507,18 @@ void gt_params_default(gt_params* p) {
     p->n_radii = 10;
 }
 
+// The linker runs one frame after another in one CTA beside the locate
+// kernels; its stream gets the device's highest priority so that its CTAs are
+// placed before further locate CTAs whenever an SM frees up.
+static int link_stream_priority() {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return greatest;
+}
+
 gt_status gt_create(int32_t device, gt_ctx** out) {
     if (!out) return GT_ERR_INVALID_ARGUMENT;
     *out = nullptr;
@@ -1521,7 +1533,7 @@ gt_status gt_create(int32_t device, gt_ctx** out) {
     ctx->device = device;
     if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->lk, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->lk, cudaStreamNonBlocking, link_stream_priority()) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->located, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->linked, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;

@@ -636,9 +636,65 @@ __device__ float warp_upper_median(const T* __restrict__ raw, int H, int W, int 
     return float_from_order_key(prefix);
 }
 
+// Same upper median with the annulus held in registers (up to 32 *
+// kMedianRegs pixels, loaded once): the key of rank len/2 is built bit by
+// bit from the top, counting keys below each trial value with one warp
+// reduction; bits that every valid key shares are taken as they are.
+constexpr int kMedianRegs = 13;
+template <typename T>
+__device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ raw, int H, int W, int mu, int mv,
+                                        const short2* __restrict__ inds, int n_inds, int* n_out) {
+    const int lane = threadIdx.x & 31;
+    uint32_t key[kMedianRegs];
+    int nv = 0;
+    uint32_t kor = 0u, kand = 0xFFFFFFFFu;
+#pragma unroll
+    for (int q = 0; q < kMedianRegs; q++) {
+        const int k = q * 32 + lane;
+        key[q] = 0xFFFFFFFFu;  // never below a trial value: left out of every count
+        if (k < n_inds) {
+            const short2 d = inds[k];
+            const int64_t a = (int64_t)mu + d.x, b = (int64_t)mv + d.y;
+            if (a >= 0 && a < H && b >= 0 && b < W) {
+                key[q] = float_order_key(load_px<T>(raw, (size_t)a * W + b));
+                kor |= key[q];
+                kand &= key[q];
+                nv++;
+            }
+        }
+    }
+    int nvalid = nv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nvalid += __shfl_xor_sync(0xffffffffu, nvalid, o);
+    *n_out = nvalid;
+    if (nvalid == 0) return 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+        kand &= __shfl_xor_sync(0xffffffffu, kand, o);
+    }
+    const uint32_t diff = kor ^ kand;
+    if (diff == 0u) return float_from_order_key(kand);
+    const uint32_t want = (uint32_t)(nvalid / 2);
+    const int hb = 31 - __clz(diff), lb = __ffs(diff) - 1;
+    uint32_t prefix = kand & ~((2u << hb) - 1u);      // bits above hb: common to all keys
+    if (hb == 31) prefix = 0u;
+    for (int bit = hb; bit >= lb; bit--) {
+        const uint32_t trial = prefix | (1u << bit);
+        int c = 0;
+#pragma unroll
+        for (int q = 0; q < kMedianRegs; q++) c += (key[q] < trial) ? 1 : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((uint32_t)c <= want) prefix = trial;
+    }
+    prefix |= kand & ((1u << lb) - 1u);                 // bits below lb: common to all keys
+    return float_from_order_key(prefix);
+}
+
 // Doughnut correction of one feature by one warp (src/execute_gpu.rs:717-790).
 template <typename T>
-__device__ void doughnut_warp(const T* __restrict__ raw, int H, int W, Feature& ft, const short2* __restrict__ sig,
+__device__ __forceinline__ void doughnut_warp(const T* __restrict__ raw, int H, int W, Feature& ft, const short2* __restrict__ sig,
                               int n_sig, const short2* __restrict__ bg, int n_bg, uint32_t* hist) {
     const int lane = threadIdx.x & 31;
     const int mu = sat_f2i(roundf(ft.x));
@@ -664,7 +720,8 @@ __device__ void doughnut_warp(const T* __restrict__ raw, int H, int W, Feature& 
         }
     }
     int nbg;
-    float med = warp_upper_median<T>(raw, H, W, mu, mv, bg, n_bg, hist, &nbg);
+    const float med = (n_bg <= 32 * kMedianRegs) ? warp_upper_median_regs<T>(raw, H, W, mu, mv, bg, n_bg, &nbg)
+                                                  : warp_upper_median<T>(raw, H, W, mu, mv, bg, n_bg, hist, &nbg);
     ft.d_raw = sum;
     ft.d_bg = med;
     ft.d_corr = __fsub_rn(sum, __fmul_rn(med, (float)nsig));

@@ -305,3 +305,16 @@ def test_zero_plateau_candidates(oracle, minmass):
     if minmass == 0.0:
         assert (df["mass"] == 0).sum() > 1000
     assert_same(df, tab, ALL_TP)
+
+
+@pytest.mark.parametrize("bg_radius,gap_radius", [(9.0, None), (14.0, 2.0), (20.0, None)])
+def test_doughnut_annulus_sizes(oracle, bg_radius, gap_radius):
+    """Doughnut correction with annuli small and large enough for both median
+    paths (register-resident and histogram radix select), spots at the edges."""
+    frames, _ = video(2, 120, 136, 35, seed=int(bg_radius) + 40, margin=1.0)
+    kw = dict(minmass=300.0, bg_radius=bg_radius)
+    if gap_radius is not None:
+        kw["gap_radius"] = gap_radius
+    df = gt.batch(frames, 9, tqdm=False, **kw)
+    tab = oracle.batch(trackpy_params(9, **kw), frames.astype(np.float32))
+    assert_same(df, tab, ALL_TP)
