@@ -27,6 +27,13 @@ constexpr int kSortSmem = 4096;
 constexpr long long kSubnetBudget = 1ll << 28;
 constexpr int kLagRegs = 4;     // backward-list offsets of up to 4 lags held in registers
 constexpr int kRingSmem = 64;   // memory ring bookkeeping in shared memory up to memory = 64
+// A frame with at most kLinkSmemD detections and kLinkSmemS sources keeps its
+// per-destination and per-source working arrays in shared memory; larger
+// frames use the same arrays in the global scratch.
+constexpr int kLinkSmemD = 2048;
+constexpr int kLinkSmemS = 2560;
+constexpr size_t kLinkSmemBytes = (size_t)(kLinkSmemD + 1) * 4 * 10 + (size_t)kLinkSmemS * (8 + 8 + 4 + 1);
+static_assert(((kLinkSmemD + 1) * 4 * 10) % 8 == 0, "source block stays 8-byte aligned");
 
 // ------------------------------------------------------- point addressing
 __device__ __forceinline__ int64_t gbase(const LinkInput& in, int g) {
@@ -191,11 +198,12 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
 }
 
 // ---------------------------------------------------------- scratch layout
+// dblk: 10 per-destination int32 arrays of G + 1 entries (d_off, d_end,
+// out_src, parent, comp_nd, comp_ns, comp_off, comp_soff, roots, tmp);
+// sblk: per-source sf0, sf1 (int64), src_pt (int32), srcUsed (u8), Smax each.
 struct Lay {
-    size_t start, idstamp, firstpos, srcidx, srcstamp, src_pt, ring_pt, ring_n, ringpre, d_off, d_end, sf0, sf1,
-        e_src, e_dist,
-        out_src, parent, comp_nd, comp_ns, comp_off, comp_soff, roots, pathD, pathS, srcLocal, srcUsed, vis_d,
-        vis_s, stack, r2a, r2b, r2c, r2used, tmp, total;
+    size_t start, idstamp, firstpos, srcidx, srcstamp, ring_pt, ring_n, ringpre, dblk, sblk, e_src, e_dist, pathD,
+        pathS, srcLocal, vis_d, vis_s, stack, r2a, r2b, r2c, r2used, total;
 };
 
 __host__ __device__ inline size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -209,27 +217,16 @@ __host__ __device__ inline Lay make_lay(int64_t G, int64_t E, int64_t NP, int64_
     l.firstpos = o; o = al(o + 8 * NP);
     l.srcidx = o; o = al(o + 4 * NP);
     l.srcstamp = o; o = al(o + 4 * NP);
-    l.src_pt = o; o = al(o + 4 * Smax);
     l.ring_pt = o; o = al(o + 4 * (M * G + 1));
     l.ring_n = o; o = al(o + 4 * (M + 1));
     l.ringpre = o; o = al(o + 4 * (M + 2));
-    l.d_off = o; o = al(o + 4 * (G + 1));
-    l.d_end = o; o = al(o + 4 * (G + 1));
-    l.sf0 = o; o = al(o + 8 * Smax);
-    l.sf1 = o; o = al(o + 8 * Smax);
+    l.dblk = o; o = al(o + 4 * 10 * (G + 1));
+    l.sblk = o; o = al(o + (8 + 8 + 4 + 1) * Smax);
     l.e_src = o; o = al(o + 4 * (E + 1));
     l.e_dist = o; o = al(o + 4 * (E + 1));
-    l.out_src = o; o = al(o + 4 * G);
-    l.parent = o; o = al(o + 4 * G);
-    l.comp_nd = o; o = al(o + 4 * G);
-    l.comp_ns = o; o = al(o + 4 * G);
-    l.comp_off = o; o = al(o + 4 * G);
-    l.comp_soff = o; o = al(o + 4 * G);
-    l.roots = o; o = al(o + 4 * G);
     l.pathD = o; o = al(o + 4 * G);
     l.pathS = o; o = al(o + 4 * Smax);
     l.srcLocal = o; o = al(o + 4 * Smax);
-    l.srcUsed = o; o = al(o + Smax);
     l.vis_d = o; o = al(o + 4 * G);
     l.vis_s = o; o = al(o + 4 * Smax);
     l.stack = o; o = al(o + 8 * (G + Smax));
@@ -237,7 +234,6 @@ __host__ __device__ inline Lay make_lay(int64_t G, int64_t E, int64_t NP, int64_
     l.r2b = o; o = al(o + 4 * G);
     l.r2c = o; o = al(o + 4 * G);
     l.r2used = o; o = al(o + Smax);
-    l.tmp = o; o = al(o + 4 * (G + Smax));
     l.total = o;
     return l;
 }
@@ -297,27 +293,16 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
     unsigned long long* firstpos = (unsigned long long*)(base + lay.firstpos);
     int32_t* srcidx = (int32_t*)(base + lay.srcidx);
     int32_t* srcstamp = (int32_t*)(base + lay.srcstamp);
-    int32_t* src_pt = (int32_t*)(base + lay.src_pt);
     int32_t* ring_pt = (int32_t*)(base + lay.ring_pt);
     int32_t* ring_n = (int32_t*)(base + lay.ring_n);
     int32_t* ringpre = (int32_t*)(base + lay.ringpre);
-    int32_t* d_off = (int32_t*)(base + lay.d_off);
-    int32_t* d_end = (int32_t*)(base + lay.d_end);
-    int64_t* sf0 = (int64_t*)(base + lay.sf0);
-    int64_t* sf1 = (int64_t*)(base + lay.sf1);
+    int32_t* const g_dblk = (int32_t*)(base + lay.dblk);
+    uint8_t* const g_sblk = base + lay.sblk;
     int32_t* e_src = (int32_t*)(base + lay.e_src);
     float* e_dist = (float*)(base + lay.e_dist);
-    int32_t* out_src = (int32_t*)(base + lay.out_src);
-    volatile int* parent = (volatile int*)(base + lay.parent);
-    int32_t* comp_nd = (int32_t*)(base + lay.comp_nd);
-    int32_t* comp_ns = (int32_t*)(base + lay.comp_ns);
-    int32_t* comp_off = (int32_t*)(base + lay.comp_off);
-    int32_t* comp_soff = (int32_t*)(base + lay.comp_soff);
-    int32_t* roots = (int32_t*)(base + lay.roots);
     int32_t* pathD = (int32_t*)(base + lay.pathD);
     int32_t* pathS = (int32_t*)(base + lay.pathS);
     int32_t* srcLocal = (int32_t*)(base + lay.srcLocal);
-    uint8_t* srcUsed = base + lay.srcUsed;
     int32_t* vis_d = (int32_t*)(base + lay.vis_d);
     int32_t* vis_s = (int32_t*)(base + lay.vis_s);
     int2* stack = (int2*)(base + lay.stack);
@@ -325,13 +310,16 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
     int32_t* r2cho = (int32_t*)(base + lay.r2b);
     int32_t* r2best = (int32_t*)(base + lay.r2c);
     uint8_t* r2used = base + lay.r2used;
-    int32_t* tmp = (int32_t*)(base + lay.tmp);
     int64_t* dur = out.dur + P0;
     int64_t* ids = out.ids;
     const int Smax = G * K;
     const float R = in.radius;
     const float R2 = __fmul_rn(R, R);
     const int tid = threadIdx.x, nth = blockDim.x;
+    // shared-memory copies of the per-frame blocks (same layout as dblk / sblk)
+    extern __shared__ int64_t lsm[];
+    int32_t* const s_dblk = (int32_t*)lsm;                             // 10 x (kLinkSmemD + 1)
+    uint8_t* const s_sblk = (uint8_t*)(s_dblk + 10 * (kLinkSmemD + 1));  // kLinkSmemS sources
 
     // ring sizes and their prefix live in shared memory for memory <= kRingSmem
     const bool ring_smem = M <= kRingSmem;
@@ -385,6 +373,29 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         const int prevg = sh_prevg;
         const int S0 = (prevg == g - 1 && prevg >= gb) ? (int)gsize(in, g - 1) : 0;
         const int64_t pa = (S0 > 0) ? gbase(in, g - 1) : 0;
+        // working arrays of this frame: shared memory when they fit
+        int ring_all = 0;
+        if (ring_smem)
+            for (int q = 0; q < M; q++) ring_all += ringN[q];
+        const bool fast = ring_smem && D <= kLinkSmemD && S0 + ring_all <= kLinkSmemS;
+        const int dstr = fast ? kLinkSmemD + 1 : G + 1;
+        const int sstr = fast ? kLinkSmemS : Smax;
+        int32_t* const dblk = fast ? s_dblk : g_dblk;
+        uint8_t* const sblk = fast ? s_sblk : g_sblk;
+        int64_t* const sf0 = (int64_t*)sblk;
+        int64_t* const sf1 = sf0 + sstr;
+        int32_t* const src_pt = (int32_t*)(sf1 + sstr);
+        uint8_t* const srcUsed = (uint8_t*)(src_pt + sstr);
+        int32_t* const d_off = dblk;
+        int32_t* const d_end = dblk + dstr;
+        int32_t* const out_src = dblk + 2 * dstr;
+        volatile int* const parent = (volatile int*)(dblk + 3 * dstr);
+        int32_t* const comp_nd = dblk + 4 * dstr;
+        int32_t* const comp_ns = dblk + 5 * dstr;
+        int32_t* const comp_off = dblk + 6 * dstr;
+        int32_t* const comp_soff = dblk + 7 * dstr;
+        int32_t* const roots = dblk + 8 * dstr;
+        int32_t* const tmp = dblk + 9 * dstr;
         // ---- P1: sources = previous frame + memory entries not already present
         for (int i0 = 2 * tid; i0 < S0; i0 += 2 * nth) {
             const int n2 = min(2, S0 - i0);
@@ -943,7 +954,8 @@ cudaError_t link_run_window(const LinkInput& in, const LinkLists& L, const LinkS
                             const LinkWindow& w, cudaStream_t st) {
     if (in.nvideos == 0) return cudaSuccess;
     if (w.g0 >= 0 && (in.nvideos != 1 || !w.state)) return cudaErrorInvalidValue;
-    link_video_kernel<<<in.nvideos, kLinkThreads, 0, st>>>(in, L, S, out, w);
+    cudaFuncSetAttribute(link_video_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLinkSmemBytes);
+    link_video_kernel<<<in.nvideos, kLinkThreads, kLinkSmemBytes, st>>>(in, L, S, out, w);
     return cudaGetLastError();
 }
 
