@@ -144,6 +144,12 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def cpu_sample_frames(cores, total):
+    """Frames in the CPU sample: about 10-20 s of oracle work on the host's cores
+    (the oracle locates ~1.3 frames/s per core at 2048x2048)."""
+    return max(16, min(total, 256, 16 * cores))
+
+
 def cpu_baseline(frames_u16, p, nthreads):
     """The oracle on the host cores; returns frames/s and the sample size."""
     import numpy as np
@@ -163,7 +169,7 @@ def run_reference(args):
     import torch
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
     cores = os.cpu_count() or 1
-    n = args.cpu_sample or max(8, min(64, 2 * cores))
+    n = args.cpu_sample or cpu_sample_frames(cores, args.frames)
     vid = make_video(n, args.size, 2, dev).cpu().numpy()
     p = params()
     vals = []
@@ -248,7 +254,7 @@ def main():
     launches = ctx.launch_count() - l0
     kernels = {}
     for name in ("bandpass_localmax", "walk_characterize", "finalize", "scatter", "link_sort", "link_lists",
-                 "link_video", "link_durations", "round_ids"):
+                 "link_video", "link_rows", "link_durations", "round_ids"):
         n, kms = ctx.profile_read(name)
         if n:
             kernels[name] = (n, kms)
@@ -305,7 +311,11 @@ def main():
     # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
     total_k = sum(v[1] for v in kernels.values()) or 1.0
-    dom = max(kernels.items(), key=lambda kv: kv[1][1]) if kernels else ("bandpass_localmax", (1, 1.0))
+    # the bandpass + local-max kernel: the longest kernel on the locate stream,
+    # whose input read is the step's algorithmic traffic (the linker's kernels
+    # run on their own stream beside it)
+    dom = ("bandpass_localmax", kernels["bandpass_localmax"]) if "bandpass_localmax" in kernels else (
+        max(kernels.items(), key=lambda kv: kv[1][1]) if kernels else ("bandpass_localmax", (1, 1.0)))
     feats_per_frame = rows_all / frames_all
     bytes_per_frame = S * S * 2 + feats_per_frame * 48.0
     # frames per launch of the per-chunk kernels: the engine's chunk size
@@ -326,7 +336,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = os.cpu_count() or 1
-        n = args.cpu_sample or max(8, min(64, 2 * cores))
+        n = args.cpu_sample or cpu_sample_frames(cores, T)
         sample = video[:n].cpu().numpy()
         fps, dt, _ = cpu_baseline(sample, p, cores)
         cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
