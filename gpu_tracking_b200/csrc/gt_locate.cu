@@ -870,23 +870,38 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
         total += tot;
         __syncthreads();
     }
-    __syncthreads();
-    if (fc.doughnut) {
-        uint32_t* myhist = hist + wid * 256;
-        for (int q = wid; q < total; q += (blockDim.x >> 5)) {
-            Feature ft = out[(size_t)g * feat_cap + q];
-            int4 m = dn_meta[fc.log_style ? ft.ridx : 0];
-            doughnut_warp<T>(raw, fc.H, fc.W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);
-            if (lane == 0) {
-                Feature* o = out + (size_t)g * feat_cap + q;
-                o->d_raw = ft.d_raw;
-                o->d_bg = ft.d_bg;
-                o->d_corr = ft.d_corr;
-            }
-            __syncwarp();
-        }
-    }
     if (threadIdx.x == 0) kept_count[g] = (uint32_t)total;
+}
+
+// Doughnut correction of the kept rows (src/execute_gpu.rs:717-790): one warp
+// per row, kDoughnutBlocks x 8 warps per frame walking the frame's rows, so the
+// per-row latency (gathers, median bits) overlaps across the whole GPU.
+constexpr int kDoughnutWarps = 8;
+constexpr int kDoughnutBlocks = 16;
+template <typename T>
+__global__ void __launch_bounds__(32 * kDoughnutWarps)
+doughnut_kernel(Feature* __restrict__ out, const uint32_t* __restrict__ kept_count, uint32_t feat_cap,
+                const FinalizeConsts fc, const T* __restrict__ frames, int64_t frame_stride,
+                const int32_t* __restrict__ frame_index, const short2* __restrict__ dn_inds,
+                const int4* __restrict__ dn_meta) {
+    __shared__ uint32_t hist[kDoughnutWarps * 256];
+    const int g = blockIdx.y;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int total = (int)kept_count[g];
+    const T* raw = frames + (size_t)frame_index[g] * frame_stride;
+    uint32_t* myhist = hist + wid * 256;
+    for (int q = blockIdx.x * kDoughnutWarps + wid; q < total; q += gridDim.x * kDoughnutWarps) {
+        Feature* o = out + (size_t)g * feat_cap + q;
+        Feature ft = *o;
+        const int4 m = dn_meta[fc.log_style ? ft.ridx : 0];
+        doughnut_warp<T>(raw, fc.H, fc.W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);
+        if (lane == 0) {
+            o->d_raw = ft.d_raw;
+            o->d_bg = ft.d_bg;
+            o->d_corr = ft.d_corr;
+        }
+        __syncwarp();
+    }
 }
 
 // Per-frame rows -> table columns at the frame's row offset.
@@ -999,6 +1014,11 @@ cudaError_t launch_finalize(const Feature* feats, const uint32_t* feat_count, ui
     finalize_kernel<T><<<ngroups, kFinalizeThreads, smem, st>>>(feats, feat_count, feat_cap, out, kept_count,
                                                                 gscratch, fc, frames, frame_stride, frame_index,
                                                                 dn_inds, dn_meta, flags);
+    if (fc.doughnut && ngroups > 0) {
+        dim3 grid(kDoughnutBlocks, ngroups);
+        doughnut_kernel<T><<<grid, 32 * kDoughnutWarps, 0, st>>>(out, kept_count, feat_cap, fc, frames,
+                                                                  frame_stride, frame_index, dn_inds, dn_meta);
+    }
     return cudaGetLastError();
 }
 
