@@ -154,6 +154,7 @@ struct Row {
     // doughnut (src/execute_gpu.rs:717-790)
     float d_raw_mass = NAN, d_bg_median = NAN, d_corrected = NAN;
     int64_t particle = -1, duration = -1;
+    int64_t key = 0;  // position in the canonical (candidate) order of its frame
 };
 
 // ------------------------------------------------------------ preprocess
@@ -353,6 +354,12 @@ static inline int32_t wgsl_i32(float f) {
     if (f <= -2147483648.0f) return INT32_MIN;
     return (int32_t)f;
 }
+// WGSL u32(f32) for the in-range values that occur here (counts).
+static inline uint32_t wgsl_u32(float f) {
+    if (!(f > 0.0f)) return 0u;
+    if (f >= 4294967295.0f) return UINT32_MAX;
+    return (uint32_t)f;
+}
 
 static void characterize(const Derived& d, const float* p, const float* raw, Row& row, bool char_points) {
     const int32_t kr = d.circle;
@@ -493,11 +500,158 @@ static void logspace_max(const Derived& d, const float* bottom, const float* mid
 }
 
 // --------------------------------------------------------- per-frame locate
+// ---------------------------------------------------------------- frame std
+// StdArray::execute (src/utils.rs:614-640): sum_image_outplace.wgsl (each of
+// N/8 outputs sums 8 values N/8 apart, skipping the 0xFFFFFFFF pattern that
+// marks masked pixels), sum_image_inplace.wgsl levels (8 values L/8 apart)
+// while the length exceeds 24, last_reduction.wgsl (sequential sum / divisor);
+// std_image.wgsl ((x - mean)^2, 0 where masked), the same levels from N, then
+// sum / (divisor - 1) and sqrt.  Exact only when every level's length is a
+// multiple of 8 (std_clean); otherwise the shaders read leftovers of earlier
+// passes beyond the valid length.
+static inline uint32_t f32_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+static inline float bits_f32(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+static constexpr uint32_t kMaskedPixel = 0xFFFFFFFFu;
+
+static bool std_clean(int64_t N) {
+    if (N <= 0 || N % 8) return false;
+    for (int64_t L : {N / 8, N}) {
+        while (L > 24) {
+            if (L % 8) return false;
+            L /= 8;
+        }
+    }
+    return true;
+}
+
+static float frame_std(const float* f, int64_t N, uint32_t divisor, std::vector<float>& tmp) {
+    tmp.resize((size_t)N);
+    auto levels = [&](int64_t L) {
+        while (L > 24) {
+            const int64_t t = L / 8;
+            for (int64_t i = 0; i < t; i++) {
+                float sum = 0.0f;
+                for (int k = 0; k < 8; k++) sum += tmp[(size_t)(i + k * t)];
+                tmp[(size_t)i] = sum;
+            }
+            L = t;
+        }
+        return L;
+    };
+    const int64_t s = N / 8;
+    for (int64_t i = 0; i < s; i++) {
+        float sum = 0.0f;
+        for (int k = 0; k < 8; k++) {
+            const float v = f[i + k * s];
+            if (f32_bits(v) != kMaskedPixel) sum += v;
+        }
+        tmp[(size_t)i] = sum;
+    }
+    int64_t L = levels(s);
+    float mean = 0.0f;
+    for (int64_t i = 0; i < L; i++) mean += tmp[(size_t)i];
+    mean /= (float)divisor;
+    for (int64_t i = 0; i < N; i++) {
+        const float v = f[i];
+        if (f32_bits(v) != kMaskedPixel) {
+            const float diff = v - mean;
+            tmp[(size_t)i] = diff * diff;
+        } else {
+            tmp[(size_t)i] = 0.0f;
+        }
+    }
+    L = levels(N);
+    float var = 0.0f;
+    for (int64_t i = 0; i < L; i++) var += tmp[(size_t)i];
+    var /= (float)(divisor - 1u);
+    return std::sqrt(var);
+}
+
+// adaptive_filter.wgsl set_nan: the row's circle marked as masked.
+static void mask_circle(const Derived& d, const Row& row, float* frame) {
+    const int32_t rint = (row.r > 0.0f) ? wgsl_i32(std::ceil(row.r)) : (d.circle - 1) / 2;
+    const int32_t u = wgsl_i32(std::rint(row.x)), v = wgsl_i32(std::rint(row.y));
+    const float r = (float)rint;
+    const float r2 = r * r;
+    for (int32_t i = -rint; i <= rint; i++) {
+        const float x = (float)i;
+        const float x2 = x * x;
+        for (int32_t j = -rint; j <= rint; j++) {
+            const float y = (float)j;
+            const float y2 = y * y;
+            if (x2 + y2 > r2) continue;
+            const int32_t pu = u + i, pv = v + j;
+            if (pu < 0 || pu >= d.H || pv < 0 || pv >= d.W) continue;
+            frame[(size_t)pu * d.W + pv] = bits_f32(kMaskedPixel);
+        }
+    }
+}
+
+// The adaptive_background loop (src/execute_gpu.rs:289-366 with
+// adaptive_filter.wgsl): n_iter passes over the rows not yet accepted; a row
+// is accepted unless mass < minmass (minmass_snr * count * std when minmass
+// is not positive) or max_intensity < snr * std; an accepted row masks its
+// circle and takes its count off the divisor; before every pass but the
+// first the std is recomputed on the masked frame.  The accepted rows keep
+// their canonical order (the reference appends them with atomics).
+static void adaptive_filter(const Derived& d, uint32_t n_iter, bool recompute, const float* img, float std0,
+                            std::vector<Row>& rows, std::vector<float>& frame, std::vector<float>& tmp) {
+    const int64_t N = (int64_t)d.H * d.W;
+    frame.assign(img, img + N);
+    uint32_t counter = (uint32_t)N;
+    float sd = std0;
+    std::vector<Row> pending = rows, accepted, next;
+    for (uint32_t it = 0; it < n_iter; it++) {
+        if (it > 0 && recompute) sd = frame_std(frame.data(), N, counter, tmp);
+        next.clear();
+        for (const Row& row : pending) {
+            float minmass;
+            if (d.minmass > 0.0f) minmass = d.minmass;
+            else minmass = d.minmass_snr * row.count * sd;
+            if ((row.mass < minmass) || (row.max_intensity < d.snr * sd)) {
+                next.push_back(row);
+            } else {
+                mask_circle(d, row, frame.data());
+                counter -= wgsl_u32(row.count);
+                accepted.push_back(row);
+            }
+        }
+        pending.swap(next);
+    }
+    std::stable_sort(accepted.begin(), accepted.end(), [](const Row& a, const Row& b) { return a.key < b.key; });
+    rows.swap(accepted);
+}
+
 struct FrameScratch {
-    std::vector<float> tg, tb, processed, mr, temp;
+    std::vector<float> tg, tb, processed, mr, temp, masked, stdtmp;
     std::vector<std::vector<float>> planes;
     std::vector<std::pair<int32_t, int32_t>> cands;
 };
+
+// snr / minmass_snr / adaptive_background combinations this restatement
+// reproduces (the library accepts the same ones):
+//  * the frame std needs a pixel count whose reduction levels are all
+//    multiples of 8 (std_clean);
+//  * adaptive_background = 0 and adaptive_background >= 2 without snr or
+//    minmass_snr make the reference panic (an empty pass iterator, a missing
+//    std pass: src/execute_gpu.rs:297-310).
+static int check_std_params(const gt_params& p, int64_t N) {
+    const bool std_pass = p.has_snr || p.has_minmass_snr;
+    if (std_pass && !std_clean(N)) return GT_ERR_INVALID_ARGUMENT;
+    if (p.has_adaptive_background) {
+        if (p.adaptive_background == 0) return GT_ERR_INVALID_ARGUMENT;
+        if (p.adaptive_background >= 2 && !std_pass) return GT_ERR_INVALID_ARGUMENT;
+    }
+    return GT_OK;
+}
 
 // One frame through the shader passes in the reference's order
 // (src/gpu_setup.rs:872-895 and src/execute_gpu.rs:231-286, 368-375).
@@ -506,13 +660,15 @@ static void locate_frame(const gt_params& p, const Derived& d, const std::vector
     const size_t n = (size_t)d.H * d.W;
     s.processed.resize(n);
     preprocess(d, p.truncate_preprocessed != 0, img, s.tg, s.tb, s.processed.data());
-    const float pic_std = 0.0f;  // std buffer is only written when snr/minmass_snr is set
+    // the std buffer is written only when snr or minmass_snr is set (src/gpu_setup.rs:990)
+    const bool std_pass = p.has_snr || p.has_minmass_snr;
+    const float pic_std = std_pass ? frame_std(img, (int64_t)n, (uint32_t)n, s.stdtmp) : 0.0f;
     rows.clear();
     if (p.style == GT_STYLE_TRACKPY) {
         extract_max(d, s.processed.data(), pic_std, s.mr, s.cands);
         for (auto& c : s.cands) {
             Row row;
-            if (walk_keep(d, s.processed.data(), c.first, c.second, -1.0f, pic_std, row)) rows.push_back(row);
+            if (walk_keep(d, s.processed.data(), c.first, c.second, -1.0f, pic_std, row)) { row.key = (int64_t)rows.size(); rows.push_back(row); }
         }
     } else {
         const size_t nr = radii.size();
@@ -530,7 +686,7 @@ static void locate_frame(const gt_params& p, const Derived& d, const std::vector
             for (auto& c : s.cands) {
                 Row row;
                 if (walk_keep(d, s.processed.data(), c.first, c.second, radii[i - 1], pic_std, row))
-                    rows.push_back(row);
+                    { row.key = (int64_t)rows.size(); rows.push_back(row); }
             }
             edge = 0;
         }
@@ -541,9 +697,12 @@ static void locate_frame(const gt_params& p, const Derived& d, const std::vector
         logspace_max(d, bottom, s.planes[mid].data(), top, s.processed.data(), pic_std, edge, s.cands);
         for (auto& c : s.cands) {
             Row row;
-            if (walk_keep(d, s.processed.data(), c.first, c.second, radii[nr - 1], pic_std, row)) rows.push_back(row);
+            if (walk_keep(d, s.processed.data(), c.first, c.second, radii[nr - 1], pic_std, row)) { row.key = (int64_t)rows.size(); rows.push_back(row); }
         }
     }
+    if (p.has_adaptive_background)
+        adaptive_filter(d, p.adaptive_background, std_pass, img, pic_std, rows, s.masked, s.stdtmp);
+    // characterize reads the unmasked frame (raw_frame, src/gpu_setup.rs:194-205)
     if (p.characterize) {
         for (auto& row : rows) characterize(d, s.processed.data(), img, row, false);
     }
@@ -1053,6 +1212,40 @@ int oracle_preprocess(const gt_params* p, const float* frame, int32_t H, int32_t
     return GT_OK;
 }
 
+// Frame std as the reference computes it (StdArray::execute); frame may
+// hold the 0xFFFFFFFF masked-pixel pattern.  Returns an error for pixel
+// counts whose reduction is not exact (see std_clean).
+int oracle_frame_std(const float* frame, int64_t N, uint32_t divisor, float* out) {
+    if (!std_clean(N)) return GT_ERR_INVALID_ARGUMENT;
+    std::vector<float> tmp;
+    *out = frame_std(frame, N, divisor, tmp);
+    return GT_OK;
+}
+
+// The adaptive_background passes over walked rows (10 floats each, ResultRow
+// order); rows_out gets the accepted rows in canonical (input) order.
+int64_t oracle_adaptive(const gt_params* p, const float* frame, int32_t H, int32_t W, const float* rows_in, int64_t n,
+                        uint32_t n_iter, float std0, int32_t recompute, float* rows_out) {
+    Derived d = derive(*p, H, W);
+    std::vector<Row> rows((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        const float* r = rows_in + 10 * i;
+        Row& w = rows[(size_t)i];
+        w.x = r[0]; w.y = r[1]; w.mass = r[2]; w.r = r[3]; w.max_intensity = r[4];
+        w.Rg = r[5]; w.raw_mass = r[6]; w.signal = r[7]; w.ecc = r[8]; w.count = r[9];
+        w.key = i;
+    }
+    std::vector<float> masked, tmp;
+    adaptive_filter(d, n_iter, recompute != 0, frame, std0, rows, masked, tmp);
+    for (size_t i = 0; i < rows.size(); i++) {
+        const Row& w = rows[i];
+        float* r = rows_out + 10 * i;
+        r[0] = w.x; r[1] = w.y; r[2] = w.mass; r[3] = w.r; r[4] = w.max_intensity;
+        r[5] = w.Rg; r[6] = w.raw_mass; r[7] = w.signal; r[8] = w.ecc; r[9] = w.count;
+    }
+    return (int64_t)rows.size();
+}
+
 int64_t oracle_candidates(const gt_params* p, const float* processed, int32_t H, int32_t W, float pic_std,
                           int32_t* uv_out, int64_t cap) {
     Derived d = derive(*p, H, W);
@@ -1069,11 +1262,11 @@ int64_t oracle_candidates(const gt_params* p, const float* processed, int32_t H,
 // Walk + (optional) characterize for the given candidates on a processed
 // frame; writes one 10-float ResultRow per candidate and keep flags.
 int oracle_walk(const gt_params* p, const float* processed, const float* raw, int32_t H, int32_t W,
-                const int32_t* uv, int64_t n, float r, float* rows_out, int32_t* keep_out) {
+                const int32_t* uv, int64_t n, float r, float pic_std, float* rows_out, int32_t* keep_out) {
     Derived d = derive(*p, H, W);
     for (int64_t i = 0; i < n; i++) {
         Row row;
-        bool k = walk_keep(d, processed, uv[2 * i], uv[2 * i + 1], r, 0.0f, row);
+        bool k = walk_keep(d, processed, uv[2 * i], uv[2 * i + 1], r, pic_std, row);
         if (!k) {
             WalkResult w = walk(d, processed, uv[2 * i], uv[2 * i + 1], r);
             row.x = w.x; row.y = w.y; row.mass = w.mass; row.count = w.count; row.max_intensity = w.max;
@@ -1103,6 +1296,10 @@ int oracle_batch(const gt_params* p, const float* frames, int64_t T, int32_t H, 
                  const int64_t* frame_numbers, const int64_t* reset, int64_t n_reset, int32_t nthreads,
                  void** out_table) {
     if (T <= 0) return GT_ERR_EMPTY_ITERATOR;
+    {
+        const int st = check_std_params(*p, (int64_t)H * W);
+        if (st != GT_OK) return st;
+    }
     Derived d = derive(*p, H, W);
     auto radii = log_radii(*p);
     std::vector<std::vector<Row>> per_frame((size_t)T);

@@ -49,7 +49,11 @@ def lib():
                                         ctypes.c_int64]
         L.oracle_candidates.restype = ctypes.c_int64
         L.oracle_walk.argtypes = [vp, c_f32p, c_f32p, ctypes.c_int32, ctypes.c_int32, c_i32p, ctypes.c_int64,
-                                  ctypes.c_float, c_f32p, c_i32p]
+                                  ctypes.c_float, ctypes.c_float, c_f32p, c_i32p]
+        L.oracle_frame_std.argtypes = [c_f32p, ctypes.c_int64, ctypes.c_uint32, c_f32p]
+        L.oracle_adaptive.argtypes = [vp, c_f32p, ctypes.c_int32, ctypes.c_int32, c_f32p, ctypes.c_int64,
+                                      ctypes.c_uint32, ctypes.c_float, ctypes.c_int32, c_f32p]
+        L.oracle_adaptive.restype = ctypes.c_int64
         L.oracle_log_planes.argtypes = [vp, c_f32p, ctypes.c_int32, ctypes.c_int32, c_f32p, c_f32p]
         L.oracle_batch.argtypes = [vp, c_f32p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
                                    ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(vp)]
@@ -87,6 +91,11 @@ def ref():
         L.ref_logspace_max.argtypes = [vp, c_f32p, c_f32p, c_f32p, c_f32p, ctypes.c_float, ctypes.c_int32,
                                        ctypes.c_float, c_i32p, ctypes.c_int64]
         L.ref_logspace_max.restype = ctypes.c_int64
+        L.ref_frame_std.argtypes = [c_f32p, ctypes.c_int64, ctypes.c_uint32, c_f32p]
+        L.ref_frame_std.restype = ctypes.c_float
+        L.ref_adaptive.argtypes = [vp, c_f32p, c_f32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_float, ctypes.c_int32,
+                                   c_f32p, c_f32p]
+        L.ref_adaptive.restype = ctypes.c_int64
         _REF = L
     return _REF
 
@@ -136,7 +145,7 @@ def candidates(p, processed, pic_std=0.0):
     return uv[:n].copy()
 
 
-def walk(p, processed, raw, uv, r=-1.0):
+def walk(p, processed, raw, uv, r=-1.0, pic_std=0.0):
     processed, raw = _f32(processed), _f32(raw)
     H, W = processed.shape
     uv = np.ascontiguousarray(uv, np.int32)
@@ -144,8 +153,27 @@ def walk(p, processed, raw, uv, r=-1.0):
     rows = np.zeros((max(n, 1), 10), np.float32)
     keep = np.zeros(max(n, 1), np.int32)
     _check(lib().oracle_walk(ctypes.byref(p), _ptr(processed, c_f32p), _ptr(raw, c_f32p), H, W,
-                             _ptr(uv, c_i32p), n, r, _ptr(rows, c_f32p), _ptr(keep, c_i32p)))
+                             _ptr(uv, c_i32p), n, r, pic_std, _ptr(rows, c_f32p), _ptr(keep, c_i32p)))
     return rows[:n], keep[:n].astype(bool)
+
+
+def frame_std(frame, divisor=None):
+    """The reference's frame std (StdArray); masked pixels hold the 0xFFFFFFFF pattern."""
+    frame = _f32(frame).ravel()
+    out = ctypes.c_float()
+    _check(lib().oracle_frame_std(_ptr(frame, c_f32p), frame.size, frame.size if divisor is None else divisor,
+                                  ctypes.byref(out)))
+    return np.float32(out.value)
+
+
+def adaptive(p, frame, rows, n_iter, std0, recompute=True):
+    frame = _f32(frame)
+    H, W = frame.shape
+    rows = _f32(rows).reshape(-1, 10)
+    out = np.zeros((max(len(rows), 1), 10), np.float32)
+    n = lib().oracle_adaptive(ctypes.byref(p), _ptr(frame, c_f32p), H, W, _ptr(rows, c_f32p), len(rows), n_iter,
+                              std0, int(recompute), _ptr(out, c_f32p))
+    return out[:n].copy()
 
 
 def log_planes(p, frame):
@@ -225,14 +253,34 @@ def ref_candidates(p, processed, pic_std=0.0):
     return uv[:n].copy()
 
 
-def ref_walk(p, processed, raw, uv, r=-1.0, characterize=True):
+def ref_walk(p, processed, raw, uv, r=-1.0, characterize=True, pic_std=0.0):
     processed, raw = _f32(processed), _f32(raw)
     H, W = processed.shape
     uv = np.ascontiguousarray(uv, np.int32)
     rows = np.zeros((max(len(uv), 1), 10), np.float32)
     n = ref().ref_walk(gpu_params(p, H, W), _ptr(processed, c_f32p), _ptr(raw, c_f32p), _ptr(uv, c_i32p),
-                       len(uv), r, 0.0, int(characterize), _ptr(rows, c_f32p))
+                       len(uv), r, pic_std, int(characterize), _ptr(rows, c_f32p))
     return rows[:n].copy()
+
+
+def ref_frame_std(frame, divisor=None, temp=None):
+    """StdArray::execute with the reference's shaders; temp (2N floats) persists like its buffer."""
+    frame = _f32(frame).ravel()
+    if temp is None:
+        temp = np.zeros(2 * frame.size, np.float32)
+    return np.float32(ref().ref_frame_std(_ptr(frame, c_f32p), frame.size,
+                                          frame.size if divisor is None else divisor, _ptr(temp, c_f32p)))
+
+
+def ref_adaptive(p, frame, rows, n_iter, std0, recompute=True):
+    frame = _f32(frame).copy()
+    H, W = frame.shape
+    rows = _f32(rows).reshape(-1, 10)
+    temp = np.zeros(2 * H * W, np.float32)
+    out = np.zeros((max(len(rows), 1), 10), np.float32)
+    n = ref().ref_adaptive(gpu_params(p, H, W), _ptr(frame, c_f32p), _ptr(rows, c_f32p), len(rows), n_iter, std0,
+                           int(recompute), _ptr(temp, c_f32p), _ptr(out, c_f32p))
+    return out[:n].copy()
 
 
 def ref_characterize_points(p, processed, raw, yxr):

@@ -89,6 +89,21 @@ inline uint32_t wgsl_atomicAdd(uint32_t* p, uint32_t v) {
     *p += v;
     return o;
 }
+inline uint32_t wgsl_atomicSub(uint32_t* p, uint32_t v) {
+    uint32_t o = *p;
+    *p -= v;
+    return o;
+}
+inline uint32_t wgsl_bitcast_u32(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    return u;
+}
+inline float wgsl_bitcast_f32(uint32_t u) {
+    float x;
+    std::memcpy(&x, &u, 4);
+    return x;
+}
 
 #include "_ref/gen_preprocess_rows.inc"
 #include "_ref/gen_preprocess_cols_trunc.inc"
@@ -100,6 +115,11 @@ inline uint32_t wgsl_atomicAdd(uint32_t* p, uint32_t v) {
 #include "_ref/gen_characterize_points.inc"
 #include "_ref/gen_separable_log.inc"
 #include "_ref/gen_logspace_max.inc"
+#include "_ref/gen_sum_image_outplace.inc"
+#include "_ref/gen_sum_image_inplace.inc"
+#include "_ref/gen_last_reduction.inc"
+#include "_ref/gen_std_image.inc"
+#include "_ref/gen_adaptive_filter.inc"
 
 // Flat copy of the WGSL Params uniform (params.wgsl:1-20).
 struct RefParams {
@@ -266,6 +286,88 @@ int64_t ref_logspace_max(const RefParams* p, const float* bottom, const float* m
         uv[2 * i + 1] = pts[i].y;
     }
     return n;
+}
+
+
+// StdArray::execute (src/utils.rs:614-640): MeanArrayOutplace over the frame,
+// std_image, MeanArray with the square root.  `temp` is the reference's shared
+// temp buffer (2N floats); it keeps its contents between calls like the
+// reference's does.  Returns the value left in std_buffer.
+float ref_frame_std(const float* frame, int64_t N, uint32_t divisor, float* temp) {
+    auto meanarray = [&](uint32_t size, uint32_t sqrt_mean) -> float {
+        // MeanArray::execute (src/utils.rs:417-440)
+        uint32_t to_start = size;
+        while (to_start > 24) {
+            to_start += 7;
+            to_start /= 8;
+            sh_sum_image_inplace::pc.stride = to_start;
+            bind(sh_sum_image_inplace::arr, temp, 2 * N);
+            for (uint32_t x = 0; x < to_start; x++) sh_sum_image_inplace::main_(uvec3{x, 0u, 0u});
+        }
+        sh_last_reduction::pc.n_elements = to_start;
+        sh_last_reduction::pc.doing_variance = sqrt_mean;
+        bind(sh_last_reduction::input, temp, 2 * N);
+        sh_last_reduction::mean_divisor = divisor;
+        sh_last_reduction::main_(uvec3{0u, 0u, 0u});
+        return sh_last_reduction::output;
+    };
+    // MeanArrayOutplace::execute (src/utils.rs:514-531)
+    const uint32_t s = (uint32_t)((N + 7) / 8);
+    sh_sum_image_outplace::pc.stride = s;
+    bind(sh_sum_image_outplace::input, const_cast<float*>(frame), N);
+    bind(sh_sum_image_outplace::output, temp, 2 * N);
+    for (uint32_t x = 0; x < s; x++) sh_sum_image_outplace::main_(uvec3{x, 0u, 0u});
+    const float mean = meanarray(s, 0u);
+    // std_pass over the frame, then MeanArray(size N, sqrt)
+    sh_std_image::pc.total_elements = (uint32_t)N;
+    bind(sh_std_image::input, const_cast<float*>(frame), N);
+    bind(sh_std_image::output, temp, 2 * N);
+    sh_std_image::mean = mean;
+    for (uint32_t x = 0; x < (uint32_t)N; x++) sh_std_image::main_(uvec3{x, 0u, 0u});
+    return meanarray((uint32_t)N, 1u);
+}
+
+// The adaptive_background loop of submit_work (src/execute_gpu.rs:289-366):
+// n_iter passes of adaptive_filter.wgsl ping-ponging between the two particle
+// buffers, the frame std recomputed (on the masked frame, divided by the
+// decremented counter) before every pass but the first.  rows_in: walked
+// ResultRows (10 floats); rows_out receives the accepted rows in the order
+// the serial dispatch accepts them.  `frame` is masked in place.
+int64_t ref_adaptive(const RefParams* p, float* frame, const float* rows_in, int64_t n_in, uint32_t n_iter,
+                     float std0, int32_t recompute_std, float* temp, float* rows_out) {
+    const int64_t N = (int64_t)p->pic_nrows * p->pic_ncols;
+    using Row = sh_adaptive_filter::ResultRow;
+    std::vector<Row> a((size_t)n_in + 1), b((size_t)n_in + 1), res((size_t)n_in + 1);
+    std::memcpy(a.data(), rows_in, (size_t)n_in * sizeof(Row));
+    uint32_t count_a = (uint32_t)n_in, count_b = 0;
+    uint32_t result_n = 0;
+    uint32_t counter = (uint32_t)N;
+    float std_buffer = std0;
+    set_params(sh_adaptive_filter::params, p);
+    bind(sh_adaptive_filter::frame, frame, N);
+    for (uint32_t it = 0; it < n_iter; it++) {
+        const bool even = (it % 2) == 0;
+        if (it > 0 && recompute_std) std_buffer = ref_frame_std(frame, N, counter, temp);
+        uint32_t& cur = even ? count_a : count_b;
+        uint32_t& nxt = even ? count_b : count_a;
+        nxt = 0;
+        bind(sh_adaptive_filter::input, even ? a.data() : b.data(), n_in + 1);
+        bind(sh_adaptive_filter::output, even ? b.data() : a.data(), n_in + 1);
+        bind(sh_adaptive_filter::results, res.data(), n_in + 1);
+        sh_adaptive_filter::image_std = std_buffer;
+        sh_adaptive_filter::current_n = cur;
+        sh_adaptive_filter::new_n = 0;
+        sh_adaptive_filter::result_n = result_n;
+        sh_adaptive_filter::counter = counter;
+        sh_adaptive_filter::dispatcher = {};
+        sh_adaptive_filter::dispatcher_results = {};
+        for (uint32_t x = 0; x < cur; x++) sh_adaptive_filter::main_(uvec3{x, 0u, 0u});
+        nxt = sh_adaptive_filter::new_n;
+        result_n = sh_adaptive_filter::result_n;
+        counter = sh_adaptive_filter::counter;
+    }
+    std::memcpy(rows_out, res.data(), (size_t)result_n * sizeof(Row));
+    return result_n;
 }
 
 }  // extern "C"

@@ -41,6 +41,12 @@ SHADERS = {
     "characterize": "src/shaders/characterize.wgsl",
     "separable_log": "src/shaders/log_style/separable_log.wgsl",
     "logspace_max": "src/shaders/log_style/logspace_max.wgsl",
+    # frame std (StdArray, src/utils.rs:297-640) and the adaptive background filter
+    "sum_image_outplace": "src/shaders/sum_image_outplace.wgsl",
+    "sum_image_inplace": "src/shaders/sum_image_inplace.wgsl",
+    "last_reduction": "src/shaders/last_reduction.wgsl",
+    "std_image": "src/shaders/std_image.wgsl",
+    "adaptive_filter": "src/shaders/adaptive_filter.wgsl",
 }
 
 TYPE_MAP = {
@@ -113,6 +119,8 @@ def has_top_level(expr, ops):
 
 def translate_expr(e):
     e = fix_literals(e)
+    e = re.sub(r"\bbitcast<u32>\s*\(", "wgsl_bitcast_u32(", e)
+    e = re.sub(r"\bbitcast<f32>\s*\(", "wgsl_bitcast_f32(", e)
     e = re.sub(r"\bvec2<i32>\s*\(", "ivec2(", e)
     e = re.sub(r"\bvec2<f32>\s*\(", "vec2f(", e)
     e = re.sub(r"\bvec2\s*\(", "vec2f(", e)
@@ -121,6 +129,7 @@ def translate_expr(e):
     for b in ("exp", "sqrt", "atan2", "sin", "cos", "ceil", "round", "max", "min", "abs", "floor"):
         e = re.sub(r"(?<![\w.])%s\s*\(" % b, "wgsl_%s(" % b, e)
     e = re.sub(r"\batomicAdd\s*\(", "wgsl_atomicAdd(", e)
+    e = re.sub(r"\batomicSub\s*\(", "wgsl_atomicSub(", e)
     return e
 
 
