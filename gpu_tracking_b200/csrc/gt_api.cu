@@ -142,6 +142,7 @@ struct gt_ctx {
     DBuf l_srt, l_sortscr, l_fcnt, l_bcnt, l_foff, l_boff, l_fpts, l_bpts, l_bdist, l_scan, l_scratch, l_ids, l_cnt,
         l_dur, l_flags, l_goff, l_pgroup, l_vgrp, l_reset, l_vpoff, l_px, l_py, l_ge, l_rowdur, l_part;
     // windowed linking inside gt_batch (slot mode)
+    DBuf fstd, std_scratch, amask, astatus, acount;   // snr / minmass_snr / adaptive_background
     DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
         w_cnt, w_flags, w_vgrp, w_reset;
     int64_t w_list_cap = 0;   // entries of each window neighbour-list buffer (0 = not sized yet)
@@ -323,6 +324,8 @@ gt_status make_locate_consts(gt_ctx* ctx, const gt_params& p, int32_t H, int32_t
     c.minmass_snr = p.has_minmass_snr ? p.minmass_snr : 0.0f;
     c.image_std = 0.0f;
     c.rough = p.has_adaptive_background ? 0.5f : 1.0f;
+    c.snr = p.has_snr ? p.snr : 0.0f;
+    c.frame_std = nullptr;  // set per call when the std pass runs
     c.characterize = p.characterize ? 1 : 0;
     {
         const int rint = std::max(0, (c.circle - 1) / 2);
@@ -843,8 +846,9 @@ int pick_chunk(int64_t T, int32_t H, int32_t W, int n_planes) {
 
 template <typename T>
 gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
-                      int32_t W, const LocateConsts& c, const LogTables* lt, int F, uint32_t* out_flags,
+                      int32_t W, const LocateConsts& c_in, const LogTables* lt, int F, uint32_t* out_flags,
                       PipeLink* pl, const std::vector<uint8_t>* reset) {
+    LocateConsts c = c_in;
     const size_t npx = (size_t)H * W;
     const bool log_style = (p.style == GT_STYLE_LOG);
     const int nslots = log_style ? (int)lt->radii.size() : 1;
@@ -933,11 +937,30 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
             fc.radius_rank_desc[k] = (uint8_t)rank;
         }
     }
+    // snr / minmass_snr: the per-frame std of each chunk, computed before its
+    // bandpass (src/execute_gpu.rs:183-186); adaptive_background: its passes
+    // after the walk (src/execute_gpu.rs:289-366)
+    const bool std_pass = p.has_snr || p.has_minmass_snr;
+    const bool adaptive = p.has_adaptive_background;
+    if (std_pass || adaptive) {
+        CK(ctx->fstd.ensure((size_t)F * 4));
+        CK(cudaMemsetAsync(ctx->fstd.p, 0, (size_t)F * 4, ctx->st));  // no std pass: the reference's buffer stays 0
+        c.frame_std = ctx->fstd.as<float>();
+    }
+    if (std_pass) CK(ctx->std_scratch.ensure(std_scratch_floats((int64_t)npx, F) * 4));
+    if (adaptive) {
+        CK(ctx->amask.ensure((size_t)F * npx));
+        CK(ctx->astatus.ensure((size_t)F * feat_cap));
+        CK(ctx->acount.ensure((size_t)F * 4));
+    }
     LogConsts lc;
     lc.H = H;
     lc.W = W;
     lc.n_radii = nslots;
     lc.thr = 0.0f;
+    lc.frame_std = c.frame_std;
+    lc.snr = c.snr;
+    lc.rough = c.rough;
 
     const size_t super_bytes = (size_t)SC * npx * sizeof(T);
     if (!on_device) {
@@ -983,6 +1006,11 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         for (int64_t c0f = 0; c0f < ns; c0f += F) {
             const int nf = (int)std::min<int64_t>(F, ns - c0f);
             const T* src = sbase + c0f * npx;
+            if (std_pass) {
+                Prof pf(ctx, "frame_std");
+                CK(launch_frame_std<T>(src, (int64_t)npx, nf, (int64_t)npx, nullptr, nullptr, ctx->fstd.as<float>(),
+                                       ctx->std_scratch.as<float>(), ctx->st));
+            }
             CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
             if (!log_style) {
                 Prof pf(ctx, "bandpass_localmax");
@@ -1013,6 +1041,26 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                                   log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
                                   ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap,
                                   ctx->feat_count.as<uint32_t>() + c0f, feat_cap, flags, ctx->st));
+            }
+            if (adaptive) {
+                // adaptive_filter passes over the chunk's walked rows; the
+                // masked frame's std is recomputed before every pass but the first
+                Prof pf(ctx, "adaptive");
+                Feature* fr = ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap;
+                uint32_t* fcn = ctx->feat_count.as<uint32_t>() + c0f;
+                uint8_t* status = ctx->astatus.as<uint8_t>();
+                uint32_t* counters = ctx->acount.as<uint32_t>();
+                uint8_t* mask = ctx->amask.as<uint8_t>();
+                CK(launch_adaptive_init(counters, (uint32_t)npx, status, (size_t)nf * feat_cap, nf, ctx->st));
+                CK(cudaMemsetAsync(mask, 0, (size_t)nf * npx, ctx->st));
+                for (uint32_t it = 0; it < p.adaptive_background; it++) {
+                    if (it > 0)
+                        CK(launch_frame_std<T>(src, (int64_t)npx, nf, (int64_t)npx, mask, counters,
+                                               ctx->fstd.as<float>(), ctx->std_scratch.as<float>(), ctx->st));
+                    CK(launch_adaptive_pass(fr, fcn, feat_cap, status, ctx->fstd.as<float>(), c.minmass,
+                                            c.minmass_snr, c.snr, mask, counters, H, W, c.circle, nf, ctx->st));
+                }
+                CK(launch_adaptive_compact(fr, fcn, feat_cap, status, nf, ctx->st));
             }
         }
         {
@@ -1094,6 +1142,23 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
     }
     if (bandpass_smem_bytes(c.R, 1, false) > 227 * 1024)
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size too large for the tile kernel");
+    {
+        // the reference computes the frame std (snr / minmass_snr) as a tree of
+        // 8-way sums; where a level's length is not a multiple of 8 its shaders
+        // read what earlier passes left in a shared buffer, so only pixel counts
+        // whose levels all divide by 8 have a reproducible result
+        const bool std_pass = p.has_snr || p.has_minmass_snr;
+        if (std_pass && !std_reduction_exact((int64_t)H * W))
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                           "snr / minmass_snr need a frame of N = H*W pixels with N = 8^k * m, m <= 24 (e.g. "
+                           "512x512, 1024x1024, 2048x2048): got %dx%d",
+                           H, W);
+        if (p.has_adaptive_background && p.adaptive_background == 0)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "adaptive_background must be at least 1");
+        if (p.has_adaptive_background && p.adaptive_background >= 2 && !std_pass)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                           "adaptive_background >= 2 needs snr or minmass_snr (the image std between passes)");
+    }
     const int F = pick_chunk(NT, H, W, log_style ? (int)lt.radii.size() : 0);
     ctx->total = NT;
     ctx->done = 0;
@@ -1220,10 +1285,8 @@ gt_status validate(gt_ctx* ctx, const gt_params* p, const void* frames, int32_t 
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype);
     if (p->style != GT_STYLE_TRACKPY && p->style != GT_STYLE_LOG)
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unknown style %d", p->style);
-    if (p->has_snr || p->has_minmass_snr || p->has_adaptive_background || p->has_illumination_sigma)
-        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
-                       "snr / minmass_snr / adaptive_background / illumination correction are not supported by "
-                       "this build");
+    if (p->has_illumination_sigma)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "illumination correction is not supported by this build");
     if (p->style == GT_STYLE_TRACKPY && p->diameter == 0)
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "diameter must be positive");
     CK(cudaSetDevice(ctx->device));

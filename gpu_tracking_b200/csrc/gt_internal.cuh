@@ -70,6 +70,11 @@ struct LocateConsts {
     // walk ends where it started with mass 0 (0/0 centroid moves nothing),
     // and minmass > 0 rejects it (walk_keep, walk.wgsl).
     int32_t skip_zero;
+    // snr / minmass_snr: per-frame std of the current chunk (nullptr when the
+    // reference computes none); the candidate threshold is std * snr * rough
+    // and the walk's minmass minmass_snr * count * std * rough
+    const float* frame_std;
+    float snr;
     float taps[kMaxTaps];
 };
 

@@ -35,8 +35,26 @@ struct TableCols {
 // start at tap_off[k] and have 2*rint[k]+1 entries.
 struct LogConsts {
     int32_t H, W, n_radii;
-    float thr;  // pic_std * snr * rough_snr_factor
+    float thr;  // pic_std * snr * rough_snr_factor when no per-frame std is given
+    const float* frame_std;  // per-frame std of the chunk (nullptr: use thr)
+    float snr, rough;
 };
+
+// Per-frame std (snr / minmass_snr), the reference's reduction tree.
+bool std_reduction_exact(int64_t N);
+size_t std_scratch_floats(int64_t N, int nframes);
+template <typename T>
+cudaError_t launch_frame_std(const T* frames, int64_t frame_stride, int nframes, int64_t N, const uint8_t* mask,
+                             const uint32_t* divisors, float* out_std, float* scratch, cudaStream_t st);
+// adaptive_background passes over the walked rows of a chunk
+cudaError_t launch_adaptive_init(uint32_t* counters, uint32_t N, uint8_t* status, size_t n_status, int nframes,
+                                 cudaStream_t st);
+cudaError_t launch_adaptive_pass(const Feature* feats, const uint32_t* count, uint32_t feat_cap, uint8_t* status,
+                                 const float* frame_std, float minmass, float minmass_snr, float snr, uint8_t* mask,
+                                 uint32_t* counters, int32_t H, int32_t W, int32_t circle, int nframes,
+                                 cudaStream_t st);
+cudaError_t launch_adaptive_compact(Feature* feats, uint32_t* count, uint32_t feat_cap, const uint8_t* status,
+                                    int nframes, cudaStream_t st);
 
 size_t bandpass_smem_bytes(int R, int kd, bool cand);
 size_t finalize_smem_bytes();

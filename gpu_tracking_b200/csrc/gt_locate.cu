@@ -114,6 +114,8 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
     __syncthreads();
 
     constexpr int PER = (TH * TW) / kLocateThreads;  // 8 consecutive pixels per thread
+    // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
+    const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
     uint32_t mask = 0;
     int cnt = 0;
 #pragma unroll
@@ -124,7 +126,7 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
         if (gr >= H || gc >= W) continue;
         if (gr < c.margin || gr >= H - c.margin || gc < c.margin || gc >= W - c.margin) continue;
         float center = sp[(r + o) * PW + cc + o];
-        if (center < c.thr) continue;
+        if (center < thr) continue;
         if (c.skip_zero && center == 0.0f) continue;
         float m = -INFINITY;
         for (int j = 0; j < kd; j++) m = fmaxf(m, sv[r * PW + cc + j]);
@@ -328,7 +330,8 @@ walk_kernel(const float* __restrict__ processed, const T* __restrict__ frames, i
     WalkRes res = walk_one(p, c, u, v, r);
     float minmass;
     if (c.minmass > 0.0f) minmass = c.minmass;
-    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.image_std), c.rough);
+    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.frame_std ? c.frame_std[f] : c.image_std),
+                             c.rough);
     if (!(res.mass >= minmass)) return;
     Feature ft;
     ft.key_hi = (uint32_t)slot;
@@ -459,7 +462,8 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
     const WalkRes res = walk_fixed<RI>(p, c, u, v);
     float minmass;
     if (c.minmass > 0.0f) minmass = c.minmass;
-    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.image_std), c.rough);
+    else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.frame_std ? c.frame_std[f] : c.image_std),
+                             c.rough);
     if (!(res.mass >= minmass)) return;
     Feature ft;
     ft.key_hi = 0;

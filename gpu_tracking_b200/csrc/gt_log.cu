@@ -113,7 +113,9 @@ logspace_max_kernel(const float* __restrict__ planes, const float* __restrict__ 
     if (pix < npx) {
         int i = pix / W, j = pix - i * W;
         float center = __ldg(mid + pix);
-        if (!(__ldg(proc + pix) < lc.thr) && !(center <= 0.0f) && max_in_plane(mid, H, W, i, j, center)) {
+        // logspace_max.wgsl:122: std_pic * snr * rough_snr_factor
+        const float thr = lc.frame_std ? __fmul_rn(__fmul_rn(lc.frame_std[f], lc.snr), lc.rough) : lc.thr;
+        if (!(__ldg(proc + pix) < thr) && !(center <= 0.0f) && max_in_plane(mid, H, W, i, j, center)) {
             bool ok = true;
             if (k > 0) ok = max_in_plane(mid - npx, H, W, i, j, center);
             if (ok && k < n - 1) ok = max_in_plane(mid + npx, H, W, i, j, center);

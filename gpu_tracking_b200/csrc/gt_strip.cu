@@ -178,6 +178,8 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     };
     load_raw(0);
     const float trunc_thr = 1.0f / 255.0f;
+    // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
+    const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
     uint32_t* cout = cand_keys + (size_t)f * cand_cap;
 
     for (int s = 0; s < nsteps; s++) {
@@ -394,7 +396,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                         if (gc >= W) continue;
                         if (!rows_ok || gc < c.margin || gc >= W - c.margin) continue;
                         const float center = cen[k];
-                        if (center < c.thr) continue;
+                        if (center < thr) continue;
                         if (c.skip_zero && center == 0.0f) continue;
                         if (m[k] > center) continue;
                         cmask |= 1u << k;
