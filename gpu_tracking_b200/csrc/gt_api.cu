@@ -143,6 +143,8 @@ struct gt_ctx {
         l_dur, l_flags, l_goff, l_pgroup, l_vgrp, l_reset, l_vpoff, l_px, l_py, l_ge, l_rowdur, l_part;
     // windowed linking inside gt_batch (slot mode)
     DBuf fstd, std_scratch, amask, astatus, acount;   // snr / minmass_snr / adaptive_background
+    DBuf illum_taps, illum_shared, illum_prof, illum_corr;  // illumination correction
+    int32_t illum_rint = 0;
     DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
         w_cnt, w_flags, w_vgrp, w_reset;
     int64_t w_list_cap = 0;   // entries of each window neighbour-list buffer (0 = not sized yet)
@@ -845,6 +847,83 @@ int pick_chunk(int64_t T, int32_t H, int32_t W, int n_planes) {
 }
 
 template <typename T>
+__global__ void mean_accumulate_kernel(const T* __restrict__ frames, int nf, int64_t npix, float* __restrict__ acc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    float a = acc[i];
+    for (int t = 0; t < nf; t++) a = __fadd_rn(a, load_px<T>(frames, (size_t)t * npix + i));
+    acc[i] = a;
+}
+
+__global__ void mean_divide_kernel(float* acc, int64_t npix, float n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < npix) acc[i] = __fdiv_rn(acc[i], n);
+}
+
+// mean_from_iter (src/execute_gpu.rs:819-847) into device memory: the
+// sequential per-pixel sum over the frames, then / n_frames.
+template <typename T>
+gt_status mean_device(gt_ctx* ctx, const T* frames, bool on_device, int64_t NT, int32_t H, int32_t W, float* acc) {
+    const size_t npx = (size_t)H * W;
+    const int F = pick_chunk(NT, H, W, 0);
+    CK(cudaMemsetAsync(acc, 0, npx * 4, ctx->st));
+    if (!on_device) CK(ctx->stage[0].ensure((size_t)F * npx * sizeof(T)));
+    for (int64_t f0 = 0; f0 < NT; f0 += F) {
+        if (interrupted(ctx)) return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
+        int nf = (int)std::min<int64_t>(F, NT - f0);
+        const T* src = frames + f0 * npx;
+        if (!on_device) {
+            CK(cudaMemcpyAsync(ctx->stage[0].p, src, (size_t)nf * npx * sizeof(T), cudaMemcpyHostToDevice,
+                               ctx->st));
+            src = ctx->stage[0].as<T>();
+        }
+        Prof pf(ctx, "mean_frame");
+        mean_accumulate_kernel<T><<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(src, nf, npx, acc);
+        CK(cudaGetLastError());
+    }
+    {
+        Prof pf(ctx, "mean_frame");
+        mean_divide_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(acc, npx, (float)NT);
+    }
+    CK(cudaGetLastError());
+    return GT_OK;
+}
+
+// Illumination correction set-up (src/execute_gpu.rs:1324-1330, 849-884): the
+// smoothing taps exp(-x^2 / (2 sigma^2)), rint = i32(4 sigma + 0.5), and,
+// unless the profile is per frame, the smoothed mean frame of the whole call.
+template <typename T>
+gt_status illumination_setup(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
+                             int32_t W) {
+    const float sigma = p.illumination_sigma;
+    const float sigma2 = sigma * sigma;
+    const float rf = 4.0f * sigma + 0.5f;
+    if (!(rf < 65536.0f)) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "illumination_sigma too large");
+    const int32_t rint = (int32_t)rf;
+    std::vector<float> taps((size_t)(2 * rint + 1));
+    for (int32_t i = -rint; i <= rint; i++) {
+        const float x = (float)i;
+        const float x2 = x * x;
+        taps[(size_t)(i + rint)] = std::exp(-x2 / (2.0f * sigma2));
+    }
+    CKS(upload(ctx, ctx->illum_taps, taps));
+    ctx->illum_rint = rint;
+    if (!p.illumination_correction_per_frame) {
+        const size_t npx = (size_t)H * W;
+        CK(ctx->illum_shared.ensure(npx * 4));
+        CK(ctx->illum_prof.ensure(npx * 4));
+        float* mean = ctx->illum_shared.as<float>();
+        CKS(mean_device<T>(ctx, frames, on_device, NT, H, W, mean));
+        float* tmp = ctx->illum_prof.as<float>();
+        CK(launch_illum_smooth<float>(mean, (int64_t)npx, tmp, H, W, 0, ctx->illum_taps.as<float>(), rint, 1,
+                                      ctx->st));
+        CK(launch_illum_smooth<float>(tmp, (int64_t)npx, mean, H, W, 1, ctx->illum_taps.as<float>(), rint, 1,
+                                      ctx->st));
+    }
+    return GT_OK;
+}
+
+template <typename T>
 gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
                       int32_t W, const LocateConsts& c_in, const LogTables* lt, int F, uint32_t* out_flags,
                       PipeLink* pl, const std::vector<uint8_t>* reset) {
@@ -942,6 +1021,12 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     // after the walk (src/execute_gpu.rs:289-366)
     const bool std_pass = p.has_snr || p.has_minmass_snr;
     const bool adaptive = p.has_adaptive_background;
+    const bool illum = p.has_illumination_sigma != 0;
+    const int32_t illum_rint = ctx->illum_rint;
+    if (illum) {
+        CK(ctx->illum_corr.ensure((size_t)F * npx * 4));
+        if (p.illumination_correction_per_frame) CK(ctx->illum_prof.ensure((size_t)F * npx * 4));
+    }
     if (std_pass || adaptive) {
         CK(ctx->fstd.ensure((size_t)F * 4));
         CK(cudaMemsetAsync(ctx->fstd.p, 0, (size_t)F * 4, ctx->st));  // no std pass: the reference's buffer stays 0
@@ -1005,62 +1090,89 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)ns * 4, ctx->st));
         for (int64_t c0f = 0; c0f < ns; c0f += F) {
             const int nf = (int)std::min<int64_t>(F, ns - c0f);
-            const T* src = sbase + c0f * npx;
-            if (std_pass) {
-                Prof pf(ctx, "frame_std");
-                CK(launch_frame_std<T>(src, (int64_t)npx, nf, (int64_t)npx, nullptr, nullptr, ctx->fstd.as<float>(),
-                                       ctx->std_scratch.as<float>(), ctx->st));
-            }
-            CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
-            if (!log_style) {
-                Prof pf(ctx, "bandpass_localmax");
-                CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
-                                      ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+            // the locate stages of one chunk, on the input frames or on the
+            // illumination-corrected f32 frames
+            auto run_chunk = [&](auto* src) -> gt_status {
+                using TS = typename std::remove_const<typename std::remove_pointer<decltype(src)>::type>::type;
+                if (std_pass) {
+                    Prof pf(ctx, "frame_std");
+                    CK(launch_frame_std<TS>(src, (int64_t)npx, nf, (int64_t)npx, nullptr, nullptr, ctx->fstd.as<float>(),
+                                           ctx->std_scratch.as<float>(), ctx->st));
+                }
+                CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
+                if (!log_style) {
+                    Prof pf(ctx, "bandpass_localmax");
+                    CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
+                                          ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+                } else {
+                    {
+                        Prof pf(ctx, "bandpass");
+                        CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
+                                              ctx->st));
+                    }
+                    {
+                        Prof pf(ctx, "laplace");
+                        CK(launch_laplace<TS>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
+                                             ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
+                                             lnd.as<float>(), lt->max_rint, nf, ctx->st));
+                    }
+                    {
+                        Prof pf(ctx, "logspace_max");
+                        CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
+                                               ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+                    }
+                }
+                {
+                    Prof pf(ctx, "walk_characterize");
+                    CK(launch_walk<TS>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
+                                      ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap,
+                                      log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
+                                      ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap,
+                                      ctx->feat_count.as<uint32_t>() + c0f, feat_cap, flags, ctx->st));
+                }
+                if (adaptive) {
+                    // adaptive_filter passes over the chunk's walked rows; the
+                    // masked frame's std is recomputed before every pass but the first
+                    Prof pf(ctx, "adaptive");
+                    Feature* fr = ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap;
+                    uint32_t* fcn = ctx->feat_count.as<uint32_t>() + c0f;
+                    uint8_t* status = ctx->astatus.as<uint8_t>();
+                    uint32_t* counters = ctx->acount.as<uint32_t>();
+                    uint8_t* mask = ctx->amask.as<uint8_t>();
+                    CK(launch_adaptive_init(counters, (uint32_t)npx, status, (size_t)nf * feat_cap, nf, ctx->st));
+                    CK(cudaMemsetAsync(mask, 0, (size_t)nf * npx, ctx->st));
+                    for (uint32_t it = 0; it < p.adaptive_background; it++) {
+                        if (it > 0)
+                            CK(launch_frame_std<TS>(src, (int64_t)npx, nf, (int64_t)npx, mask, counters,
+                                                   ctx->fstd.as<float>(), ctx->std_scratch.as<float>(), ctx->st));
+                        CK(launch_adaptive_pass(fr, fcn, feat_cap, status, ctx->fstd.as<float>(), c.minmass,
+                                                c.minmass_snr, c.snr, mask, counters, H, W, c.circle, nf, ctx->st));
+                    }
+                    CK(launch_adaptive_compact(fr, fcn, feat_cap, status, nf, ctx->st));
+                }
+
+                return GT_OK;
+            };
+            const T* csrc = sbase + c0f * npx;
+            if (illum) {
+                Prof pf(ctx, "illumination");
+                float* corr = ctx->illum_corr.as<float>();
+                if (p.illumination_correction_per_frame) {
+                    // the profile of each frame is the frame itself, smoothed
+                    float* prof = ctx->illum_prof.as<float>();
+                    CK(launch_illum_smooth<T>(csrc, (int64_t)npx, corr, H, W, 0, ctx->illum_taps.as<float>(),
+                                              illum_rint, nf, ctx->st));
+                    CK(launch_illum_smooth<float>(corr, (int64_t)npx, prof, H, W, 1, ctx->illum_taps.as<float>(),
+                                                  illum_rint, nf, ctx->st));
+                    CK(launch_illum_divide<T>(csrc, (int64_t)npx, prof, (int64_t)npx, corr, (int64_t)npx, nf,
+                                              ctx->st));
+                } else {
+                    CK(launch_illum_divide<T>(csrc, (int64_t)npx, ctx->illum_shared.as<float>(), 0, corr,
+                                              (int64_t)npx, nf, ctx->st));
+                }
+                CKS(run_chunk((const float*)corr));
             } else {
-                {
-                    Prof pf(ctx, "bandpass");
-                    CK(launch_bandpass<T>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
-                                          ctx->st));
-                }
-                {
-                    Prof pf(ctx, "laplace");
-                    CK(launch_laplace<T>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
-                                         ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
-                                         lnd.as<float>(), lt->max_rint, nf, ctx->st));
-                }
-                {
-                    Prof pf(ctx, "logspace_max");
-                    CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
-                                           ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
-                }
-            }
-            {
-                Prof pf(ctx, "walk_characterize");
-                CK(launch_walk<T>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
-                                  ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap,
-                                  log_style ? lrad.as<float>() : nullptr, ctx->tabs_i.as<int32_t>(),
-                                  ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap,
-                                  ctx->feat_count.as<uint32_t>() + c0f, feat_cap, flags, ctx->st));
-            }
-            if (adaptive) {
-                // adaptive_filter passes over the chunk's walked rows; the
-                // masked frame's std is recomputed before every pass but the first
-                Prof pf(ctx, "adaptive");
-                Feature* fr = ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap;
-                uint32_t* fcn = ctx->feat_count.as<uint32_t>() + c0f;
-                uint8_t* status = ctx->astatus.as<uint8_t>();
-                uint32_t* counters = ctx->acount.as<uint32_t>();
-                uint8_t* mask = ctx->amask.as<uint8_t>();
-                CK(launch_adaptive_init(counters, (uint32_t)npx, status, (size_t)nf * feat_cap, nf, ctx->st));
-                CK(cudaMemsetAsync(mask, 0, (size_t)nf * npx, ctx->st));
-                for (uint32_t it = 0; it < p.adaptive_background; it++) {
-                    if (it > 0)
-                        CK(launch_frame_std<T>(src, (int64_t)npx, nf, (int64_t)npx, mask, counters,
-                                               ctx->fstd.as<float>(), ctx->std_scratch.as<float>(), ctx->st));
-                    CK(launch_adaptive_pass(fr, fcn, feat_cap, status, ctx->fstd.as<float>(), c.minmass,
-                                            c.minmass_snr, c.snr, mask, counters, H, W, c.circle, nf, ctx->st));
-                }
-                CK(launch_adaptive_compact(fr, fcn, feat_cap, status, nf, ctx->st));
+                CKS(run_chunk(csrc));
             }
         }
         {
@@ -1128,6 +1240,11 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
     LocateConsts c;
     CKS(make_locate_consts(ctx, p, H, W, c));
     set_fast_div<T>(ctx, c);
+    if (p.has_illumination_sigma) {
+        // the locate stages see the corrected f32 frames
+        c.fast_div = 0;
+        CKS(illumination_setup<T>(ctx, p, frames, on_device, NT, H, W));
+    }
     LogTables lt;
     const bool log_style = (p.style == GT_STYLE_LOG);
     if (log_style) {
@@ -1285,8 +1402,8 @@ gt_status validate(gt_ctx* ctx, const gt_params* p, const void* frames, int32_t 
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype);
     if (p->style != GT_STYLE_TRACKPY && p->style != GT_STYLE_LOG)
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "unknown style %d", p->style);
-    if (p->has_illumination_sigma)
-        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "illumination correction is not supported by this build");
+    if (p->has_illumination_sigma && !(p->illumination_sigma > 0.0f))
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "illumination_sigma must be positive");
     if (p->style == GT_STYLE_TRACKPY && p->diameter == 0)
         return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "diameter must be positive");
     CK(cudaSetDevice(ctx->device));
@@ -1328,45 +1445,11 @@ gt_status subset_groups(gt_ctx* ctx, const float* rows, int64_t n, int ncols, st
 }
 
 template <typename T>
-__global__ void mean_accumulate_kernel(const T* __restrict__ frames, int nf, int64_t npix, float* __restrict__ acc) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npix) return;
-    float a = acc[i];
-    for (int t = 0; t < nf; t++) a = __fadd_rn(a, load_px<T>(frames, (size_t)t * npix + i));
-    acc[i] = a;
-}
-
-__global__ void mean_divide_kernel(float* acc, int64_t npix, float n) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < npix) acc[i] = __fdiv_rn(acc[i], n);
-}
-
-template <typename T>
 gt_status mean_impl(gt_ctx* ctx, const T* frames, bool on_device, int64_t NT, int32_t H, int32_t W, float* out) {
     const size_t npx = (size_t)H * W;
-    const int F = pick_chunk(NT, H, W, 0);
     CK(ctx->processed.ensure(npx * 4));
     float* acc = ctx->processed.as<float>();
-    CK(cudaMemsetAsync(acc, 0, npx * 4, ctx->st));
-    if (!on_device) CK(ctx->stage[0].ensure((size_t)F * npx * sizeof(T)));
-    for (int64_t f0 = 0; f0 < NT; f0 += F) {
-        if (interrupted(ctx)) return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
-        int nf = (int)std::min<int64_t>(F, NT - f0);
-        const T* src = frames + f0 * npx;
-        if (!on_device) {
-            CK(cudaMemcpyAsync(ctx->stage[0].p, src, (size_t)nf * npx * sizeof(T), cudaMemcpyHostToDevice,
-                               ctx->st));
-            src = ctx->stage[0].as<T>();
-        }
-        Prof pf(ctx, "mean_frame");
-        mean_accumulate_kernel<T><<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(src, nf, npx, acc);
-        CK(cudaGetLastError());
-    }
-    {
-        Prof pf(ctx, "mean_frame");
-        mean_divide_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, ctx->st>>>(acc, npx, (float)NT);
-    }
-    CK(cudaGetLastError());
+    CKS(mean_device<T>(ctx, frames, on_device, NT, H, W, acc));
     CK(cudaMemcpyAsync(out, acc, npx * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return GT_OK;

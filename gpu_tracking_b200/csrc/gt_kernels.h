@@ -55,6 +55,14 @@ cudaError_t launch_adaptive_pass(const Feature* feats, const uint32_t* count, ui
                                  cudaStream_t st);
 cudaError_t launch_adaptive_compact(Feature* feats, uint32_t* count, uint32_t feat_cap, const uint8_t* status,
                                     int nframes, cudaStream_t st);
+// illumination correction: one separable smoothing pass of nframes profiles
+// (stride H*W in the output) and frame / profile (prof_stride 0: one profile)
+template <typename TIn>
+cudaError_t launch_illum_smooth(const TIn* in, int64_t in_stride, float* out, int H, int W, int dim, const float* g,
+                                int rint, int nframes, cudaStream_t st);
+template <typename T>
+cudaError_t launch_illum_divide(const T* frames, int64_t frame_stride, const float* prof, int64_t prof_stride,
+                                float* out, int64_t out_stride, int nframes, cudaStream_t st);
 
 size_t bandpass_smem_bytes(int R, int kd, bool cand);
 size_t finalize_smem_bytes();

@@ -278,4 +278,70 @@ GT_STD_INST(float)
 GT_STD_INST(uint8_t)
 #undef GT_STD_INST
 
+// --------------------------------------------------- illumination correction
+// smooth_mean_frame.wgsl, one pass (dim 0: along the rows' direction, u =
+// row; dim 1: along the columns): out = sum_i g_i * in / sum_i g_i over the
+// in-frame taps, the products accumulated by fused multiply-adds.  n_frames
+// is 1 in every call of the reference, so dim 0's norm is the tap sum.
+template <typename TIn>
+__global__ void illum_smooth_kernel(const TIn* __restrict__ in, int64_t in_stride, float* __restrict__ out, int H,
+                                    int W, int dim, const float* __restrict__ g, int rint) {
+    const int f = blockIdx.z;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (c >= W || r >= H) return;
+    const TIn* src = in + (size_t)f * in_stride;
+    const int u = dim == 0 ? r : c;
+    const int bound = dim == 0 ? H : W;
+    float gsum = 0.0f, nsum = 0.0f;
+    for (int i = -rint; i <= rint; i++) {
+        const int pu = u + i;
+        if (pu < 0 || pu >= bound) continue;
+        const size_t idx = dim == 0 ? (size_t)pu * W + c : (size_t)r * W + pu;
+        const float gv = __ldg(g + i + rint);
+        gsum = __fmaf_rn(gv, load_px<TIn>(src, idx), gsum);
+        nsum = __fadd_rn(nsum, gv);
+    }
+    out[(size_t)f * H * W + (size_t)r * W + c] = __fdiv_rn(gsum, nsum);
+}
+
+// correct_illumination.wgsl: frame / profile, per pixel
+template <typename T>
+__global__ void illum_divide_kernel(const T* __restrict__ frames, int64_t frame_stride, const float* __restrict__ prof,
+                                    int64_t prof_stride, float* __restrict__ out, int64_t out_stride, int64_t N) {
+    const int f = blockIdx.y;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    out[(size_t)f * out_stride + i] =
+        __fdiv_rn(load_px<T>(frames + (size_t)f * frame_stride, (size_t)i), prof[(size_t)f * prof_stride + i]);
+}
+
+template <typename TIn>
+cudaError_t launch_illum_smooth(const TIn* in, int64_t in_stride, float* out, int H, int W, int dim, const float* g,
+                                int rint, int nframes, cudaStream_t st) {
+    if (nframes <= 0) return cudaSuccess;
+    dim3 grid((W + 127) / 128, H, nframes);
+    illum_smooth_kernel<TIn><<<grid, 128, 0, st>>>(in, in_stride, out, H, W, dim, g, rint);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_illum_divide(const T* frames, int64_t frame_stride, const float* prof, int64_t prof_stride,
+                                float* out, int64_t out_stride, int nframes, cudaStream_t st) {
+    if (nframes <= 0) return cudaSuccess;
+    dim3 grid((unsigned)((out_stride + 255) / 256), nframes);
+    illum_divide_kernel<T><<<grid, 256, 0, st>>>(frames, frame_stride, prof, prof_stride, out, out_stride, out_stride);
+    return cudaGetLastError();
+}
+
+#define GT_ILLUM_INST(T)                                                                                      \
+    template cudaError_t launch_illum_smooth<T>(const T*, int64_t, float*, int, int, int, const float*, int, int, \
+                                                cudaStream_t);                                               \
+    template cudaError_t launch_illum_divide<T>(const T*, int64_t, const float*, int64_t, float*, int64_t, int, \
+                                                cudaStream_t);
+GT_ILLUM_INST(uint16_t)
+GT_ILLUM_INST(float)
+GT_ILLUM_INST(uint8_t)
+#undef GT_ILLUM_INST
+
 }  // namespace gt

@@ -636,6 +636,72 @@ struct FrameScratch {
     std::vector<std::pair<int32_t, int32_t>> cands;
 };
 
+// ------------------------------------------------------ illumination profile
+// smooth_mean_frame.wgsl through SeparableConvolution<2> (src/utils.rs:120-245,
+// src/gpu_setup.rs:317-340): pass 0 along the rows' direction (u = row), then
+// pass 1 along the columns, each result = sum_i gauss_i * x / sum_i gauss_i
+// over the in-frame taps i in [-rint, rint], rint = i32(4 sigma + 0.5),
+// gauss_i = exp(-x^2 / (2 sigma^2)); the accumulation of gauss * x is a fused
+// multiply-add (`gauss_sum += gauss * input[...]`).  n_frames = 1 in every
+// call the reference makes, so pass 0's norm is unchanged.
+static void smooth_profile(const float* in, int32_t H, int32_t W, float sigma, float* out, std::vector<float>& tmp) {
+    const float sigma2 = sigma * sigma;
+    const int32_t rint = wgsl_i32(4.0f * sigma + 0.5f);
+    std::vector<float> g((size_t)(2 * rint + 1));
+    for (int32_t i = -rint; i <= rint; i++) {
+        const float x = (float)i;
+        const float x2 = x * x;
+        g[(size_t)(i + rint)] = std::exp(-x2 / (2.0f * sigma2));
+    }
+    tmp.resize((size_t)H * W);
+    for (int pass = 0; pass < 2; pass++) {
+        const float* src = pass == 0 ? in : tmp.data();
+        float* dst = pass == 0 ? tmp.data() : out;
+        for (int32_t r = 0; r < H; r++) {
+            for (int32_t c = 0; c < W; c++) {
+                const int32_t u = pass == 0 ? r : c;
+                const int32_t bound = pass == 0 ? H : W;
+                float gsum = 0.0f, nsum = 0.0f;
+                for (int32_t i = -rint; i <= rint; i++) {
+                    const int32_t pu = u + i;
+                    if (pu < 0 || pu >= bound) continue;
+                    const size_t idx = pass == 0 ? (size_t)pu * W + c : (size_t)r * W + pu;
+                    const float gv = g[(size_t)(i + rint)];
+                    gsum = std::fmaf(gv, src[idx], gsum);
+                    nsum += gv;
+                }
+                float norm = nsum;
+                if (pass == 0) norm *= 1.0f;
+                dst[(size_t)r * W + c] = gsum / norm;
+            }
+        }
+    }
+}
+
+// The illumination-corrected frames (src/execute_gpu.rs:138-166, 819-884):
+// the profile is the smoothed mean frame (mean_from_iter: sequential sum over
+// the frames, / n_frames) or, per frame, the smoothed frame itself; every
+// pixel is divided by it (correct_illumination.wgsl: acc /= frame).
+static void illumination_correct(const gt_params& p, const float* frames, int64_t T, int32_t H, int32_t W,
+                                 std::vector<float>& out) {
+    const size_t npix = (size_t)H * W;
+    out.resize((size_t)T * npix);
+    std::vector<float> prof(npix), tmp;
+    if (!p.illumination_correction_per_frame) {
+        std::vector<float> mean(npix, 0.0f);
+        for (int64_t t = 0; t < T; t++)
+            for (size_t i = 0; i < npix; i++) mean[i] += frames[(size_t)t * npix + i];
+        const float nf = (float)T;
+        for (size_t i = 0; i < npix; i++) mean[i] /= nf;
+        smooth_profile(mean.data(), H, W, p.illumination_sigma, prof.data(), tmp);
+    }
+    for (int64_t t = 0; t < T; t++) {
+        const float* f = frames + (size_t)t * npix;
+        if (p.illumination_correction_per_frame) smooth_profile(f, H, W, p.illumination_sigma, prof.data(), tmp);
+        for (size_t i = 0; i < npix; i++) out[(size_t)t * npix + i] = f[i] / prof[i];
+    }
+}
+
 // snr / minmass_snr / adaptive_background combinations this restatement
 // reproduces (the library accepts the same ones):
 //  * the frame std needs a pixel count whose reduction levels are all
@@ -1212,6 +1278,14 @@ int oracle_preprocess(const gt_params* p, const float* frame, int32_t H, int32_t
     return GT_OK;
 }
 
+// The smoothed illumination profile of one frame (SeparableConvolution<2>
+// with smooth_mean_frame.wgsl).
+int oracle_smooth_profile(const float* in, int32_t H, int32_t W, float sigma, float* out) {
+    std::vector<float> tmp;
+    smooth_profile(in, H, W, sigma, out, tmp);
+    return GT_OK;
+}
+
 // Frame std as the reference computes it (StdArray::execute); frame may
 // hold the 0xFFFFFFFF masked-pixel pattern.  Returns an error for pixel
 // counts whose reduction is not exact (see std_clean).
@@ -1304,6 +1378,11 @@ int oracle_batch(const gt_params* p, const float* frames, int64_t T, int32_t H, 
     auto radii = log_radii(*p);
     std::vector<std::vector<Row>> per_frame((size_t)T);
     const size_t npix = (size_t)H * W;
+    // with illumination correction every stage but the doughnut sees the
+    // corrected frames (the doughnut reads the host frames)
+    std::vector<float> corrected;
+    if (p->has_illumination_sigma) illumination_correct(*p, frames, T, H, W, corrected);
+    const float* located = p->has_illumination_sigma ? corrected.data() : frames;
     // frames are independent: locate them on nthreads host threads
     if (nthreads <= 0) nthreads = (int32_t)std::max(1u, std::thread::hardware_concurrency());
     nthreads = (int32_t)std::min<int64_t>(nthreads, T);
@@ -1311,7 +1390,7 @@ int oracle_batch(const gt_params* p, const float* frames, int64_t T, int32_t H, 
     auto worker = [&]() {
         FrameScratch s;
         for (int64_t t = next++; t < T; t = next++)
-            locate_frame(*p, d, radii, frames + (size_t)t * npix, s, per_frame[(size_t)t]);
+            locate_frame(*p, d, radii, located + (size_t)t * npix, s, per_frame[(size_t)t]);
     };
     std::vector<std::thread> pool;
     for (int32_t i = 1; i < nthreads; i++) pool.emplace_back(worker);

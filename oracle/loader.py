@@ -54,6 +54,7 @@ def lib():
         L.oracle_adaptive.argtypes = [vp, c_f32p, ctypes.c_int32, ctypes.c_int32, c_f32p, ctypes.c_int64,
                                       ctypes.c_uint32, ctypes.c_float, ctypes.c_int32, c_f32p]
         L.oracle_adaptive.restype = ctypes.c_int64
+        L.oracle_smooth_profile.argtypes = [c_f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_f32p]
         L.oracle_log_planes.argtypes = [vp, c_f32p, ctypes.c_int32, ctypes.c_int32, c_f32p, c_f32p]
         L.oracle_batch.argtypes = [vp, c_f32p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
                                    ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(vp)]
@@ -96,6 +97,7 @@ def ref():
         L.ref_adaptive.argtypes = [vp, c_f32p, c_f32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_float, ctypes.c_int32,
                                    c_f32p, c_f32p]
         L.ref_adaptive.restype = ctypes.c_int64
+        L.ref_illumination.argtypes = [vp, c_f32p, ctypes.c_float, c_f32p, c_f32p]
         _REF = L
     return _REF
 
@@ -164,6 +166,14 @@ def frame_std(frame, divisor=None):
     _check(lib().oracle_frame_std(_ptr(frame, c_f32p), frame.size, frame.size if divisor is None else divisor,
                                   ctypes.byref(out)))
     return np.float32(out.value)
+
+
+def smooth_profile(frame, sigma):
+    frame = _f32(frame)
+    H, W = frame.shape
+    out = np.empty_like(frame)
+    _check(lib().oracle_smooth_profile(_ptr(frame, c_f32p), H, W, sigma, _ptr(out, c_f32p)))
+    return out
 
 
 def adaptive(p, frame, rows, n_iter, std0, recompute=True):
@@ -313,3 +323,12 @@ def ref_logspace_max(p, bottom, middle, top, processed, edge, radius, pic_std=0.
     n = ref().ref_logspace_max(gpu_params(p, H, W), _ptr(bottom, c_f32p), _ptr(middle, c_f32p), _ptr(top, c_f32p),
                                _ptr(processed, c_f32p), pic_std, edge, radius, _ptr(uv, c_i32p), cap)
     return uv[:n].copy()
+
+
+def ref_illumination(p, profile, sigma, frame):
+    """Smoothed profile and the corrected frame, with the reference's shaders."""
+    profile, frame = _f32(profile), _f32(frame).copy()
+    H, W = frame.shape
+    out = np.empty_like(profile)
+    ref().ref_illumination(gpu_params(p, H, W), _ptr(profile, c_f32p), sigma, _ptr(frame, c_f32p), _ptr(out, c_f32p))
+    return out, frame

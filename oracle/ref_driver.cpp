@@ -120,6 +120,8 @@ inline float wgsl_bitcast_f32(uint32_t u) {
 #include "_ref/gen_last_reduction.inc"
 #include "_ref/gen_std_image.inc"
 #include "_ref/gen_adaptive_filter.inc"
+#include "_ref/gen_smooth_mean_frame.inc"
+#include "_ref/gen_correct_illumination.inc"
 
 // Flat copy of the WGSL Params uniform (params.wgsl:1-20).
 struct RefParams {
@@ -368,6 +370,32 @@ int64_t ref_adaptive(const RefParams* p, float* frame, const float* rows_in, int
     }
     std::memcpy(rows_out, res.data(), (size_t)result_n * sizeof(Row));
     return result_n;
+}
+
+// SeparableConvolution<2>::execute with smooth_mean_frame.wgsl on the
+// illumination buffer (input = output = the buffer, temp = the shared temp
+// buffer; push constants dim, sigma, n_frames = 1), then correct_illumination
+// over `frame` (frame /= profile).  profile_out receives the smoothed buffer.
+int ref_illumination(const RefParams* p, const float* profile_in, float sigma, float* frame_inout,
+                     float* profile_out) {
+    const int32_t H = p->pic_nrows, W = p->pic_ncols;
+    const int64_t N = (int64_t)H * W;
+    std::vector<float> buf(profile_in, profile_in + N), temp((size_t)(2 * N));
+    set_params(sh_smooth_mean_frame::params, p);
+    sh_smooth_mean_frame::pc = {0u, sigma, 1.0f};
+    bind(sh_smooth_mean_frame::input, buf.data(), N);
+    bind(sh_smooth_mean_frame::output, temp.data(), 2 * N);
+    dispatch2d(H, W, [](uvec3 g) { sh_smooth_mean_frame::main_(g); });
+    sh_smooth_mean_frame::pc = {1u, sigma, 1.0f};
+    bind(sh_smooth_mean_frame::input, temp.data(), 2 * N);
+    bind(sh_smooth_mean_frame::output, buf.data(), N);
+    dispatch2d(H, W, [](uvec3 g) { sh_smooth_mean_frame::main_(g); });
+    std::memcpy(profile_out, buf.data(), (size_t)N * 4);
+    sh_correct_illumination::pc.arraylen = (uint32_t)N;
+    bind(sh_correct_illumination::frame, buf.data(), N);
+    bind(sh_correct_illumination::acc, frame_inout, N);
+    for (uint32_t x = 0; x < (uint32_t)N; x++) sh_correct_illumination::main_(uvec3{x, 0u, 0u});
+    return 0;
 }
 
 }  // extern "C"

@@ -47,6 +47,9 @@ SHADERS = {
     "last_reduction": "src/shaders/last_reduction.wgsl",
     "std_image": "src/shaders/std_image.wgsl",
     "adaptive_filter": "src/shaders/adaptive_filter.wgsl",
+    # illumination correction (src/execute_gpu.rs:138-166, 849-884)
+    "smooth_mean_frame": "src/shaders/correct_illumination/smooth_mean_frame.wgsl",
+    "correct_illumination": "src/shaders/correct_illumination/correct_illumination.wgsl",
 }
 
 TYPE_MAP = {

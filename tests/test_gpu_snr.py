@@ -61,3 +61,34 @@ def test_snr_errors():
         gt.batch(ok, 9, adaptive_background=2, tqdm=False)
     # one adaptive pass needs no std: the std buffer stays 0 as in the reference
     gt.batch(ok, 9, adaptive_background=1, minmass=100.0, tqdm=False)
+
+
+def vignetted(T, H, W, seed):
+    frames, _ = video(T, H, W, 40, seed=seed)
+    yy, xx = np.mgrid[0:H, 0:W]
+    shade = 0.6 + 0.4 * np.exp(-((yy - H * 0.4) ** 2 + (xx - W * 0.6) ** 2) / (0.5 * H * W))
+    return np.round(frames * shade).astype(np.uint16)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(correct_illumination=True),
+    dict(illumination_sigma=6.0, illumination_correction_per_frame=True),
+    dict(illumination_sigma=10.0, snr=0.3, minmass_snr=0.3, adaptive_background=2),
+])
+def test_illumination_correction_matches_oracle(oracle, kw):
+    """Every locate stage sees frame / smoothed profile; the doughnut reads the
+    uncorrected frames (the reference's host frames)."""
+    frames = vignetted(3, 128, 128, 71)
+    kw = dict(kw, minmass=kw.get("minmass", 1.5) if "minmass_snr" not in kw else 0.0, search_range=5.0)
+    df = gt.batch(frames, 9, tqdm=False, **kw)
+    tab = oracle.batch(trackpy_params(9, **kw), frames.astype(np.float32))
+    assert len(df) > 20
+    assert_same(df, tab, ALL_TP + ["particle"])
+
+
+def test_illumination_with_log(oracle):
+    frames = vignetted(2, 96, 128, 72).astype(np.float32)
+    kw = dict(n_radii=5, illumination_sigma=8.0)
+    df = gt.LoG(frames, 2.0, 4.0, tqdm=False, **kw)
+    tab = oracle.batch(log_params(2.0, 4.0, **kw), frames)
+    assert_same(df, tab, ["frame", "y", "x", "mass", "r"])

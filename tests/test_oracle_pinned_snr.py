@@ -82,3 +82,17 @@ def test_adaptive_filter_bit_exact(oracle, n_iter, kw):
     if n_iter > 1:
         # later passes see a masked frame: fewer or equal acceptances than one pass would give
         assert len(mine) >= len(oracle.adaptive(p, f, walked, 1, sd))
+
+
+@pytest.mark.parametrize("sigma,shape", [(3.0, (40, 56)), (7.5, (64, 48)), (30.0, (33, 70))])
+def test_illumination_profile_and_correction_bit_exact(oracle, sigma, shape):
+    """smooth_mean_frame.wgsl (two separable passes) and correct_illumination.wgsl."""
+    rng = np.random.default_rng(int(sigma * 10))
+    yy, xx = np.mgrid[0:shape[0], 0:shape[1]]
+    prof = (100 + 40 * np.exp(-((yy - shape[0] / 3) ** 2 + (xx - shape[1] / 2) ** 2) / 400.0)).astype(np.float32)
+    frame = (prof * rng.uniform(0.5, 2.0, shape)).astype(np.float32)
+    p = trackpy_params(9, illumination_sigma=sigma)
+    smooth, corrected = oracle.ref_illumination(p, prof, sigma, frame)
+    mine = oracle.smooth_profile(prof, sigma)
+    assert np.array_equal(bits(mine), bits(smooth))
+    assert np.array_equal(bits(frame / mine), bits(corrected))
