@@ -72,6 +72,7 @@ def lib():
         L.gt_table_has_column.restype = i32
         L.gt_table_free.argtypes = [vp]
         L.gt_batch.argtypes = [vp, P(GtParams), vp, i32, i64, i32, i32, P(i64), P(i64), i64, P(vp)]
+        L.gt_batch_videos.argtypes = [vp, P(GtParams), i32, P(vp), i32, P(i64), P(i32), P(i32), P(vp)]
         L.gt_characterize_points.argtypes = [vp, P(GtParams), vp, i32, i64, i32, i32, P(f32), i64, i32, i32,
                                              P(vp)]
         L.gt_link.argtypes = [vp, P(f32), i64, f32, ctypes.c_uint32, P(i64)]
@@ -82,7 +83,7 @@ def lib():
         L.gt_launch_count.argtypes = [vp]
         L.gt_launch_count.restype = i64
         for name in ("gt_create", "gt_set_interrupt", "gt_progress", "gt_table_column_f32", "gt_table_column_i64",
-                     "gt_batch", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
+                     "gt_batch", "gt_batch_videos", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
                      "gt_profile_enable", "gt_profile_read"):
             getattr(L, name).restype = i32
         _lib = L

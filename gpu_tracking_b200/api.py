@@ -194,6 +194,43 @@ def batch(file_or_array, diameter, **kwargs):
     return _locate(file_or_array, params, kwargs)
 
 
+def batch_videos(videos, diameter, **kwargs):
+    """``batch`` over many videos (any frame sizes and lengths) in one call.
+
+    Returns one DataFrame per video, each equal to ``batch(video, diameter,
+    **kwargs)``.  The videos are located one after another and then linked
+    together in one GPU launch (one linker per video running side by side),
+    which is where a loop of ``batch`` calls spends most of its time on many
+    short videos.  ``frames`` and ``linker_reset_points`` are not supported
+    here.  Not part of the reference's API (it processes one video per call).
+    """
+    for k in ("frames", "linker_reset_points"):
+        if kwargs.get(k) is not None:
+            raise TypeError("batch_videos does not take %r" % k)
+    params = trackpy_params(diameter, **kwargs)
+    ctx = _ffi.context(_DEVICE)
+    frs = [_Frames(v) for v in videos]
+    if len({f.dtype for f in frs}) > 1:
+        frs = [_Frames(np.asarray(v, np.float32)) if not hasattr(v, "is_cuda") else _Frames(v.float())
+               for v in videos]
+    n = len(frs)
+    if n == 0:
+        return []
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
+    ptrs = (vp * n)(*[f.ptr for f in frs])
+    Ts = (i64 * n)(*[f.T for f in frs])
+    Hs = (i32 * n)(*[f.H for f in frs])
+    Ws = (i32 * n)(*[f.W for f in frs])
+    outs = (vp * n)()
+
+    def call():
+        return _ffi.lib().gt_batch_videos(ctx.handle, ctypes.byref(params), n, ptrs, frs[0].dtype, Ts, Hs, Ws, outs)
+
+    st = _run(ctx, call, False)
+    ctx.check(st)
+    return [_table_to_frame(ctx, ctypes.c_void_p(outs[i]), params) for i in range(n)]
+
+
 def LoG(file_or_array, min_radius, max_radius, **kwargs):
     """Laplacian-of-Gaussian blob tracking (generated.py:164-227).
 

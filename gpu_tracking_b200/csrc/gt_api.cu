@@ -1613,6 +1613,88 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
     return GT_OK;
 }
 
+// Many videos in one call: each video is located into its own table (as
+// gt_batch would, without linking), then every video is linked in ONE launch
+// of the whole-video linker (one CTA per video), so the videos' sequential
+// frame scans run side by side.  Results equal separate gt_batch calls.
+template <typename T>
+gt_status batch_videos_impl(gt_ctx* ctx, const gt_params& p, int32_t n_videos, const void* const* frames,
+                            const int64_t* T_, const int32_t* H_, const int32_t* W_, gt_table** tabs) {
+    gt_params pl = p;
+    pl.has_search_range = 0;
+    std::vector<std::vector<int64_t>> row_off((size_t)n_videos);
+    for (int32_t v = 0; v < n_videos; v++) {
+        bool on_device = false;
+        CKS(check_frames_ptr(ctx, frames[v], &on_device));
+        const int64_t NT = T_[v];
+        gt_status st = batch_impl<T>(ctx, pl, (const T*)frames[v], on_device, NT, H_[v], W_[v], nullptr, nullptr, 0,
+                                     tabs[v]);
+        if (st != GT_OK) return st;
+        // rows of frame t are [row_off[t], row_off[t+1]) (batch_impl's kept counts)
+        std::vector<uint32_t> kept((size_t)NT);
+        CK(cudaMemcpyAsync(kept.data(), ctx->kept_count.p, (size_t)NT * 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        auto& ro = row_off[(size_t)v];
+        ro.assign((size_t)NT + 1, 0);
+        for (int64_t t = 0; t < NT; t++) ro[(size_t)t + 1] = ro[(size_t)t] + kept[(size_t)t];
+        if (ro.back() != tabs[v]->n) return set_err(ctx, GT_ERR_INTERNAL, "row count mismatch");
+    }
+    if (!p.has_search_range) return GT_OK;
+    LinkJob job;
+    job.vgrp.push_back(0);
+    job.goff.push_back(0);
+    int64_t N = 0;
+    for (int32_t v = 0; v < n_videos; v++) {
+        const auto& ro = row_off[(size_t)v];
+        for (size_t t = 1; t < ro.size(); t++) job.goff.push_back(N + ro[t]);
+        N += ro.back();
+        job.vgrp.push_back((int32_t)(job.goff.size() - 1));
+    }
+    job.reset.assign(job.goff.size() - 1, 0);
+    job.radius = p.search_range;
+    job.memory = (int32_t)p.memory;
+    const size_t n1 = (size_t)std::max<int64_t>(N, 1);
+    CK(ctx->l_px.ensure(n1 * 4));
+    CK(ctx->l_py.ensure(n1 * 4));
+    CK(ctx->l_ids.ensure(n1 * 8));
+    CK(ctx->l_rowdur.ensure(n1 * 8));
+    float* px = ctx->l_px.as<float>();
+    float* py = ctx->l_py.as<float>();
+    int64_t base = 0;
+    for (int32_t v = 0; v < n_videos; v++) {
+        const int64_t n = tabs[v]->n;
+        if (n > 0) {
+            CK(cudaMemcpyAsync(px + base, tabs[v]->col[GT_COL_Y].p, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(py + base, tabs[v]->col[GT_COL_X].p, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->st));
+        }
+        base += n;
+    }
+    {
+        HostSpan hs(ctx, "host_link");
+        CKS(run_link(ctx, job, px, py, ctx->l_ids.as<int64_t>(), ctx->l_rowdur.as<int64_t>(), nullptr, nullptr));
+    }
+    base = 0;
+    for (int32_t v = 0; v < n_videos; v++) {
+        gt_table* tab = tabs[v];
+        const int64_t n = tab->n;
+        const size_t m = (size_t)std::max<int64_t>(n, 1);
+        CK(tab->particle.ensure(m * 8));
+        CK(tab->duration.ensure(m * 8));
+        if (n > 0) {
+            f32_round_ids_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->st>>>(ctx->l_ids.as<int64_t>() + base,
+                                                                                 tab->particle.as<int64_t>(), n);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(tab->duration.p, ctx->l_rowdur.as<int64_t>() + base, (size_t)n * 8,
+                               cudaMemcpyDeviceToDevice, ctx->st));
+        }
+        tab->has[GT_COL_PARTICLE] = true;
+        tab->has[GT_COL_DURATION] = true;
+        base += n;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return GT_OK;
+}
+
 }  // namespace
 
 // =================================================================== C ABI
@@ -1795,6 +1877,33 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
         return st;
     }
     *out = tab.release();
+    return GT_OK;
+}
+
+gt_status gt_batch_videos(gt_ctx* ctx, const gt_params* params, int32_t n_videos, const void* const* frames,
+                          int32_t dtype, const int64_t* T, const int32_t* H, const int32_t* W, gt_table** out) {
+    if (!out || !frames || !T || !H || !W || n_videos < 0) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
+    for (int32_t v = 0; v < n_videos; v++) out[v] = nullptr;
+    for (int32_t v = 0; v < n_videos; v++) CKS(validate(ctx, params, frames[v], dtype, T[v], H[v], W[v]));
+    std::vector<std::unique_ptr<gt_table>> tabs((size_t)n_videos);
+    std::vector<gt_table*> raw((size_t)n_videos);
+    for (int32_t v = 0; v < n_videos; v++) {
+        tabs[(size_t)v].reset(new gt_table(ctx->device, ctx->st));
+        raw[(size_t)v] = tabs[(size_t)v].get();
+    }
+    gt_status st;
+    if (dtype == GT_DTYPE_U16)
+        st = batch_videos_impl<uint16_t>(ctx, *params, n_videos, frames, T, H, W, raw.data());
+    else if (dtype == GT_DTYPE_F32)
+        st = batch_videos_impl<float>(ctx, *params, n_videos, frames, T, H, W, raw.data());
+    else
+        st = batch_videos_impl<uint8_t>(ctx, *params, n_videos, frames, T, H, W, raw.data());
+    if (st != GT_OK) {
+        cudaStreamSynchronize(ctx->st);
+        cudaStreamSynchronize(ctx->lk);
+        return st;
+    }
+    for (int32_t v = 0; v < n_videos; v++) out[v] = tabs[(size_t)v].release();
     return GT_OK;
 }
 

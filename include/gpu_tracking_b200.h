@@ -161,6 +161,19 @@ GT_API gt_status gt_batch(gt_ctx* ctx, const gt_params* params,
                    gt_table** out);
 
 /*
+ * gt_batch over many videos of any sizes in one call: out[v] receives video
+ * v's table, equal to what gt_batch(frames[v], T[v], H[v], W[v]) returns
+ * (frame numbers 0..T[v]-1, no linker resets).  The videos share params and
+ * dtype; linking runs for all videos in one launch.  Replaces a loop of
+ * execute_ndarray calls (src/execute_gpu.rs:1378-1403), one per video; the
+ * reference has no multi-video entry point.
+ */
+GT_API gt_status gt_batch_videos(gt_ctx* ctx, const gt_params* params, int32_t n_videos,
+                          const void* const* frames, int32_t dtype,
+                          const int64_t* T, const int32_t* H, const int32_t* W,
+                          gt_table** out);
+
+/*
  * Characterize given points instead of detected ones.  Replaces
  * characterize_points_rust (gpu_tracking_macros/src/lib.rs:641-683) and the
  * FrameSubsetter characterization path (src/execute_gpu.rs:189-229,
