@@ -1695,6 +1695,15 @@ gt_status batch_videos_impl(gt_ctx* ctx, const gt_params& p, int32_t n_videos, c
     return GT_OK;
 }
 
+// Fills the shared memory of every resident CTA slot with hashed non-zero
+// words: what a kernel finds in shared memory it has not written depends on
+// the kernels that ran before it, and this makes that content adversarial.
+__global__ void scribble_shared_kernel(uint32_t seed, int nwords) {
+    extern __shared__ uint32_t sw[];
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x)
+        sw[i] = (seed ^ ((uint32_t)i * 2654435761u) ^ (blockIdx.x * 40503u)) | 0x00800000u;
+}
+
 }  // namespace
 
 // =================================================================== C ABI
@@ -1713,6 +1722,21 @@ GT_API gt_status gt__set_link_window_caps(gt_ctx* ctx, int64_t list_entries, int
     if (!ctx) return GT_ERR_INVALID_ARGUMENT;
     ctx->w_list_cap = list_entries;
     ctx->w_edge_cap = edges_per_frame;
+    return GT_OK;
+}
+
+// Test hook (exported, not part of the public header): overwrite the shared
+// memory of every SM with non-zero words on the context's stream, so that a
+// following call shows any dependence on shared memory it did not write.
+GT_API gt_status gt__scribble_shared_memory(gt_ctx* ctx, uint32_t seed) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, ctx->device));
+    const int bytes = (int)prop.sharedMemPerBlockOptin;
+    CK(cudaFuncSetAttribute(scribble_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    scribble_shared_kernel<<<prop.multiProcessorCount * 4, 1024, bytes, ctx->st>>>(seed, bytes / 4);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
     return GT_OK;
 }
 

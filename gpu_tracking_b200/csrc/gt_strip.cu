@@ -177,6 +177,13 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
         }
     };
     load_raw(0);
+    // The first column-pass groups read row-pass rows above x0 that no step
+    // writes.  The outputs that need them are never used, but the sliding
+    // boxcar sum of a group carries its first window into the rows after it
+    // (cs + new - old cancels exactly only for finite integers), so the rings
+    // start as zeros instead of whatever the previous kernel left.
+    for (int i = tid; i < 2 * 2 * XR * PWp / 4; i += kStripThreads)
+        ((float4*)xg)[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float trunc_thr = 1.0f / 255.0f;
     // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
     const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
