@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="frames in the CPU-baseline sample (0: auto)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="headline", choices=["headline", "ragged"],
+                    help="headline: the 2000-frame 2048^2 video; ragged: 64 videos of uneven size and length")
+    ap.add_argument("--scale", type=float, default=0.25,
+                    help="ragged: fraction of the configured 50-1000 frames per video")
     return ap.parse_args()
 
 
@@ -190,10 +194,110 @@ def run_reference(args):
     return 0
 
 
+RAGGED = dict(workload="64 ragged uint16 videos: sides in {256,512,1024,2048}, 50-1000 frames (x scale), "
+                        "density 1e-4..2e-3 spots/px^2, D 0.2..2", videos=64, diameter=11, minmass=220.0,
+              search_range=7.0, memory=3, seed=4)
+
+
+def ragged_videos(scale, device):
+    """The 64 videos of the ragged workload, generated on the device."""
+    import numpy as np
+    from gpu_tracking_b200.synth import brownian_video
+    rng = np.random.default_rng(RAGGED["seed"])
+    vids = []
+    for k in range(RAGGED["videos"]):
+        H = int(rng.choice([256, 512, 1024, 2048]))
+        W = int(rng.choice([256, 512, 1024, 2048]))
+        T = max(1, int(rng.integers(50, 1001) * scale))
+        n = max(1, int(rng.uniform(1e-4, 2e-3) * H * W))
+        D = float(rng.uniform(0.2, 2.0))
+        vids.append(brownian_video(T, H, W, n, seed=1000 + k, device=device, D=D))
+    return vids
+
+
+def run_ragged(args):
+    """Frames/s of the ragged workload through gt_batch_videos (device-resident),
+    beside the same videos through one gt_batch call each."""
+    import ctypes
+
+    import torch
+    from gpu_tracking_b200 import _ffi
+    from gpu_tracking_b200._params import DTYPE_U16, trackpy_params
+    torch.cuda.set_device(0)
+    vids = ragged_videos(args.scale, "cuda:0")
+    torch.cuda.synchronize()
+    p = trackpy_params(RAGGED["diameter"], minmass=RAGGED["minmass"], search_range=RAGGED["search_range"],
+                       memory=RAGGED["memory"])
+    ctx = _ffi.context(0)
+    L = _ffi.lib()
+    n = len(vids)
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
+    ptrs = (vp * n)(*[v.data_ptr() for v in vids])
+    Ts = (i64 * n)(*[v.shape[0] for v in vids])
+    Hs = (i32 * n)(*[v.shape[1] for v in vids])
+    Ws = (i32 * n)(*[v.shape[2] for v in vids])
+    frames = sum(v.shape[0] for v in vids)
+    pixels = sum(v.numel() for v in vids)
+
+    def together():
+        outs = (vp * n)()
+        ctx.check(L.gt_batch_videos(ctx.handle, ctypes.byref(p), n, ptrs, DTYPE_U16, Ts, Hs, Ws, outs))
+        rows = 0
+        for i in range(n):
+            rows += L.gt_table_nrows(outs[i])
+            L.gt_table_free(outs[i])
+        return rows
+
+    def loop():
+        rows = 0
+        for v in vids:
+            out = vp()
+            ctx.check(L.gt_batch(ctx.handle, ctypes.byref(p), vp(v.data_ptr()), DTYPE_U16, v.shape[0], v.shape[1],
+                                 v.shape[2], None, None, 0, ctypes.byref(out)))
+            rows += L.gt_table_nrows(out)
+            L.gt_table_free(out)
+        return rows
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rows = 0
+        for _ in range(args.steps):
+            rows = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, rows
+
+    clocks = Clocks(0)
+    clocks.start()
+    n0 = ctx.launch_count()
+    ms, rows = timed(together)
+    launches = (ctx.launch_count() - n0) // (args.warmup + args.steps)
+    clk = clocks.stop()
+    ms_loop, rows_loop = timed(loop)
+    if rows != rows_loop:
+        raise SystemExit("gt_batch_videos found %d rows, the gt_batch loop %d" % (rows, rows_loop))
+    line = {"metric": "frames/s, 64 ragged videos (one gt_batch_videos call)", "value": frames / (ms / 1000.0),
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(RAGGED, scale=args.scale, frames=frames, pixels=pixels,
+                           l2="inputs (%.1f GB) larger than L2; no flush" % (pixels * 2 / 1e9)),
+            "features_per_s": rows / (ms / 1000.0), "features": rows,
+            "loop_of_gt_batch": {"value": frames / (ms_loop / 1000.0), "ms_per_step": ms_loop},
+            "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ragged":
+        return run_ragged(args)
     import ctypes
 
     import numpy as np
