@@ -45,6 +45,13 @@ def to_exception(status, message):
     return GpuTrackingError(status, message)
 
 
+class TrainOpts(ctypes.Structure):
+    """gt_train_opts (include/gpu_tracking_b200.h)."""
+    _fields_ = [("steps", ctypes.c_int32), ("batch", ctypes.c_int32), ("crop", ctypes.c_int32),
+                ("lr", ctypes.c_float), ("pos_weight", ctypes.c_float), ("offset_weight", ctypes.c_float),
+                ("seed", ctypes.c_uint32)]
+
+
 def lib():
     global _lib
     with _lock:
@@ -82,9 +89,25 @@ def lib():
         L.gt_profile_read.argtypes = [vp, ctypes.c_char_p, P(i64), P(ctypes.c_double)]
         L.gt_launch_count.argtypes = [vp]
         L.gt_launch_count.restype = i64
+        L.gt_train_opts_default.argtypes = [P(TrainOpts)]
+        L.gt_proposal_num_params.restype = i64
+        L.gt_proposal_create.argtypes = [vp, ctypes.c_uint64, P(vp)]
+        L.gt_proposal_destroy.argtypes = [vp]
+        L.gt_proposal_set.argtypes = [vp, vp, P(f32), f32, f32, f32]
+        L.gt_proposal_get.argtypes = [vp, vp, P(f32), P(f32), P(f32), P(f32)]
+        L.gt_proposal_train.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(i64), P(f32), P(f32), i64, P(TrainOpts),
+                                        P(f32)]
+        L.gt_proposal_maps.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(f32)]
+        L.gt_batch_learned.argtypes = [vp, P(GtParams), vp, vp, i32, i64, i32, i32, P(i64), P(i64), i64, P(vp)]
+        L.gt_last_walk_starts.argtypes = [vp]
+        L.gt_last_walk_starts.restype = i64
+        L.gt__proposal_loss_grad.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(i64), P(f32), P(f32), i64, P(i32), i32,
+                                             i32, f32, f32, P(f32), P(f32)]
         for name in ("gt_create", "gt_set_interrupt", "gt_progress", "gt_table_column_f32", "gt_table_column_i64",
                      "gt_batch", "gt_batch_videos", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
-                     "gt_profile_enable", "gt_profile_read"):
+                     "gt_profile_enable", "gt_profile_read", "gt_proposal_create", "gt_proposal_set",
+                     "gt_proposal_get", "gt_proposal_train", "gt_proposal_maps", "gt_batch_learned",
+                     "gt__proposal_loss_grad"):
             getattr(L, name).restype = i32
         _lib = L
         return L

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "gt_kernels.h"
+#include "gt_proposal.h"
 
 using namespace gt;
 
@@ -121,6 +122,7 @@ struct KernelStat {
 
 struct gt_ctx {
     int device = 0;
+    int num_sms = 148;
     cudaStream_t st = nullptr;   // compute
     cudaStream_t cp = nullptr;   // host -> device copies
     cudaStream_t lk = nullptr;   // linking of located frames, overlapped with locating
@@ -144,6 +146,9 @@ struct gt_ctx {
     // windowed linking inside gt_batch (slot mode)
     DBuf fstd, std_scratch, amask, astatus, acount;   // snr / minmass_snr / adaptive_background
     DBuf illum_taps, illum_shared, illum_prof, illum_corr;  // illumination correction
+    DBuf cnn_x, cnn_p, cnn_q, cnn_head;   // learned proposals: network input, activations, outputs
+    DBuf walk_starts;                     // walk starts of the current call (u64)
+    int64_t last_walk_starts = 0;
     int32_t illum_rint = 0;
     DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
         w_cnt, w_flags, w_vgrp, w_reset;
@@ -679,6 +684,15 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     return GT_OK;
 }
 
+// acc += sum of min(count[i], cap) over the chunk's frames (walk starts)
+__global__ void sum_counts_kernel(const uint32_t* __restrict__ count, int n, uint32_t cap,
+                                  unsigned long long* __restrict__ acc) {
+    unsigned long long s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += min(count[i], cap);
+    for (int d = 16; d; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
+}
+
 __global__ void f32_round_ids_kernel(const int64_t* ids, int64_t* out, int64_t n) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (int64_t)(float)ids[i];
@@ -926,7 +940,7 @@ gt_status illumination_setup(gt_ctx* ctx, const gt_params& p, const T* frames, b
 template <typename T>
 gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
                       int32_t W, const LocateConsts& c_in, const LogTables* lt, int F, uint32_t* out_flags,
-                      PipeLink* pl, const std::vector<uint8_t>* reset) {
+                      PipeLink* pl, const std::vector<uint8_t>* reset, const gt_proposal* net) {
     LocateConsts c = c_in;
     const size_t npx = (size_t)H * W;
     const bool log_style = (p.style == GT_STYLE_LOG);
@@ -947,6 +961,8 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     CK(ctx->kept_count.ensure((size_t)NT * 4));
     CK(ctx->flags.ensure(16));
     CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
+    CK(ctx->walk_starts.ensure(8));
+    CK(cudaMemsetAsync(ctx->walk_starts.p, 0, 8, ctx->st));
     if (pl) CKS(pl->setup(ctx, NT, feat_cap, SC, p.search_range, (int)p.memory, *reset));
     // finalize scratch for frames with more detections than shared memory sorts
     size_t fin_per_frame = 0;
@@ -1047,6 +1063,17 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     lc.snr = c.snr;
     lc.rough = c.rough;
 
+    // learned proposals: the network runs on groups of cnn_g frames whose
+    // activations (64 B per 4x4 cell) stay small enough to live in L2
+    const int Hc = (H + 3) / 4, Wc = (W + 3) / 4;
+    const size_t cells = (size_t)Hc * Wc;
+    const int cnn_g = net ? (int)std::max<size_t>(1, std::min<size_t>((size_t)F, (40u << 20) / (cells * 64))) : 0;
+    if (net) {
+        CK(ctx->cnn_x.ensure((size_t)cnn_g * cells * 32));
+        CK(ctx->cnn_p.ensure((size_t)cnn_g * cells * 64));
+        CK(ctx->cnn_q.ensure((size_t)cnn_g * cells * 64));
+        CK(ctx->cnn_head.ensure((size_t)cnn_g * cells * 16));
+    }
     const size_t super_bytes = (size_t)SC * npx * sizeof(T);
     if (!on_device) {
         CK(ctx->stage[0].ensure(super_bytes));
@@ -1100,6 +1127,36 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                                            ctx->std_scratch.as<float>(), ctx->st));
                 }
                 CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)nf * nslots * 4, ctx->st));
+                if (net) {
+                    // seeds from the network, then the walk on per-seed patches
+                    {
+                        Prof pf(ctx, "proposal_net");
+                        const CnnNet nv = net->views();
+                        for (int g0 = 0; g0 < nf; g0 += cnn_g) {
+                            const int ng = std::min(cnn_g, nf - g0);
+                            CK(cnn_input<TS>(src + (size_t)g0 * npx, (int64_t)npx, H, W, nullptr, ng, Hc, Wc,
+                                             net->mean, net->scale, ctx->cnn_x.as<__nv_bfloat16>(), ctx->st));
+                            CK(cnn_forward(nv, ctx->cnn_x.as<__nv_bfloat16>(), ng, Hc, Wc,
+                                           ctx->cnn_p.as<__nv_bfloat16>(), ctx->cnn_q.as<__nv_bfloat16>(),
+                                           ctx->cnn_p.as<__nv_bfloat16>(), ctx->cnn_head.as<float4>(), flags,
+                                           ctx->num_sms, ctx->st));
+                            CK(cnn_proposals(ctx->cnn_head.as<float4>(), ng, Hc, Wc, H, W, c.margin, net->threshold,
+                                             ctx->cand_count.as<uint32_t>() + g0,
+                                             ctx->cand_keys.as<uint32_t>() + (size_t)g0 * cand_cap, cand_cap, flags,
+                                             ctx->st));
+                        }
+                    }
+                    sum_counts_kernel<<<1, 256, 0, ctx->st>>>(ctx->cand_count.as<uint32_t>(), nf, cand_cap,
+                                                              ctx->walk_starts.as<unsigned long long>());
+                    CK(cudaGetLastError());
+                    Prof pf(ctx, "walk_local");
+                    CK(launch_walk_local<TS>(src, (int64_t)npx, c, nf, ctx->cand_count.as<uint32_t>(),
+                                             ctx->cand_keys.as<uint32_t>(), cand_cap, ctx->tabs_i.as<int32_t>(),
+                                             ctx->tabs_f.as<float2>(),
+                                             ctx->feats_raw.as<Feature>() + (size_t)c0f * feat_cap,
+                                             ctx->feat_count.as<uint32_t>() + c0f, feat_cap, flags, ctx->st));
+                    return GT_OK;
+                }
                 if (!log_style) {
                     Prof pf(ctx, "bandpass_localmax");
                     CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, true, ctx->cand_count.as<uint32_t>(),
@@ -1122,6 +1179,9 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                                                ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
                     }
                 }
+                sum_counts_kernel<<<1, 256, 0, ctx->st>>>(ctx->cand_count.as<uint32_t>(), nf * nslots, cand_cap,
+                                                          ctx->walk_starts.as<unsigned long long>());
+                CK(cudaGetLastError());
                 {
                     Prof pf(ctx, "walk_characterize");
                     CK(launch_walk<TS>(proc, src, (int64_t)npx, c, nf, nslots, ctx->cand_count.as<uint32_t>(),
@@ -1188,7 +1248,10 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         ctx->done = s0 + ns;
     }
     CK(cudaMemcpyAsync(out_flags, flags, 4, cudaMemcpyDeviceToHost, ctx->st));
+    unsigned long long starts = 0;
+    CK(cudaMemcpyAsync(&starts, ctx->walk_starts.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    ctx->last_walk_starts = (int64_t)starts;
     drain_profile(ctx, false);
     return GT_OK;
 }
@@ -1236,10 +1299,17 @@ gt_status assemble_table(gt_ctx* ctx, int64_t NT, const std::vector<int64_t>& fr
 template <typename T>
 gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_device, int64_t NT, int32_t H,
                      int32_t W, const int64_t* frame_numbers, const int64_t* reset_points, int64_t n_reset,
-                     gt_table* tab) {
+                     gt_table* tab, const gt_proposal* net = nullptr) {
     LocateConsts c;
     CKS(make_locate_consts(ctx, p, H, W, c));
     set_fast_div<T>(ctx, c);
+    if (net) {
+        const int ri = (c.circle - 1) / 2;
+        if (ri < 2 || ri > 7)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "learned proposals need a diameter between 5 and 16");
+        if (walk_local_smem_bytes(c.circle, c.R) > 227 * 1024)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size too large for the seed-patch walk");
+    }
     if (p.has_illumination_sigma) {
         // the locate stages see the corrected f32 frames
         c.fast_div = 0;
@@ -1294,10 +1364,16 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         // detections sort in shared memory (the group sort's limit)
         windowed = p.has_search_range && ctx->feat_cap <= 4096u;
         gt_status st = locate_pass<T>(ctx, p, frames, on_device, NT, H, W, c, log_style ? &lt : nullptr, F, &fl,
-                                      windowed ? &pl : nullptr, &reset);
+                                      windowed ? &pl : nullptr, &reset, net);
         if (st != GT_OK) {
             cudaStreamSynchronize(ctx->lk);
             return st;
+        }
+        if (fl & (kFlagTensorTimeout | kFlagLocalWalk)) {
+            cudaStreamSynchronize(ctx->lk);
+            return set_err(ctx, GT_ERR_INTERNAL,
+                           (fl & kFlagTensorTimeout) ? "a tensor-core kernel timed out waiting for its UMMAs"
+                                                     : "a learned seed's walk did not finish");
         }
         if (!(fl & (kFlagCandOverflow | kFlagFeatOverflow))) break;
         CK(cudaStreamSynchronize(ctx->lk));
@@ -1783,6 +1859,7 @@ gt_status gt_create(int32_t device, gt_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return GT_ERR_NO_DEVICE;
     gt_ctx* ctx = new gt_ctx();
     ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->lk, cudaStreamNonBlocking, link_stream_priority()) != cudaSuccess ||
@@ -1903,6 +1980,46 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
     *out = tab.release();
     return GT_OK;
 }
+
+gt_status gt_batch_learned(gt_ctx* ctx, const gt_params* params, const gt_proposal* net, const void* frames,
+                           int32_t dtype, int64_t T, int32_t H, int32_t W, const int64_t* frame_numbers,
+                           const int64_t* linker_reset_points, int64_t n_reset, gt_table** out) {
+    if (!out || !net) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    CKS(validate(ctx, params, frames, dtype, T, H, W));
+    if (net->device != ctx->device)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "the network lives on device %d, the context on %d", net->device,
+                       ctx->device);
+    if (params->style != GT_STYLE_TRACKPY)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "learned proposals replace the trackpy-style local maxima");
+    if (params->has_snr || params->has_minmass_snr || params->has_adaptive_background ||
+        params->has_illumination_sigma)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                       "snr, minmass_snr, adaptive_background and illumination correction are not supported with "
+                       "learned proposals");
+    bool on_device = false;
+    CKS(check_frames_ptr(ctx, frames, &on_device));
+    std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
+    gt_status st;
+    if (dtype == GT_DTYPE_U16)
+        st = batch_impl<uint16_t>(ctx, *params, (const uint16_t*)frames, on_device, T, H, W, frame_numbers,
+                                  linker_reset_points, n_reset, tab.get(), net);
+    else if (dtype == GT_DTYPE_F32)
+        st = batch_impl<float>(ctx, *params, (const float*)frames, on_device, T, H, W, frame_numbers,
+                               linker_reset_points, n_reset, tab.get(), net);
+    else
+        st = batch_impl<uint8_t>(ctx, *params, (const uint8_t*)frames, on_device, T, H, W, frame_numbers,
+                                 linker_reset_points, n_reset, tab.get(), net);
+    if (st != GT_OK) {
+        cudaStreamSynchronize(ctx->st);
+        cudaStreamSynchronize(ctx->lk);
+        return st;
+    }
+    *out = tab.release();
+    return GT_OK;
+}
+
+int64_t gt_last_walk_starts(const gt_ctx* ctx) { return ctx ? ctx->last_walk_starts : 0; }
 
 gt_status gt_batch_videos(gt_ctx* ctx, const gt_params* params, int32_t n_videos, const void* const* frames,
                           int32_t dtype, const int64_t* T, const int32_t* H, const int32_t* W, gt_table** out) {

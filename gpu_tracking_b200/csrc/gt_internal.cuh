@@ -33,6 +33,8 @@ enum : uint32_t {
     kFlagScratch = 16u,
     kFlagListOverflow = 32u,   // windowed linking: a neighbour list buffer is full
     kFlagEdgeOverflow = 64u,   // windowed linking: a frame has more edges than the scratch holds
+    kFlagTensorTimeout = 128u,  // a tensor-core kernel gave up waiting for its UMMAs
+    kFlagLocalWalk = 256u,      // a learned seed did not finish its walk in the rounds allowed
 };
 // Linker flags after which the remaining frames of a video are not linked.
 constexpr uint32_t kLinkStopFlags = 4u | 8u | 16u | 32u | 64u;

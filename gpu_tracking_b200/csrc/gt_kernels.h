@@ -1,6 +1,7 @@
 // gt_kernels.h — host-visible launch interface of the engine's kernels.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,6 +40,58 @@ struct LogConsts {
     const float* frame_std;  // per-frame std of the chunk (nullptr: use thr)
     float snr, rough;
 };
+
+// ---- learned proposal network (gt_cnn.cu): 4 layers of 3x3 convolutions
+// over 4x4-pixel cells; layer l maps kCnnCin[l] to kCnnCout[l] channels.
+constexpr int kCnnLayers = 4;
+constexpr int kCnnCin[kCnnLayers] = {16, 32, 32, 32};
+constexpr int kCnnCout[kCnnLayers] = {32, 32, 32, 3};
+constexpr int kCnnParams = 32 * 16 * 9 + 32 + 2 * (32 * 32 * 9 + 32) + 3 * 32 * 9 + 3;
+constexpr int cnn_layer_offset(int l) {
+    return l == 0 ? 0 : cnn_layer_offset(l - 1) + kCnnCout[l - 1] * kCnnCin[l - 1] * 9 + kCnnCout[l - 1];
+}
+// Device views of one network: packed BF16 UMMA operands of the forward
+// convolutions (wf) and of the input-gradient convolutions (wd, layers 1-3),
+// fp32 biases.
+struct CnnNet {
+    const uint8_t* wf[kCnnLayers];
+    const uint8_t* wd[kCnnLayers];
+    const float* bias[kCnnLayers];
+};
+size_t cnn_packed_bytes(int layer, bool backward);
+cudaError_t cnn_pack(const float* W, int layer, bool backward, __nv_bfloat16* dst, cudaStream_t st);
+template <typename T>
+cudaError_t cnn_input(const T* frames, int64_t frame_stride, int H, int W, const int4* crops, int nimg, int Hc,
+                      int Wc, float mean, float scale, __nv_bfloat16* out, cudaStream_t st);
+cudaError_t cnn_forward(const CnnNet& net, const __nv_bfloat16* x, int nimg, int Hc, int Wc, __nv_bfloat16* a1,
+                        __nv_bfloat16* a2, __nv_bfloat16* a3, float4* head, uint32_t* flags, int num_sms,
+                        cudaStream_t st);
+cudaError_t cnn_backward_input(const CnnNet& net, int layer, const __nv_bfloat16* gout, const __nv_bfloat16* act_below,
+                               int nimg, int Hc, int Wc, __nv_bfloat16* gin, uint32_t* flags, int num_sms,
+                               cudaStream_t st);
+size_t cnn_wgrad_partial_floats(int nblocks);
+cudaError_t cnn_wgrad(int layer, const __nv_bfloat16* X, const __nv_bfloat16* G, int nimg, int Hc, int Wc,
+                      float* partial, int nblocks, float* grad, cudaStream_t st);
+cudaError_t cnn_labels(const int32_t* lf, const float* ly, const float* lx, int64_t n, int T, int Hc, int Wc,
+                       int32_t* owner, float4* tmap, cudaStream_t st);
+cudaError_t cnn_crops(uint32_t seed, uint32_t step, int nimg, int T, int Hc, int Wc, int CH, int CW, int4* crops,
+                      cudaStream_t st);
+cudaError_t cnn_loss(const float4* head, const float4* tmap, const int4* crops, int nimg, int CH, int CW, int Hc_f,
+                     int Wc_f, float pos_weight, float lambda, __nv_bfloat16* grad, float* partial, int* nblocks,
+                     cudaStream_t st);
+cudaError_t cnn_adam(float* p, float* m, float* v, const float* g, int n, float lr_t, float b1, float b2, float eps,
+                     cudaStream_t st);
+cudaError_t cnn_loss_sum(const float* partial, int nblocks, float inv, float* out, cudaStream_t st);
+cudaError_t cnn_proposals(const float4* head, int nimg, int Hc, int Wc, int H, int W, int margin, float thr,
+                          uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags,
+                          cudaStream_t st);
+// walk + characterize from seeds with the processed image built per seed
+size_t walk_local_smem_bytes(int circle, int R);
+template <typename T>
+cudaError_t launch_walk_local(const T* frames, int64_t frame_stride, const LocateConsts& c, int nframes,
+                              const uint32_t* cand_count, const uint32_t* cand_keys, uint32_t cand_cap,
+                              const int32_t* angle_off, const float2* angles, Feature* feats, uint32_t* feat_count,
+                              uint32_t feat_cap, uint32_t* flags, cudaStream_t st);
 
 // Per-frame std (snr / minmass_snr), the reference's reduction tree.
 bool std_reduction_exact(int64_t N);

@@ -502,6 +502,320 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
     else atomicOr(flags, kFlagFeatOverflow);
 }
 
+// ------------------------------------------------ walk from learned seeds
+// Seeds proposed by the learned network come without a processed image.
+// Each warp takes 32 seeds and builds, for each, a PS x PS patch of processed
+// values around it: the bandpass of preprocess_rows.wgsl / preprocess_cols.wgsl
+// evaluated with the operation order of bandpass_kernel (clamped raw rows and
+// columns, Gaussian taps skipped outside the frame, sequential sums, IEEE
+// division), so every value equals the full-frame one bit for bit.  Each lane
+// then moves its seed to the largest processed value of the 3x3 block around
+// it (inside the candidate margin; the seed itself wins ties, then row-major
+// order) -- a bandpass local maximum, the kind of pixel the plain method
+// starts its walks from -- and walks and characterizes from there with the
+// operation sequence of walk_kernel_fixed, reading its patch.  A lane whose
+// walk or characterize circle leaves the patch asks for a patch centred
+// where it stands and resumes there.
+constexpr int kLwWarps = 4;
+constexpr int kLwShift = 1;   // walk steps a patch covers around its centre
+
+__host__ __device__ constexpr int lw_patch(int RI) { return 2 * (RI + kLwShift) + 1; }
+__host__ __device__ constexpr int lw_warp_floats(int RI, int R) {
+    return 32 * lw_patch(RI) * lw_patch(RI) + (lw_patch(RI) + 2 * R) * (lw_patch(RI) + 2 * R) +
+           2 * (lw_patch(RI) + 2 * R) * lw_patch(RI);
+}
+
+template <typename T, int RI>
+__device__ void lw_build_patch(const T* __restrict__ img, const LocateConsts& c, int cu, int cv, float* patch,
+                               float* raw, float* xg, float* xb, int lane) {
+    constexpr int PS = lw_patch(RI);
+    const int H = c.H, W = c.W, R = c.R, RW = PS + 2 * R;
+    const int r0 = cu - RI - kLwShift, c0 = cv - RI - kLwShift;  // patch origin
+    const int br = r0 - R, bc = c0 - R;                          // raw origin
+    for (int idx = lane; idx < RW * RW; idx += 32) {
+        const int rr = idx / RW, cc = idx - rr * RW;
+        const int gr = min(max(br + rr, 0), H - 1), gc = min(max(bc + cc, 0), W - 1);
+        raw[idx] = load_px<T>(img, (size_t)gr * W + gc);
+    }
+    __syncwarp();
+    for (int idx = lane; idx < RW * PS; idx += 32) {
+        const int rr = idx / PS, pc = idx - rr * PS;
+        const float* rowp = raw + rr * RW + pc;
+        const int gcol = c0 + pc;
+        float gs = 0.0f, cs = 0.0f;
+        for (int i = 0; i <= 2 * R; i++) {
+            const float x = rowp[i];
+            const int gc = gcol + i - R;
+            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
+            cs = __fadd_rn(cs, x);
+        }
+        xg[idx] = __fdiv_rn(gs, c.gnorm);
+        xb[idx] = cs;
+    }
+    __syncwarp();
+    const float trunc_thr = 1.0f / 255.0f;
+    for (int idx = lane; idx < PS * PS; idx += 32) {
+        const int pr = idx / PS, pc = idx - pr * PS;
+        const int grow = r0 + pr, gcol = c0 + pc;
+        float res = 0.0f;
+        if (grow >= 0 && grow < H && gcol >= 0 && gcol < W) {
+            // raw row (pr + i) holds row clamp(grow + i - R): the row pass of a
+            // clamped row is the row pass of the edge row
+            float gs = 0.0f, cs = 0.0f;
+            for (int i = 0; i <= 2 * R; i++) {
+                const int gr = grow + i - R;
+                const int xr = (pr + i) * PS + pc;
+                if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], xg[xr], gs);
+                cs = __fadd_rn(cs, xb[xr]);
+            }
+            res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
+            if (c.truncate && res < trunc_thr) res = 0.0f;
+        }
+        patch[idx] = res;
+    }
+    __syncwarp();
+}
+
+// One processed value computed on its own (the same sequence as the patch).
+template <typename T>
+__device__ float lw_processed_at(const T* __restrict__ img, const LocateConsts& c, int u, int v) {
+    const int H = c.H, W = c.W, R = c.R;
+    float gs = 0.0f, cs = 0.0f;
+    for (int i = 0; i <= 2 * R; i++) {
+        const int gr = u + i - R;
+        const int row = min(max(gr, 0), H - 1);
+        float rg = 0.0f, rb = 0.0f;
+        for (int j = 0; j <= 2 * R; j++) {
+            const int gc = v + j - R;
+            const float x = load_px<T>(img, (size_t)row * W + min(max(gc, 0), W - 1));
+            if (gc >= 0 && gc < W) rg = __fmaf_rn(c.taps[j], x, rg);
+            rb = __fadd_rn(rb, x);
+        }
+        if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], __fdiv_rn(rg, c.gnorm), gs);
+        cs = __fadd_rn(cs, rb);
+    }
+    float res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
+    if (c.truncate && res < 1.0f / 255.0f) res = 0.0f;
+    return res;
+}
+
+// get_center_fixed over a patch: `pc` points at (u, v), rows `stride` apart.
+template <int RI, bool CHECK>
+__device__ __forceinline__ WalkRes lw_get_center(const float* pc, int stride, int H, int W, int u, int v) {
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int i = -RI; i <= RI; i++) {
+        const float* prow = pc + i * stride;
+        const bool row_in = !CHECK || (u + i >= 0 && u + i < H);
+#pragma unroll
+        for (int j = -RI; j <= RI; j++) {
+            if (i * i + j * j > RI * RI) continue;
+            if (CHECK && (!row_in || v + j < 0 || v + j >= W)) continue;
+            const float data = prow[j];
+            res.x = __fmaf_rn(data, (float)i, res.x);
+            res.y = __fmaf_rn(data, (float)j, res.y);
+            res.mass = __fadd_rn(res.mass, data);
+            res.count = __fadd_rn(res.count, 1.0f);
+            res.max = wgsl_max(res.max, data);
+        }
+    }
+    res.x = __fdiv_rn(res.x, res.mass);
+    res.y = __fdiv_rn(res.y, res.mass);
+    return res;
+}
+
+// characterize_fixed_at with the processed values from a patch.
+template <typename T, int RI, bool CHECK>
+__device__ __forceinline__ void lw_characterize(const float* pc, int stride, const T* __restrict__ raw, int H, int W,
+                                                int u, int v, const float2* __restrict__ angles, float* Rg_,
+                                                float* raw_mass_, float* signal_, float* es_, float* ec_) {
+    constexpr int side = 2 * RI + 1;
+    float Rg = 0.0f, raw_mass = 0.0f, signal = 0.0f, es = 0.0f, ec = 0.0f;
+#pragma unroll
+    for (int i = -RI; i <= RI; i++) {
+        const bool row_in = !CHECK || (u + i >= 0 && u + i < H);
+#pragma unroll
+        for (int j = -RI; j <= RI; j++) {
+            if (i * i + j * j > RI * RI) continue;
+            if (CHECK && (!row_in || v + j < 0 || v + j >= W)) continue;
+            const float data = pc[i * stride + j];
+            Rg = __fmaf_rn(data, (float)(i * i + j * j), Rg);
+            raw_mass = __fadd_rn(raw_mass, load_px<T>(raw, (size_t)(u + i) * W + (v + j)));
+            signal = wgsl_max(signal, data);
+            if ((i != 0) | (j != 0)) {
+                const float2 sc = __ldg(angles + (i + RI) * side + (j + RI));
+                es = __fmaf_rn(data, sc.x, es);
+                ec = __fmaf_rn(data, sc.y, ec);
+            } else {
+                ec = __fadd_rn(ec, data);
+            }
+        }
+    }
+    *Rg_ = Rg;
+    *raw_mass_ = raw_mass;
+    *signal_ = signal;
+    *es_ = es;
+    *ec_ = ec;
+}
+
+template <typename T, int RI>
+__global__ void __launch_bounds__(32 * kLwWarps)
+walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const LocateConsts c,
+                  const uint32_t* __restrict__ cand_count, const uint32_t* __restrict__ cand_keys, uint32_t cand_cap,
+                  const int32_t* __restrict__ angle_off, const float2* __restrict__ angles,
+                  Feature* __restrict__ feats, uint32_t* __restrict__ feat_count, uint32_t feat_cap,
+                  uint32_t* __restrict__ flags) {
+    extern __shared__ float lsm[];
+    constexpr int PS = lw_patch(RI);
+    constexpr int OFF = RI + kLwShift;
+    const int R = c.R, RW = PS + 2 * R;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int f = blockIdx.y;
+    const uint32_t n = min(cand_count[f], cand_cap);
+    const uint32_t first = (blockIdx.x * kLwWarps + warp) * 32u;
+    if (first >= n) return;  // warp-uniform
+    float* wbase = lsm + (size_t)warp * lw_warp_floats(RI, R);
+    float* patches = wbase;
+    float* raw = wbase + 32 * PS * PS;
+    float* xg = raw + RW * RW;
+    float* xb = xg + RW * PS;
+    float* my = patches + lane * PS * PS;
+    const int H = c.H, W = c.W;
+    const T* img = frames + (size_t)f * frame_stride;
+    const uint32_t i = first + lane;
+    const bool active = i < n;
+    const uint32_t key = active ? cand_keys[(size_t)f * cand_cap + i] : 0u;
+    int pu = (int)(key / (uint32_t)W), pv = (int)(key % (uint32_t)W);
+    int stage = active ? 0 : 2;  // 0 walk, 1 characterize, 2 done
+    uint32_t it = 0;
+    WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float fx = 0.0f, fy = 0.0f;
+    bool need = active, snapped = false;
+    int want_u = pu, want_v = pv, cen_u = pu, cen_v = pv;
+    const float thr = c.shift_thr;
+    for (int round = 0; round < (int)c.max_iter + 4; round++) {
+        const unsigned needmask = __ballot_sync(0xffffffffu, need);
+        if (needmask == 0u && !__any_sync(0xffffffffu, stage != 2)) break;
+        for (unsigned m = needmask; m; m &= m - 1u) {
+            const int k = __ffs(m) - 1;
+            const int cu = __shfl_sync(0xffffffffu, want_u, k), cv = __shfl_sync(0xffffffffu, want_v, k);
+            lw_build_patch<T, RI>(img, c, cu, cv, patches + k * PS * PS, raw, xg, xb, lane);
+        }
+        if (need) {
+            cen_u = want_u;
+            cen_v = want_v;
+            need = false;
+        }
+        if (stage == 0 && !need && it == 0 && pu == cen_u && pv == cen_v && !snapped) {
+            snapped = true;
+            const float* pc = my + OFF * PS + OFF;
+            float best = pc[0];
+            int bu = 0, bv = 0;
+            for (int di = -1; di <= 1; di++)
+                for (int dj = -1; dj <= 1; dj++) {
+                    const int u = pu + di, v = pv + dj;
+                    if (u < c.margin || u >= H - c.margin || v < c.margin || v >= W - c.margin) continue;
+                    const float val = pc[di * PS + dj];
+                    if (val > best) {
+                        best = val;
+                        bu = di;
+                        bv = dj;
+                    }
+                }
+            pu += bu;
+            pv += bv;
+        }
+        if (stage == 0) {
+            bool fin = false;
+            for (;;) {
+                if (it >= c.max_iter) {
+                    fin = true;
+                    break;
+                }
+                if (abs(pu - cen_u) > kLwShift || abs(pv - cen_v) > kLwShift) {
+                    need = true;
+                    want_u = pu;
+                    want_v = pv;
+                    break;
+                }
+                const float* pc = my + (pu - cen_u + OFF) * PS + (pv - cen_v + OFF);
+                if (pu >= RI && pu + RI < H && pv >= RI && pv + RI < W)
+                    res = lw_get_center<RI, false>(pc, PS, H, W, pu, pv);
+                else
+                    res = lw_get_center<RI, true>(pc, PS, H, W, pu, pv);
+                it++;
+                bool changed = false;
+                if ((res.x > thr) && (pu < H - 1 - RI)) { pu += 1; changed = true; }
+                else if (res.x < -thr && pu > RI) { pu -= 1; changed = true; }
+                if ((res.y > thr) && (pv < W - 1 - RI)) { pv += 1; changed = true; }
+                else if ((res.y < -thr) && (pv > RI)) { pv -= 1; changed = true; }
+                if (!changed) {
+                    fin = true;
+                    break;
+                }
+            }
+            if (fin) {
+                fx = __fadd_rn(res.x, (float)pu);
+                fy = __fadd_rn(res.y, (float)pv);
+                float minmass;
+                if (c.minmass > 0.0f) minmass = c.minmass;
+                else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.image_std), c.rough);
+                // a seed in an empty region (mass 0) proposes nothing
+                stage = (res.mass >= minmass && res.mass > 0.0f) ? 1 : 2;
+            }
+        }
+        if (stage == 1 && !need) {
+            const int cu = sat_f2i(rintf(fx)), cv = sat_f2i(rintf(fy));
+            if (abs(cu - cen_u) > kLwShift || abs(cv - cen_v) > kLwShift) {
+                need = true;
+                want_u = cu;
+                want_v = cv;
+            } else {
+                Feature ft;
+                ft.key_hi = 0;
+                ft.key_lo = key;
+                ft.x = fx;
+                ft.y = fy;
+                ft.mass = res.mass;
+                ft.r = 0.0f;
+                ft.max_i = res.max;
+                ft.count = res.count;
+                ft.Rg = ft.raw = ft.signal = ft.ecc = 0.0f;
+                ft.d_raw = ft.d_bg = ft.d_corr = __int_as_float(0x7fc00000);
+                ft.ridx = 0;
+                if (c.characterize) {
+                    const float2* ang = angles + angle_off[RI];
+                    const float* pc = my + (cu - cen_u + OFF) * PS + (cv - cen_v + OFF);
+                    float middle = 0.0f;
+                    const int64_t middle_idx = (int64_t)cu * W + cv;
+                    if (middle_idx >= 0 && middle_idx < (int64_t)H * W) {
+                        if (cu >= 0 && cu < H && cv >= 0 && cv < W) middle = *pc;
+                        else middle = lw_processed_at<T>(img, c, (int)(middle_idx / W), (int)(middle_idx % W));
+                    }
+                    float Rg, raw_mass, signal, es, ec;
+                    if (cu >= RI && cu + RI < H && cv >= RI && cv + RI < W)
+                        lw_characterize<T, RI, false>(pc, PS, img, H, W, cu, cv, ang, &Rg, &raw_mass, &signal, &es,
+                                                      &ec);
+                    else
+                        lw_characterize<T, RI, true>(pc, PS, img, H, W, cu, cv, ang, &Rg, &raw_mass, &signal, &es,
+                                                     &ec);
+                    es = __fmul_rn(es, es);
+                    ec = __fmul_rn(ec, ec);
+                    ft.ecc = __fdiv_rn(__fsqrt_rn(__fadd_rn(es, ec)), __fsub_rn(ft.mass, middle));
+                    ft.Rg = __fsqrt_rn(__fdiv_rn(Rg, ft.mass));
+                    ft.raw = raw_mass;
+                    ft.signal = signal;
+                }
+                const uint32_t pos = atomicAdd(feat_count + f, 1u);
+                if (pos < feat_cap) feats[(size_t)f * feat_cap + pos] = ft;
+                else atomicOr(flags, kFlagFeatOverflow);
+                stage = 2;
+            }
+        }
+    }
+    if (stage != 2) atomicOr(flags, kFlagLocalWalk);
+}
+
 // characterize_points: characterize.wgsl with _feat_characterize_points (mass
 // recomputed at the rounded position); one thread per given point.
 template <typename T>
@@ -993,6 +1307,33 @@ cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_s
     return cudaGetLastError();
 }
 
+size_t walk_local_smem_bytes(int circle, int R) {
+    const int ri = (circle - 1) / 2;
+    return (size_t)kLwWarps * lw_warp_floats(ri, R) * sizeof(float);
+}
+
+template <typename T>
+cudaError_t launch_walk_local(const T* frames, int64_t frame_stride, const LocateConsts& c, int nframes,
+                              const uint32_t* cand_count, const uint32_t* cand_keys, uint32_t cand_cap,
+                              const int32_t* angle_off, const float2* angles, Feature* feats, uint32_t* feat_count,
+                              uint32_t feat_cap, uint32_t* flags, cudaStream_t st) {
+    if (cand_cap == 0 || nframes == 0) return cudaSuccess;
+    const int ri = (c.circle - 1) / 2;
+    const size_t smem = walk_local_smem_bytes(c.circle, c.R);
+    dim3 grid((cand_cap + 32 * kLwWarps - 1) / (32 * kLwWarps), nframes);
+#define GT_WALK_LOCAL(RI)                                                                                        \
+    if (ri == RI) {                                                                                              \
+        cudaFuncSetAttribute(walk_local_kernel<T, RI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        walk_local_kernel<T, RI><<<grid, 32 * kLwWarps, smem, st>>>(frames, frame_stride, c, cand_count,         \
+                                                                    cand_keys, cand_cap, angle_off, angles,      \
+                                                                    feats, feat_count, feat_cap, flags);          \
+        return cudaGetLastError();                                                                               \
+    }
+    GT_WALK_LOCAL(2) GT_WALK_LOCAL(3) GT_WALK_LOCAL(4) GT_WALK_LOCAL(5) GT_WALK_LOCAL(6) GT_WALK_LOCAL(7)
+#undef GT_WALK_LOCAL
+    return cudaErrorInvalidValue;
+}
+
 template <typename T>
 cudaError_t launch_characterize_points(const float* processed, const T* frames, int64_t frame_stride,
                                        const LocateConsts& c, const float* pts, const int64_t* grp_off,
@@ -1042,6 +1383,9 @@ cudaError_t launch_scatter(const Feature* feats, uint32_t feat_cap, const uint32
                                         const uint32_t*, const uint32_t*, uint32_t, uint32_t, const float*,      \
                                         const int32_t*, const float2*, Feature*, uint32_t*, uint32_t, uint32_t*, \
                                         cudaStream_t);                                                           \
+    template cudaError_t launch_walk_local<T>(const T*, int64_t, const LocateConsts&, int, const uint32_t*,     \
+                                              const uint32_t*, uint32_t, const int32_t*, const float2*, Feature*, \
+                                              uint32_t*, uint32_t, uint32_t*, cudaStream_t);                     \
     template cudaError_t launch_characterize_points<T>(const float*, const T*, int64_t, const LocateConsts&,     \
                                                        const float*, const int64_t*, const int32_t*, int32_t,     \
                                                        int, int64_t, const float2*, const int32_t*, int32_t,      \

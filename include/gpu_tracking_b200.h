@@ -227,6 +227,60 @@ GT_API gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype,
 GT_API gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_frame_y_x, int64_t n, float search_range,
                                  uint32_t memory, int64_t* d_particle_out);
 
+/* ------------------------------------------------- learned proposals
+ * No counterpart in the reference.  A small BF16 network (4 layers of 3x3
+ * convolutions, 32 channels, over 4x4-pixel cells) proposes walk seeds in
+ * place of the bandpass local maxima; the walk, characterization,
+ * filter_close, doughnut correction and linking are the plain method's.  It
+ * is trained on the plain method's own detections.
+ */
+typedef struct gt_proposal gt_proposal;
+
+typedef struct gt_train_opts {
+    int32_t steps;        /* optimizer steps */
+    int32_t batch;        /* crops per step */
+    int32_t crop;         /* crop side in pixels, a multiple of 4 */
+    float lr;             /* Adam step size, cosine-decayed to lr / 20 over the steps */
+    float pos_weight;     /* weight of the labelled cells in the score loss */
+    float offset_weight;  /* weight of the squared offset error at labelled cells */
+    uint32_t seed;        /* crop sampling */
+} gt_train_opts;
+
+GT_API void gt_train_opts_default(gt_train_opts* o);
+/* Number of fp32 parameters (layer by layer: W[co][ci][ky*3+kx], then b[co]). */
+GT_API int64_t gt_proposal_num_params(void);
+/* A network with seeded He-normal weights. */
+GT_API gt_status gt_proposal_create(gt_ctx* ctx, uint64_t seed, gt_proposal** out);
+GT_API void gt_proposal_destroy(gt_proposal* p);
+/* Set (params may be NULL to keep them) or read the parameters, the input
+ * normalisation (pixel - mean) * scale and the score-logit threshold. */
+GT_API gt_status gt_proposal_set(gt_ctx* ctx, gt_proposal* p, const float* params, float mean, float scale,
+                                 float threshold);
+GT_API gt_status gt_proposal_get(gt_ctx* ctx, const gt_proposal* p, float* params, float* mean, float* scale,
+                                 float* threshold);
+/* Train on crops of the frames (host or device memory) labelled by the
+ * detections (label_frame indexes 0..T-1, label_y / label_x in pixels).
+ * loss_out (nullable, 2 * steps floats) receives the score and offset loss
+ * of every step. */
+GT_API gt_status gt_proposal_train(gt_ctx* ctx, gt_proposal* p, const void* frames, int32_t dtype, int64_t T,
+                                   int32_t H, int32_t W, const int64_t* label_frame, const float* label_y,
+                                   const float* label_x, int64_t n_labels, const gt_train_opts* opts,
+                                   float* loss_out);
+/* Network outputs of every cell: maps is (T, ceil(H/4), ceil(W/4), 4) float32
+ * holding (score logit, row offset, column offset, 0). */
+GT_API gt_status gt_proposal_maps(gt_ctx* ctx, const gt_proposal* p, const void* frames, int32_t dtype, int64_t T,
+                                  int32_t H, int32_t W, float* maps);
+/* gt_batch with the network's seeds instead of the bandpass local maxima
+ * (trackpy style; snr, minmass_snr, adaptive_background and illumination
+ * correction are not supported here). */
+GT_API gt_status gt_batch_learned(gt_ctx* ctx, const gt_params* params, const gt_proposal* p,
+                                  const void* frames, int32_t dtype, int64_t T, int32_t H, int32_t W,
+                                  const int64_t* frame_numbers, const int64_t* linker_reset_points,
+                                  int64_t n_reset, gt_table** out);
+/* Walk starts (bandpass candidates or learned seeds) of the last gt_batch /
+ * gt_batch_learned call on this context, summed over its frames. */
+GT_API int64_t gt_last_walk_starts(const gt_ctx* ctx);
+
 /* Library version string. */
 GT_API const char* gt_version(void);
 
