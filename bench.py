@@ -55,8 +55,11 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="frames in the CPU-baseline sample (0: auto)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="headline", choices=["headline", "ragged"],
-                    help="headline: the 2000-frame 2048^2 video; ragged: 64 videos of uneven size and length")
+    ap.add_argument("--workload", default="headline", choices=["headline", "ragged", "learned"],
+                    help="headline: the 2000-frame 2048^2 video; ragged: 64 videos of uneven size and length; "
+                         "learned: plain vs learned-proposal seeds on 1000 frames of 2048^2 at 4000 spots/frame")
+    ap.add_argument("--learned-scale", type=float, default=1.0, help="learned: fraction of the 1000 frames timed")
+    ap.add_argument("--epochs", type=float, default=3.0, help="learned: passes over the 200k training crops")
     ap.add_argument("--scale", type=float, default=0.25,
                     help="ragged: fraction of the configured 50-1000 frames per video")
     return ap.parse_args()
@@ -194,7 +197,7 @@ def run_reference(args):
     return 0
 
 
-RAGGED = dict(workload="64 ragged uint16 videos: sides in {256,512,1024,2048}, 50-1000 frames (x scale), "
+RAGGED = dict(workload="64 ragged uint16 videos: sides in {256,512,1024,1536,2048}, 50-1000 frames (x scale), "
                         "density 1e-4..2e-3 spots/px^2, D 0.2..2", videos=64, diameter=11, minmass=220.0,
               search_range=7.0, memory=3, seed=4)
 
@@ -206,8 +209,8 @@ def ragged_videos(scale, device):
     rng = np.random.default_rng(RAGGED["seed"])
     vids = []
     for k in range(RAGGED["videos"]):
-        H = int(rng.choice([256, 512, 1024, 2048]))
-        W = int(rng.choice([256, 512, 1024, 2048]))
+        H = int(rng.choice([256, 512, 1024, 1536, 2048]))
+        W = int(rng.choice([256, 512, 1024, 1536, 2048]))
         T = max(1, int(rng.integers(50, 1001) * scale))
         n = max(1, int(rng.uniform(1e-4, 2e-3) * H * W))
         D = float(rng.uniform(0.2, 2.0))
@@ -292,12 +295,165 @@ def run_ragged(args):
     return 0
 
 
+LEARNED = dict(workload="plain vs learned-proposal seeds: 1000 frames 2048x2048 uint16, 4000 spots/frame, SNR 2-10",
+               frames=1000, size=2048, spots_per_frame=4000, snr=[2, 10], sigma_px=[1.2, 2.5], background=100,
+               D=1.0, births_deaths=0.02, diameter=11, minmass=220.0, search_range=7.0, memory=3,
+               net="4 x conv3x3 over 4x4-pixel cells: 16-32-32-32-3 channels, 24003 parameters, BF16/FP32 accumulate",
+               train="200k crops of 128x128 (782 steps of 256 per epoch) from 800 frames of the 2000-spot SNR 3-20 "
+                     "generator, labelled by the plain method's detections",
+               calibration="8 held-out frames of the 4000-spot SNR 2-10 generator, recall target 0.997")
+
+
+def cnn_flops_per_cell():
+    """Multiply-adds x 2 of the four convolutions per 4x4-pixel cell."""
+    return 2 * 9 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 3)
+
+
+def run_learned(args):
+    """Plain and learned-seed tracking of the same device-resident video."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    import gpu_tracking_b200 as gt
+    from gpu_tracking_b200 import _ffi, learned
+    from gpu_tracking_b200._params import DTYPE_U16, trackpy_params
+    from gpu_tracking_b200.synth import brownian_video
+    torch.cuda.set_device(0)
+    cfg = LEARNED
+    S = cfg["size"]
+    T = max(4, int(cfg["frames"] * args.learned_scale))
+    epochs = args.epochs
+    gen = dict(sigma_range=tuple(cfg["sigma_px"]), bg=cfg["background"], D=cfg["D"], turnover=cfg["births_deaths"])
+
+    # training: frames of the 2000-spot generator labelled by the plain method
+    t_start = time.perf_counter()
+    train = brownian_video(800, S, S, 2000, seed=101, device="cuda:0", snr_range=(3.0, 20.0), **gen)
+    labels = gt.batch(train, cfg["diameter"], minmass=cfg["minmass"], tqdm=False)
+    net = learned.ProposalNet(seed=1)
+    net.fit_normalization(train)
+    steps = int(round(epochs * 200_000 / 256))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = net.train(train, labels, steps=steps, batch=256, crop=128, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del train, labels
+    torch.cuda.empty_cache()
+    calib = brownian_video(8, S, S, cfg["spots_per_frame"], seed=202, device="cuda:0",
+                           snr_range=tuple(cfg["snr"]), **gen)
+    thr, curve = learned.calibrate(net, calib, cfg["diameter"], recall=0.997, minmass=cfg["minmass"])
+    del calib
+    setup_s = time.perf_counter() - t_start
+
+    video = brownian_video(T, S, S, cfg["spots_per_frame"], seed=303, device="cuda:0",
+                           snr_range=tuple(cfg["snr"]), **gen)
+    torch.cuda.synchronize()
+    p = trackpy_params(cfg["diameter"], minmass=cfg["minmass"], search_range=cfg["search_range"],
+                       memory=cfg["memory"])
+    ctx = _ffi.context(0)
+    L = _ffi.lib()
+
+    def call(fn):
+        out = ctypes.c_void_p()
+        ctx.check(fn(ctypes.byref(out)))
+        n = L.gt_table_nrows(out)
+        L.gt_table_free(out)
+        return n
+
+    def plain_call(out):
+        return L.gt_batch(ctx.handle, ctypes.byref(p), ctypes.c_void_p(video.data_ptr()), DTYPE_U16, T, S, S, None,
+                          None, 0, out)
+
+    def learned_call(out):
+        return L.gt_batch_learned(ctx.handle, ctypes.byref(p), net.handle, ctypes.c_void_p(video.data_ptr()),
+                                  DTYPE_U16, T, S, S, None, None, 0, out)
+
+    def timed(fn, names):
+        for _ in range(args.warmup):
+            call(fn)
+        torch.cuda.synchronize()
+        starts = L.gt_last_walk_starts(ctx.handle)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        rows = 0
+        for _ in range(args.steps):
+            rows += call(fn)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        # kernel times from one more, profiled call
+        ctx.profile(True)
+        l0 = ctx.launch_count()
+        call(fn)
+        launches = ctx.launch_count() - l0
+        kern = {}
+        for k in names:
+            n, kms = ctx.profile_read(k)
+            if n:
+                kern[k] = {"launches": n, "ms": kms}
+        ctx.profile(False)
+        return ms, rows / args.steps, starts, kern, launches
+
+    common = ("finalize", "scatter", "link_video", "link_lists", "link_sort", "link_rows")
+    clocks = Clocks(0)
+    clocks.start()
+    ms_p, rows_p, starts_p, kern_p, launches_p = timed(plain_call, ("bandpass_localmax", "walk_characterize") + common)
+    ms_l, rows_l, starts_l, kern_l, launches_l = timed(learned_call, ("proposal_net", "walk_local") + common)
+    clk = clocks.stop()
+    kw = dict(minmass=cfg["minmass"], search_range=cfg["search_range"], memory=cfg["memory"], tqdm=False)
+    score = learned.compare(gt.batch(video, cfg["diameter"], **kw),
+                            learned.batch_learned(video, cfg["diameter"], net, **kw))
+
+    pk = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+    except Exception:
+        pass
+    tc_peak = float(pk.get("bf16_tflops", 1590.0))
+    net_ms = kern_l.get("proposal_net", {}).get("ms")
+    flops = cnn_flops_per_cell() * ((S + 3) // 4) ** 2 * T
+    tensor = None
+    if net_ms:
+        achieved = flops / (net_ms / 1000.0) / 1e12
+        tensor = {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
+                  "frac": achieved / tc_peak, "kernel": "proposal_net (4 conv3x3 launches per frame group)",
+                  "flops_per_frame": flops / T, "peak_kind": "measured" if pk else "fallback"}
+    hbm_peak, hbm_kind = load_peaks()
+    bytes_per_frame_p = S * S * 2 + rows_p / T * 48.0
+    bytes_per_frame_l = S * S * 2 + rows_l / T * 48.0
+    line = {"metric": METRIC, "value": T / (ms_l / 1000.0), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network, f32 walk", "data": "synthetic",
+            "config": dict(cfg, frames=T, epochs=epochs, train_steps=steps,
+                           l2="inputs (%.1f GB) larger than L2; no flush" % (T * S * S * 2 / 1e9)),
+            "features_per_s": rows_l / (ms_l / 1000.0),
+            "plain": {"value": T / (ms_p / 1000.0), "ms_per_step": ms_p, "features_per_s": rows_p / (ms_p / 1000.0),
+                      "walk_starts": int(starts_p), "kernels": kern_p, "gpu_launches": int(launches_p),
+                      "hbm_frac_whole_step": T * bytes_per_frame_p / (ms_p / 1000.0) / 1e9 / hbm_peak},
+            "learned": {"value": T / (ms_l / 1000.0), "ms_per_step": ms_l, "features_per_s": rows_l / (ms_l / 1000.0),
+                        "walk_starts": int(starts_l), "kernels": kern_l, "gpu_launches": int(launches_l),
+                        "hbm_frac_whole_step": T * bytes_per_frame_l / (ms_l / 1000.0) / 1e9 / hbm_peak,
+                        "threshold": thr, "calibration": curve},
+            "speedup_learned_over_plain": ms_p / ms_l,
+            "score_vs_plain": score,
+            "training": {"steps": steps, "seconds": train_s, "loss_first": loss[:20].mean(0).tolist(),
+                         "loss_last": loss[-20:].mean(0).tolist(), "setup_seconds": setup_s},
+            "roofline": tensor, "hbm_peak": hbm_peak, "hbm_peak_kind": hbm_kind,
+            "gpu_launches": int(launches_l), "clocks": clk}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ragged":
         return run_ragged(args)
+    if args.workload == "learned":
+        return run_learned(args)
     import ctypes
 
     import numpy as np

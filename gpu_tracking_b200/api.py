@@ -78,6 +78,9 @@ class _Frames:
             t = t[keys]
             self.frame_numbers = np.asarray(keys, np.int64)
         t = t.contiguous()
+        # the engine's streams do not wait for torch's: the tensor must be
+        # complete before its pointer is handed over
+        torch.cuda.current_stream(t.device).synchronize()
         if t.dtype == torch.uint16:
             code = DTYPE_U16
         elif t.dtype == torch.uint8:

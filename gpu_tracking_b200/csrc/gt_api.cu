@@ -1307,8 +1307,9 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         const int ri = (c.circle - 1) / 2;
         if (ri < 2 || ri > 7)
             return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "learned proposals need a diameter between 5 and 16");
-        if (walk_local_smem_bytes(c.circle, c.R) > 227 * 1024)
-            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "smoothing_size too large for the seed-patch walk");
+        if (c.R > 7 || walk_local_smem_bytes(c.circle, c.R) > 227 * 1024)
+            return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                           "learned proposals need a smoothing_size of at most 15 (the seed-patch walk)");
     }
     if (p.has_illumination_sigma) {
         // the locate stages see the corrected f32 frames

@@ -46,7 +46,7 @@ struct ConvGeom {
     static constexpr int COPY = (kConvTH + 2) * ROW;    // one dx-shifted copy (with the row halo)
     static constexpr int A_BYTES = 3 * COPY;
     static constexpr int B_BYTES = 9 * KS * (N / 8) * 256;
-    static constexpr int SMEM = 128 + A_BYTES + B_BYTES + 16;
+    static constexpr int SMEM = 128 + 2 * A_BYTES + B_BYTES + 16;  // two staging buffers
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
@@ -54,9 +54,50 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
+// Stage the input cells (y0 - 1 + r, x0 - 1 + j) of a tile into the three
+// shifted copies at A: every load of the tile is issued before the first
+// shared-memory store, so the tile costs one round trip to L2.
+template <int KS>
+__device__ __forceinline__ void conv_fill(uint8_t* A, const __nv_bfloat16* __restrict__ src, int Hc, int Wc, int y0,
+                                          int x0, int tid) {
+    using G = ConvGeom<KS, 32>;
+    constexpr int NQ = 2 * KS, NJ = kConvTW + 2;
+    constexpr int TOTAL = (kConvTH + 2) * NQ * NJ;
+    constexpr int NIT = (TOTAL + kConvThreads - 1) / kConvThreads;
+    uint4 v[NIT];
+#pragma unroll
+    for (int k = 0; k < NIT; k++) {
+        const int it = tid + k * kConvThreads;
+        v[k] = make_uint4(0u, 0u, 0u, 0u);
+        if (it < TOTAL) {
+            const int j = it % NJ, rest = it / NJ;
+            const int q = rest % NQ, r = rest / NQ;
+            const int gy = y0 - 1 + r, gx = x0 - 1 + j;
+            if (gy >= 0 && gy < Hc && gx >= 0 && gx < Wc)
+                v[k] = __ldg((const uint4*)(src + ((size_t)gy * Wc + gx) * G::CIN) + q);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NIT; k++) {
+        const int it = tid + k * kConvThreads;
+        if (it < TOTAL) {
+            const int j = it % NJ, rest = it / NJ;
+            const int q = rest % NQ, r = rest / NQ;
+#pragma unroll
+            for (int dx = 0; dx < 3; dx++) {
+                const int c = j - dx;
+                if (c >= 0 && c < kConvTW)
+                    *(uint4*)(A + dx * G::COPY + r * G::ROW + (c >> 3) * G::GROUP + q * 128 + (c & 7) * 16) = v[k];
+            }
+        }
+    }
+}
+
 // MODE 0: relu(acc + bias) -> bf16 [cell][32]
 // MODE 1: acc + bias      -> float4 [cell] (score, row offset, column offset, 0), N = 16
 // MODE 2: acc * (mask > 0) -> bf16 [cell][32] (backward through the ReLU of the layer below)
+// A CTA walks its tiles with two staging buffers: the next tile is staged
+// while the tensor cores work on the current one.
 template <int KS, int N, int MODE>
 __global__ void __launch_bounds__(kConvThreads)
 conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, const uint8_t* __restrict__ wpk,
@@ -64,8 +105,8 @@ conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, c
                uint32_t* __restrict__ flags) {
     using G = ConvGeom<KS, N>;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* A = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    uint8_t* B = A + G::A_BYTES;
+    uint8_t* A0 = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint8_t* B = A0 + 2 * G::A_BYTES;
     uint64_t* mbar = (uint64_t*)(B + G::B_BYTES);
     uint32_t* tslot = (uint32_t*)(mbar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -78,52 +119,55 @@ conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, c
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
     const uint32_t idesc = tc::idesc_bf16_f32(128, N);
-    const uint32_t a_base = tc::smem_addr(A), b_base = tc::smem_addr(B);
+    const uint32_t b_base = tc::smem_addr(B);
 
     const int ntx = (Wc + kConvTW - 1) / kConvTW, nty = (Hc + kConvTH - 1) / kConvTH;
-    const int64_t ntiles = (int64_t)nimg * nty * ntx;
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int img = (int)(tile / ((int64_t)nty * ntx));
-        const int rem = (int)(tile - (int64_t)img * nty * ntx);
-        const int y0 = (rem / ntx) * kConvTH, x0 = (rem % ntx) * kConvTW;
-        const __nv_bfloat16* src = in + (size_t)img * Hc * Wc * G::CIN;
-        // stage cells (y0 - 1 + r, x0 - 1 + j) into the three shifted copies
-        constexpr int NQ = 2 * KS, NJ = kConvTW + 2;
-        for (int it = tid; it < (kConvTH + 2) * NQ * NJ; it += kConvThreads) {
-            const int j = it % NJ, rest = it / NJ;
-            const int q = rest % NQ, r = rest / NQ;
-            const int gy = y0 - 1 + r, gx = x0 - 1 + j;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (gy >= 0 && gy < Hc && gx >= 0 && gx < Wc)
-                v = __ldg((const uint4*)(src + ((size_t)gy * Wc + gx) * G::CIN) + q);
+    const int64_t per_img = (int64_t)nty * ntx;
+    const int64_t ntiles = (int64_t)nimg * per_img;
+    auto tile_pos = [&](int64_t tile, int& img, int& y0, int& x0) {
+        img = (int)(tile / per_img);
+        const int rem = (int)(tile - (int64_t)img * per_img);
+        y0 = (rem / ntx) * kConvTH;
+        x0 = (rem % ntx) * kConvTW;
+    };
+    auto issue = [&](const uint8_t* A) {
+        const uint32_t a_base = tc::smem_addr(A);
+        uint32_t acc = 0;
 #pragma unroll
-            for (int dx = 0; dx < 3; dx++) {
-                const int c = j - dx;
-                if (c >= 0 && c < kConvTW)
-                    *(uint4*)(A + dx * G::COPY + r * G::ROW + (c >> 3) * G::GROUP + q * 128 + (c & 7) * 16) = v;
+        for (int t = 0; t < 9; t++) {
+            const int dy = t / 3, dx = t % 3;
+#pragma unroll
+            for (int k = 0; k < KS; k++) {
+                const uint64_t ad = tc::desc_kmajor(a_base + dx * G::COPY + dy * G::ROW + k * 256, 128, G::GROUP);
+                const uint64_t bd = tc::desc_kmajor(b_base + (t * KS + k) * (N / 8) * 256, 128, 256);
+                tc::mma_bf16(tmem, ad, bd, idesc, acc);
+                acc = 1;
             }
         }
+        tc::mma_commit(mbar);
+    };
+
+    uint32_t phase = 0;
+    bool ok = true, pending = false;
+    int64_t tile = blockIdx.x;
+    if (tile < ntiles) {
+        int img, y0, x0;
+        tile_pos(tile, img, y0, x0);
+        conv_fill<KS>(A0, in + (size_t)img * Hc * Wc * G::CIN, Hc, Wc, y0, x0, tid);
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
-        if (tid == 0) {
-            uint32_t acc = 0;
-#pragma unroll
-            for (int t = 0; t < 9; t++) {
-                const int dy = t / 3, dx = t % 3;
-#pragma unroll
-                for (int k = 0; k < KS; k++) {
-                    const uint64_t ad =
-                        tc::desc_kmajor(a_base + dx * G::COPY + dy * G::ROW + k * 256, 128, G::GROUP);
-                    const uint64_t bd = tc::desc_kmajor(b_base + (t * KS + k) * (N / 8) * 256, 128, 256);
-                    tc::mma_bf16(tmem, ad, bd, idesc, acc);
-                    acc = 1;
-                }
-            }
-            tc::mma_commit(mbar);
+        if (tid == 0) issue(A0);
+        pending = true;
+    }
+    for (int k = 0; tile < ntiles; k++, tile += gridDim.x) {
+        const int64_t next = tile + gridDim.x;
+        uint8_t* An = A0 + ((k + 1) & 1) * G::A_BYTES;
+        if (next < ntiles) {
+            int img, y0, x0;
+            tile_pos(next, img, y0, x0);
+            conv_fill<KS>(An, in + (size_t)img * Hc * Wc * G::CIN, Hc, Wc, y0, x0, tid);
         }
         const bool done = __syncthreads_and(tc::mbar_wait_bounded(mbar, phase, kConvPolls) ? 1 : 0) != 0;
         if (!done) {
@@ -131,8 +175,11 @@ conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, c
             ok = false;
             break;
         }
+        pending = false;
         phase ^= 1u;
         tc::fence_after_sync();
+        int img, y0, x0;
+        tile_pos(tile, img, y0, x0);
         const int gy = y0 + warp, gx = x0 + lane;
         const bool in_frame = gy < Hc && gx < Wc;
         const size_t cell = ((size_t)img * Hc + gy) * Wc + gx;
@@ -182,11 +229,18 @@ conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, c
                                       pack_bf16x2(v[8 * q + 6], v[8 * q + 7]));
             }
         }
+        // the staged next tile becomes visible to the tensor cores and TMEM
+        // is free again once every warp has read it
+        tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
+        if (next < ntiles) {
+            if (tid == 0) issue(An);
+            pending = true;
+        }
     }
-    if (!ok) tc::mbar_wait_bounded(mbar, phase, kConvPolls);  // let issued UMMAs drain before the free
+    if (!ok && pending) tc::mbar_wait_bounded(mbar, phase, kConvPolls);  // let issued UMMAs drain before the free
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -202,8 +256,8 @@ cudaError_t conv_launch(const __nv_bfloat16* in, int nimg, int Hc, int Wc, const
     if (e != cudaSuccess) return e;
     const int64_t ntiles = (int64_t)nimg * ((Hc + kConvTH - 1) / kConvTH) * ((Wc + kConvTW - 1) / kConvTW);
     if (ntiles == 0) return cudaSuccess;
-    // 4 CTAs per SM hold 4 x 32 of the 512 TMEM columns
-    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms * 4);
+    // 2 CTAs per SM (shared memory) hold 2 x 32 of the 512 TMEM columns
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms * 2);
     conv3x3_kernel<KS, N, MODE><<<(unsigned)grid, kConvThreads, G::SMEM, st>>>(in, nimg, Hc, Wc, wpk, bias, mask,
                                                                                out, flags);
     return cudaGetLastError();

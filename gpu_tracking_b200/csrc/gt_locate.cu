@@ -525,19 +525,51 @@ __host__ __device__ constexpr int lw_warp_floats(int RI, int R) {
            2 * (lw_patch(RI) + 2 * R) * lw_patch(RI);
 }
 
+// The raw pixels of a patch (clamped rows and columns) are gathered into
+// registers, lane-strided, so the next patch's loads are in flight while the
+// current patch's passes run.
+constexpr int kLwMaxR = 7;  // largest smoothing radius of the seed-patch walk
+template <int RI>
+struct LwRaw {
+    static constexpr int RWMAX = lw_patch(RI) + 2 * kLwMaxR;
+    static constexpr int NR = (RWMAX * RWMAX + 31) / 32;
+    float v[NR];
+};
+
 template <typename T, int RI>
-__device__ void lw_build_patch(const T* __restrict__ img, const LocateConsts& c, int cu, int cv, float* patch,
-                               float* raw, float* xg, float* xb, int lane) {
+__device__ __forceinline__ void lw_raw_load(const T* __restrict__ img, const LocateConsts& c, int cu, int cv,
+                                            LwRaw<RI>& reg, int lane) {
+    constexpr int PS = lw_patch(RI);
+    const int H = c.H, W = c.W, RW = PS + 2 * c.R;
+    const int br = cu - RI - kLwShift - c.R, bc = cv - RI - kLwShift - c.R;
+#pragma unroll
+    for (int k = 0; k < LwRaw<RI>::NR; k++) {
+        const int idx = lane + 32 * k;
+        if (idx < RW * RW) {
+            const int rr = idx / RW, cc = idx - rr * RW;
+            const int gr = min(max(br + rr, 0), H - 1), gc = min(max(bc + cc, 0), W - 1);
+            reg.v[k] = load_px<T>(img, (size_t)gr * W + gc);
+        }
+    }
+}
+
+template <int RI>
+__device__ __forceinline__ void lw_raw_store(const LwRaw<RI>& reg, const LocateConsts& c, float* raw, int lane) {
+    const int RW = lw_patch(RI) + 2 * c.R;
+#pragma unroll
+    for (int k = 0; k < LwRaw<RI>::NR; k++) {
+        const int idx = lane + 32 * k;
+        if (idx < RW * RW) raw[idx] = reg.v[k];
+    }
+}
+
+// Row and column passes of a patch centred at (cu, cv) from its raw pixels.
+template <int RI>
+__device__ void lw_passes(const LocateConsts& c, int cu, int cv, float* patch, const float* raw, float* xg, float* xb,
+                          int lane) {
     constexpr int PS = lw_patch(RI);
     const int H = c.H, W = c.W, R = c.R, RW = PS + 2 * R;
     const int r0 = cu - RI - kLwShift, c0 = cv - RI - kLwShift;  // patch origin
-    const int br = r0 - R, bc = c0 - R;                          // raw origin
-    for (int idx = lane; idx < RW * RW; idx += 32) {
-        const int rr = idx / RW, cc = idx - rr * RW;
-        const int gr = min(max(br + rr, 0), H - 1), gc = min(max(bc + cc, 0), W - 1);
-        raw[idx] = load_px<T>(img, (size_t)gr * W + gc);
-    }
-    __syncwarp();
     for (int idx = lane; idx < RW * PS; idx += 32) {
         const int rr = idx / PS, pc = idx - rr * PS;
         const float* rowp = raw + rr * RW + pc;
@@ -696,10 +728,24 @@ walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const Loca
     for (int round = 0; round < (int)c.max_iter + 4; round++) {
         const unsigned needmask = __ballot_sync(0xffffffffu, need);
         if (needmask == 0u && !__any_sync(0xffffffffu, stage != 2)) break;
-        for (unsigned m = needmask; m; m &= m - 1u) {
-            const int k = __ffs(m) - 1;
-            const int cu = __shfl_sync(0xffffffffu, want_u, k), cv = __shfl_sync(0xffffffffu, want_v, k);
-            lw_build_patch<T, RI>(img, c, cu, cv, patches + k * PS * PS, raw, xg, xb, lane);
+        if (needmask) {
+            // patch k's passes run while patch k+1's pixels are loaded
+            LwRaw<RI> reg;
+            int k = __ffs(needmask) - 1;
+            int cu = __shfl_sync(0xffffffffu, want_u, k), cv = __shfl_sync(0xffffffffu, want_v, k);
+            lw_raw_load<T, RI>(img, c, cu, cv, reg, lane);
+            for (unsigned m = needmask; m;) {
+                m &= m - 1u;
+                lw_raw_store<RI>(reg, c, raw, lane);
+                __syncwarp();
+                const int kn = m ? __ffs(m) - 1 : 0;
+                const int nu = __shfl_sync(0xffffffffu, want_u, kn), nv = __shfl_sync(0xffffffffu, want_v, kn);
+                if (m) lw_raw_load<T, RI>(img, c, nu, nv, reg, lane);
+                lw_passes<RI>(c, cu, cv, patches + k * PS * PS, raw, xg, xb, lane);
+                k = kn;
+                cu = nu;
+                cv = nv;
+            }
         }
         if (need) {
             cen_u = want_u;

@@ -193,65 +193,79 @@ def compare(plain, learned, tol=0.5):
     and maximum added position error (pixels)."""
     from scipy.spatial import cKDTree
     cols = [c for c in plain.columns if c in learned.columns and c not in ("particle", "duration")]
-    matched = identical = same_position = 0
     iy, ix = cols.index("y"), cols.index("x")
-    errs = []
-    pa = plain.sort_values(["frame", "y", "x"]).reset_index(drop=True)
-    la = learned.sort_values(["frame", "y", "x"]).reset_index(drop=True)
-    pg = {f: g for f, g in pa.groupby("frame")}
-    lg = {f: g for f, g in la.groupby("frame")}
-    for f, gp in pg.items():
-        gl = lg.get(f)
-        if gl is None or len(gl) == 0:
+    vp_all = plain[cols].to_numpy(np.float32)
+    vl_all = learned[cols].to_numpy(np.float32)
+    fp = plain["frame"].to_numpy()
+    fl = learned["frame"].to_numpy()
+    op, ol = np.argsort(fp, kind="stable"), np.argsort(fl, kind="stable")
+    up, sp = np.unique(fp[op], return_index=True)
+    ul, sl = np.unique(fl[ol], return_index=True)
+    ep, el = np.append(sp[1:], len(op)), np.append(sl[1:], len(ol))
+    lpos = {f: (a, b) for f, a, b in zip(ul, sl, el)}
+    pi_all, li_all, d_all = [], [], []
+    for f, a, b in zip(up, sp, ep):
+        if f not in lpos:
             continue
-        tree = cKDTree(gl[["y", "x"]].to_numpy())
-        d, j = tree.query(gp[["y", "x"]].to_numpy(), distance_upper_bound=tol)
-        used = set()
-        order = np.argsort(d)
-        vp = gp[cols].to_numpy(np.float32)
-        vl = gl[cols].to_numpy(np.float32)
-        for i in order:
-            if not np.isfinite(d[i]) or j[i] in used:
-                continue
-            used.add(j[i])
-            matched += 1
-            errs.append(d[i])
-            a, b = vp[i], vl[j[i]]
-            if a[iy] == b[iy] and a[ix] == b[ix]:
-                same_position += 1
-            if np.all((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))):
-                identical += 1
-    n_plain, n_learned = len(plain), len(learned)
-    errs = np.asarray(errs, np.float64)
+        la, lb = lpos[f]
+        ip, il = op[a:b], ol[la:lb]
+        tree = cKDTree(vl_all[il][:, [iy, ix]].astype(np.float64))
+        d, j = tree.query(vp_all[ip][:, [iy, ix]].astype(np.float64), distance_upper_bound=tol)
+        ok = np.isfinite(d)
+        ip, d, j = ip[ok], d[ok], j[ok]
+        order = np.argsort(d, kind="stable")
+        _, first = np.unique(j[order], return_index=True)
+        keep = order[first]
+        pi_all.append(ip[keep])
+        li_all.append(il[j[keep]])
+        d_all.append(d[keep])
+    if pi_all:
+        pi, li, d = np.concatenate(pi_all), np.concatenate(li_all), np.concatenate(d_all)
+    else:
+        pi = li = np.zeros(0, np.int64)
+        d = np.zeros(0)
+    a, b = vp_all[pi], vl_all[li]
+    same_pos = (a[:, iy] == b[:, iy]) & (a[:, ix] == b[:, ix])
+    same_all = np.all((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b)), axis=1)
+    n_plain, n_learned, matched = len(plain), len(learned), len(pi)
     return {
         "recall": matched / n_plain if n_plain else 1.0,
         "precision": matched / n_learned if n_learned else 1.0,
-        "matched": matched,
-        "identical": identical,
-        "same_position": same_position,
+        "matched": int(matched),
+        "identical": int(same_all.sum()),
+        "same_position": int(same_pos.sum()),
         "plain": n_plain,
         "learned": n_learned,
-        "mean_position_error": float(errs.mean()) if len(errs) else 0.0,
-        "max_position_error": float(errs.max()) if len(errs) else 0.0,
+        "mean_position_error": float(d.mean()) if matched else 0.0,
+        "max_position_error": float(d.max()) if matched else 0.0,
     }
 
 
 def calibrate(net, frames, diameter, plain=None, recall=0.997, thresholds=None, **kwargs):
     """Highest score threshold whose learned table reaches ``recall`` of the
-    plain method's detections on ``frames``; sets and returns it."""
+    plain method's detections on ``frames`` (else the one with the best
+    recall); sets it on ``net`` and returns (threshold, [(threshold, recall,
+    precision)] for every threshold tried)."""
     from .api import batch
     kw = {k: v for k, v in kwargs.items() if k not in ("search_range", "memory")}
     kw["tqdm"] = False
     if plain is None:
         plain = batch(frames, diameter, **kw)
+    if len(plain) == 0:
+        raise ValueError("the plain method finds nothing in the calibration frames")
     if thresholds is None:
         thresholds = np.arange(2.0, -6.01, -0.5)
-    best = float(thresholds[-1])
+    curve = []
+    chosen = None
     for t in thresholds:
         net.threshold = float(t)
-        r = compare(plain, batch_learned(frames, diameter, net, **kw))["recall"]
-        if r >= recall:
-            best = float(t)
+        s = compare(plain, batch_learned(frames, diameter, net, **kw))
+        curve.append((float(t), s["recall"], s["precision"]))
+        if s["recall"] >= recall:
+            chosen = float(t)
             break
-    net.threshold = best
-    return best
+    if chosen is None:
+        best = max(r for _, r, _ in curve)
+        chosen = next(t for t, r, _ in curve if r == best)
+    net.threshold = chosen
+    return chosen, curve

@@ -148,6 +148,9 @@ GT_API void gt_table_free(gt_table* t);
  * (src/execute_gpu.rs:1378-1403, 1272-1352, 886-1184), i.e. the pyo3
  * functions batch_rust and LoG_rust (gpu_tracking_macros/src/lib.rs:57-156).
  * style selects Crocker–Grier (batch) or LoG.
+ * frames may live in host memory or in device memory of the context's
+ * device; device frames must be complete when the call is made (the
+ * engine's streams do not wait for the caller's).
  * frame_numbers (nullable, length T) gives the frame index written to the
  * "frame" column and used for linker_reset_points; NULL means 0..T-1 (the
  * reference's `frames`/keys selection, src/execute_gpu.rs:1041-1077).

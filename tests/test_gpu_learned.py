@@ -113,7 +113,8 @@ def test_trained_seeds_recover_plain_detections():
     loss = net.train(train, plain_train, steps=800, batch=64, crop=64, lr=3e-3)
     assert np.isfinite(loss).all()
     assert loss[-40:, 0].mean() < 0.5 * loss[:40, 0].mean()
-    learned.calibrate(net, train[:6], 9, recall=0.99, **kw)
+    thr, curve = learned.calibrate(net, train[:6], 9, recall=0.99, **kw)
+    assert curve and thr == net.threshold
 
     test, _ = video(4, 256, 256, 150, seed=22, turnover=1.0)
     plain = gt.batch(test, 9, tqdm=False, **kw)
