@@ -13,17 +13,27 @@
 // Convolutions pad with zeros ("same").  The parameter vector (fp32 master
 // copy) stores each layer as W[co][ci][ky*3 + kx] followed by b[co].
 //
-// Convolution as an implicit GEMM on the tensor cores: a CTA owns a tile of
-// 4 x 32 cells (M = 128 rows of D), the output channels are N and K runs over
-// the 9 taps x input channels.  The input tile (6 x 34 cells with the halo)
-// is staged three times in shared memory, shifted by -1, 0 and +1 cells, in
-// the K-major "interleave" layout (8 cells x 8 channels = one 128-byte core
-// matrix): a tap (dy, dx) is then the copy of dx read from row dy, a plain
-// descriptor offset, and one UMMA of K = 16 per tap and 16 input channels.
-// D lives in TMEM (32 columns); the epilogue reads it with tcgen05.ld, adds
-// the bias, applies the ReLU (or the ReLU mask of the backward pass) and
-// writes BF16 cells.
+// Activations are BF16 in planes of 8 channels: [image][C/8][Hc][Wc][8].
+// Convolution as an implicit GEMM on the tensor cores: a CTA owns tiles of
+// 16 rows x 8 cells (M = 128 rows of D), the output channels are N and K runs
+// over the 9 taps x input channels.  One TMA box per tile (8 channels x 10
+// cells x 18 rows x C/8 planes, the tile and its halo) lands in shared memory
+// as [plane][row][10 cells][8 channels]: 8 consecutive cells of a row are one
+// 128-byte K-major core matrix, so the operand of a tap (dy, dx) is a plain
+// descriptor at row dy, cell dx (rows 160 bytes apart, planes one plane
+// apart) and one UMMA of K = 16 covers a tap and 16 input channels.
+// The CTA is warp-specialised and persistent over its tiles: warp 0 issues
+// the TMA loads into a ring of staging buffers, one thread of warp 1 issues
+// the UMMAs into a ring of TMEM accumulators (32 columns each), and warps
+// 2-5 drain the accumulators (tcgen05.ld, bias, ReLU or the ReLU mask of the
+// backward pass, BF16 planes out).  The roles hand buffers to each other
+// through mbarriers only (full / empty per staging buffer, full / empty per
+// accumulator), so loads, UMMAs and epilogues of different tiles overlap.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
 
 #include "gt_internal.cuh"
 #include "gt_kernels.h"
@@ -33,233 +43,255 @@ namespace gt {
 
 namespace {
 
-constexpr int kConvTW = 32;       // tile width in cells (4 core-matrix groups)
-constexpr int kConvTH = 4;        // tile rows: M = 128
-constexpr int kConvThreads = 128;  // 4 warps: warp w reads TMEM lanes 32w..32w+31 = tile row w
+constexpr int kConvRows = 16;     // tile rows (one core-matrix row of M each)
+constexpr int kConvCols = 8;      // tile cells per row
 constexpr uint32_t kConvPolls = 1u << 22;
 
 template <int KS, int N>
 struct ConvGeom {
-    static constexpr int CIN = 16 * KS;
-    static constexpr int GROUP = KS * 2 * 128;          // bytes of 8 cells x CIN channels
-    static constexpr int ROW = (kConvTW / 8) * GROUP;   // one row of the tile
-    static constexpr int COPY = (kConvTH + 2) * ROW;    // one dx-shifted copy (with the row halo)
-    static constexpr int A_BYTES = 3 * COPY;
+    static constexpr int PLANES = 2 * KS;                 // 8-channel input planes
+    static constexpr int RS = (kConvCols + 2) * 16;       // staged row: 10 cells x 16 bytes
+    static constexpr int PLANE = (kConvRows + 2) * RS;    // one plane: 18 rows
+    static constexpr int STAGE = ((PLANES * PLANE + 127) / 128) * 128;
+    static constexpr int NSTAGE = 6;
+    static constexpr int NACC = 4;                        // TMEM accumulators of 32 columns
     static constexpr int B_BYTES = 9 * KS * (N / 8) * 256;
-    static constexpr int SMEM = 128 + 2 * A_BYTES + B_BYTES + 16;  // two staging buffers
+    static constexpr int SMEM = 128 + NSTAGE * STAGE + B_BYTES + 128 + 8 * (2 * NSTAGE + 2 * NACC) + 16;
 };
+constexpr int kConvWsThreads = 192;  // warp 0 loads, warp 1 issues, warps 2-5 drain
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// Stage the input cells (y0 - 1 + r, x0 - 1 + j) of a tile into the three
-// shifted copies at A: every load of the tile is issued before the first
-// shared-memory store, so the tile costs one round trip to L2.
-template <int KS>
-__device__ __forceinline__ void conv_fill(uint8_t* A, const __nv_bfloat16* __restrict__ src, int Hc, int Wc, int y0,
-                                          int x0, int tid) {
-    using G = ConvGeom<KS, 32>;
-    constexpr int NQ = 2 * KS, NJ = kConvTW + 2;
-    constexpr int TOTAL = (kConvTH + 2) * NQ * NJ;
-    constexpr int NIT = (TOTAL + kConvThreads - 1) / kConvThreads;
-    uint4 v[NIT];
-#pragma unroll
-    for (int k = 0; k < NIT; k++) {
-        const int it = tid + k * kConvThreads;
-        v[k] = make_uint4(0u, 0u, 0u, 0u);
-        if (it < TOTAL) {
-            const int j = it % NJ, rest = it / NJ;
-            const int q = rest % NQ, r = rest / NQ;
-            const int gy = y0 - 1 + r, gx = x0 - 1 + j;
-            if (gy >= 0 && gy < Hc && gx >= 0 && gx < Wc)
-                v[k] = __ldg((const uint4*)(src + ((size_t)gy * Wc + gx) * G::CIN) + q);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < NIT; k++) {
-        const int it = tid + k * kConvThreads;
-        if (it < TOTAL) {
-            const int j = it % NJ, rest = it / NJ;
-            const int q = rest % NQ, r = rest / NQ;
-#pragma unroll
-            for (int dx = 0; dx < 3; dx++) {
-                const int c = j - dx;
-                if (c >= 0 && c < kConvTW)
-                    *(uint4*)(A + dx * G::COPY + r * G::ROW + (c >> 3) * G::GROUP + q * 128 + (c & 7) * 16) = v[k];
-            }
-        }
-    }
-}
+// bf16 > 0: sign bit clear and not +0
+__device__ __forceinline__ bool bf16_pos(uint32_t h) { return h != 0u && !(h & 0x8000u); }
 
-// MODE 0: relu(acc + bias) -> bf16 [cell][32]
+// MODE 0: relu(acc + bias) -> bf16 planes (32 channels)
 // MODE 1: acc + bias      -> float4 [cell] (score, row offset, column offset, 0), N = 16
-// MODE 2: acc * (mask > 0) -> bf16 [cell][32] (backward through the ReLU of the layer below)
-// A CTA walks its tiles with two staging buffers: the next tile is staged
-// while the tensor cores work on the current one.
+// MODE 2: acc * (mask > 0) -> bf16 planes (backward through the ReLU of the layer below)
 template <int KS, int N, int MODE>
-__global__ void __launch_bounds__(kConvThreads)
-conv3x3_kernel(const __nv_bfloat16* __restrict__ in, int nimg, int Hc, int Wc, const uint8_t* __restrict__ wpk,
+__global__ void __launch_bounds__(kConvWsThreads)
+conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc, const uint8_t* __restrict__ wpk,
                const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask, void* __restrict__ out,
                uint32_t* __restrict__ flags) {
     using G = ConvGeom<KS, N>;
+    constexpr int NS = G::NSTAGE, NA = G::NACC;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* A0 = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    uint8_t* B = A0 + 2 * G::A_BYTES;
-    uint64_t* mbar = (uint64_t*)(B + G::B_BYTES);
-    uint32_t* tslot = (uint32_t*)(mbar + 1);
+    uint8_t* S0 = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint8_t* B = S0 + NS * G::STAGE;
+    float* sbias = (float*)(B + G::B_BYTES);  // [32]
+    uint64_t* full = (uint64_t*)(sbias + 32);  // [NS] staging buffer loaded
+    uint64_t* empty = full + NS;               // [NS] staging buffer consumed by its UMMAs
+    uint64_t* accf = empty + NS;               // [NA] accumulator written
+    uint64_t* acce = accf + NA;                // [NA] accumulator read by the 4 epilogue warps
+    uint32_t* tslot = (uint32_t*)(acce + NA);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    for (int i = tid; i < G::B_BYTES / 16; i += kConvThreads) ((uint4*)B)[i] = __ldg((const uint4*)wpk + i);
-    if (tid == 0) tc::mbar_init(mbar, 1);
-    if (warp == 0) tc::tmem_alloc(tslot, 32);
+    for (int i = tid; i < G::B_BYTES / 16; i += kConvWsThreads) ((uint4*)B)[i] = __ldg((const uint4*)wpk + i);
+    if (tid < 32) sbias[tid] = (bias && tid < (MODE == 1 ? 3 : 32)) ? bias[tid] : 0.0f;
+    if (tid == 0) {
+        for (int i = 0; i < 2 * NS + NA; i++) tc::mbar_init(full + i, 1);
+        for (int i = 0; i < NA; i++) tc::mbar_init(acce + i, 4);
+    }
+    if (warp == 0) tc::tmem_alloc(tslot, 32 * NA);
+    tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = tc::idesc_bf16_f32(128, N);
-    const uint32_t b_base = tc::smem_addr(B);
 
-    const int ntx = (Wc + kConvTW - 1) / kConvTW, nty = (Hc + kConvTH - 1) / kConvTH;
+    const int ntx = (Wc + kConvCols - 1) / kConvCols, nty = (Hc + kConvRows - 1) / kConvRows;
     const int64_t per_img = (int64_t)nty * ntx;
     const int64_t ntiles = (int64_t)nimg * per_img;
-    auto tile_pos = [&](int64_t tile, int& img, int& y0, int& x0) {
+    const int64_t t0 = blockIdx.x, stride = gridDim.x;
+    // this CTA's tiles are t0 + k * stride, k = 0 .. nmine - 1
+    const int nmine = t0 < ntiles ? (int)((ntiles - 1 - t0) / stride) + 1 : 0;
+    auto tile_pos = [&](int k, int& img, int& y0, int& x0) {
+        const int64_t tile = t0 + (int64_t)k * stride;
         img = (int)(tile / per_img);
         const int rem = (int)(tile - (int64_t)img * per_img);
-        y0 = (rem / ntx) * kConvTH;
-        x0 = (rem % ntx) * kConvTW;
-    };
-    auto issue = [&](const uint8_t* A) {
-        const uint32_t a_base = tc::smem_addr(A);
-        uint32_t acc = 0;
-#pragma unroll
-        for (int t = 0; t < 9; t++) {
-            const int dy = t / 3, dx = t % 3;
-#pragma unroll
-            for (int k = 0; k < KS; k++) {
-                const uint64_t ad = tc::desc_kmajor(a_base + dx * G::COPY + dy * G::ROW + k * 256, 128, G::GROUP);
-                const uint64_t bd = tc::desc_kmajor(b_base + (t * KS + k) * (N / 8) * 256, 128, 256);
-                tc::mma_bf16(tmem, ad, bd, idesc, acc);
-                acc = 1;
-            }
-        }
-        tc::mma_commit(mbar);
+        y0 = (rem / ntx) * kConvRows;
+        x0 = (rem % ntx) * kConvCols;
     };
 
-    uint32_t phase = 0;
-    bool ok = true, pending = false;
-    int64_t tile = blockIdx.x;
-    if (tile < ntiles) {
-        int img, y0, x0;
-        tile_pos(tile, img, y0, x0);
-        conv_fill<KS>(A0, in + (size_t)img * Hc * Wc * G::CIN, Hc, Wc, y0, x0, tid);
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
-        tc::fence_after_sync();
-        if (tid == 0) issue(A0);
-        pending = true;
-    }
-    for (int k = 0; tile < ntiles; k++, tile += gridDim.x) {
-        const int64_t next = tile + gridDim.x;
-        uint8_t* An = A0 + ((k + 1) & 1) * G::A_BYTES;
-        if (next < ntiles) {
-            int img, y0, x0;
-            tile_pos(next, img, y0, x0);
-            conv_fill<KS>(An, in + (size_t)img * Hc * Wc * G::CIN, Hc, Wc, y0, x0, tid);
-        }
-        const bool done = __syncthreads_and(tc::mbar_wait_bounded(mbar, phase, kConvPolls) ? 1 : 0) != 0;
-        if (!done) {
-            if (tid == 0) atomicOr(flags, kFlagTensorTimeout);
-            ok = false;
-            break;
-        }
-        pending = false;
-        phase ^= 1u;
-        tc::fence_after_sync();
-        int img, y0, x0;
-        tile_pos(tile, img, y0, x0);
-        const int gy = y0 + warp, gx = x0 + lane;
-        const bool in_frame = gy < Hc && gx < Wc;
-        const size_t cell = ((size_t)img * Hc + gy) * Wc + gx;
-        if (MODE == 1) {
-            uint32_t r[16];
-            tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16), r);
-            tc::tmem_ld_wait();
-            if (in_frame) {
-                float4 o;
-                o.x = __fadd_rn(__uint_as_float(r[0]), bias[0]);
-                o.y = __fadd_rn(__uint_as_float(r[1]), bias[1]);
-                o.z = __fadd_rn(__uint_as_float(r[2]), bias[2]);
-                o.w = 0.0f;
-                ((float4*)out)[cell] = o;
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: stage k % NS is free again once tile k - NS's UMMAs completed
+            int k = 0;
+            for (; k < nmine; k++) {
+                const int st = k % NS;
+                if (k >= NS && !tc::mbar_wait_bounded(empty + st, (uint32_t)((k / NS - 1) & 1), kConvPolls)) {
+                    atomicOr(flags, kFlagTensorTimeout);
+                    break;
+                }
+                int img, y0, x0;
+                tile_pos(k, img, y0, x0);
+                tc::mbar_arrive_expect_tx(full + st, G::PLANES * G::PLANE);
+                tc::tma_load_4d(S0 + st * G::STAGE, &tin, 0, x0 - 1, y0 - 1, img * G::PLANES, full + st);
             }
-        } else {
-            uint32_t r[32];
-            tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16), r);
-            tc::tmem_ld_wait();
-            if (in_frame) {
-                float v[32];
+            // no load may still be landing when the CTA leaves
+            for (int j = max(0, k - NS); j < k; j++)
+                tc::mbar_wait_bounded(full + j % NS, (uint32_t)((j / NS) & 1), kConvPolls);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16_f32(128, N);
+            const uint32_t b_base = tc::smem_addr(B);
+            int k = 0;
+            for (; k < nmine; k++) {
+                const int st = k % NS, ab = k % NA;
+                if (!tc::mbar_wait_bounded(full + st, (uint32_t)((k / NS) & 1), kConvPolls) ||
+                    (k >= NA && !tc::mbar_wait_bounded(acce + ab, (uint32_t)((k / NA - 1) & 1), kConvPolls))) {
+                    atomicOr(flags, kFlagTensorTimeout);
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t a_base = tc::smem_addr(S0 + st * G::STAGE);
+                uint32_t acc = 0;
 #pragma unroll
-                for (int n = 0; n < 32; n++) v[n] = __uint_as_float(r[n]);
-                if (MODE == 0) {
+                for (int t = 0; t < 9; t++) {
+                    const int dy = t / 3, dx = t % 3;
 #pragma unroll
-                    for (int n = 0; n < 32; n++) v[n] = fmaxf(__fadd_rn(v[n], bias[n]), 0.0f);
-                } else {
-                    const uint4* mk = (const uint4*)(mask + cell * 32);
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        uint4 m4 = __ldg(mk + q);
-                        const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
-#pragma unroll
-                        for (int h = 0; h < 4; h++) {
-                            // bf16 > 0: sign bit clear and not +0
-                            const uint32_t lo = mw[h] & 0xFFFFu, hi = mw[h] >> 16;
-                            if (!(lo != 0u && !(lo & 0x8000u))) v[8 * q + 2 * h] = 0.0f;
-                            if (!(hi != 0u && !(hi & 0x8000u))) v[8 * q + 2 * h + 1] = 0.0f;
-                        }
+                    for (int kk = 0; kk < KS; kk++) {
+                        const uint64_t ad =
+                            tc::desc_kmajor(a_base + 2 * kk * G::PLANE + dy * G::RS + dx * 16, G::PLANE, G::RS);
+                        const uint64_t bd = tc::desc_kmajor(b_base + (t * KS + kk) * (N / 8) * 256, 128, 256);
+                        tc::mma_bf16(tmem + 32 * ab, ad, bd, idesc, acc);
+                        acc = 1;
                     }
                 }
-                uint4* o = (uint4*)((__nv_bfloat16*)out + cell * 32);
+                tc::mma_commit(empty + st);
+                tc::mma_commit(accf + ab);
+            }
+            // the accumulators of the issued tiles must be complete before TMEM is freed
+            for (int j = max(0, k - NA); j < k; j++)
+                tc::mbar_wait_bounded(accf + j % NA, (uint32_t)((j / NA) & 1), kConvPolls);
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 = tile rows 4 * (w % 4) .. + 3
+        const int sub = warp & 3;
+        for (int k = 0; k < nmine; k++) {
+            const int ab = k % NA;
+            const bool ready = tc::mbar_wait_bounded(accf + ab, (uint32_t)((k / NA) & 1), kConvPolls);
+            if (!__all_sync(0xffffffffu, ready)) {
+                if (lane == 0) atomicOr(flags, kFlagTensorTimeout);
+                break;
+            }
+            tc::fence_after_sync();
+            int img, y0, x0;
+            tile_pos(k, img, y0, x0);
+            const int gy = y0 + 4 * sub + (lane >> 3), gx = x0 + (lane & 7);
+            const bool in_frame = gy < Hc && gx < Wc;
+            const uint32_t taddr = tmem + 32 * ab + ((uint32_t)(32 * sub) << 16);
+            if (MODE == 1) {
+                uint32_t r[16];
+                tc::tmem_ld16(taddr, r);
+                tc::tmem_ld_wait();
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(acce + ab);
+                if (in_frame) {
+                    float4 o;
+                    o.x = __fadd_rn(__uint_as_float(r[0]), sbias[0]);
+                    o.y = __fadd_rn(__uint_as_float(r[1]), sbias[1]);
+                    o.z = __fadd_rn(__uint_as_float(r[2]), sbias[2]);
+                    o.w = 0.0f;
+                    ((float4*)out)[((size_t)img * Hc + gy) * Wc + gx] = o;
+                }
+            } else {
+                uint32_t r[32];
+                tc::tmem_ld32(taddr, r);
+                tc::tmem_ld_wait();
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(acce + ab);
+                if (in_frame) {
+                    float v[32];
 #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    o[q] = make_uint4(pack_bf16x2(v[8 * q], v[8 * q + 1]), pack_bf16x2(v[8 * q + 2], v[8 * q + 3]),
-                                      pack_bf16x2(v[8 * q + 4], v[8 * q + 5]),
-                                      pack_bf16x2(v[8 * q + 6], v[8 * q + 7]));
+                    for (int n = 0; n < 32; n++) v[n] = __uint_as_float(r[n]);
+                    if (MODE == 0) {
+#pragma unroll
+                        for (int n = 0; n < 32; n++) v[n] = fmaxf(__fadd_rn(v[n], sbias[n]), 0.0f);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const uint4 m4 =
+                                __ldg((const uint4*)(mask + ((((size_t)img * 4 + q) * Hc + gy) * Wc + gx) * 8));
+                            const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+                            for (int h = 0; h < 4; h++) {
+                                if (!bf16_pos(mw[h] & 0xFFFFu)) v[8 * q + 2 * h] = 0.0f;
+                                if (!bf16_pos(mw[h] >> 16)) v[8 * q + 2 * h + 1] = 0.0f;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        *(uint4*)((__nv_bfloat16*)out + ((((size_t)img * 4 + q) * Hc + gy) * Wc + gx) * 8) =
+                            make_uint4(pack_bf16x2(v[8 * q], v[8 * q + 1]), pack_bf16x2(v[8 * q + 2], v[8 * q + 3]),
+                                       pack_bf16x2(v[8 * q + 4], v[8 * q + 5]),
+                                       pack_bf16x2(v[8 * q + 6], v[8 * q + 7]));
+                }
             }
         }
-        // the staged next tile becomes visible to the tensor cores and TMEM
-        // is free again once every warp has read it
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
-        tc::fence_after_sync();
-        if (next < ntiles) {
-            if (tid == 0) issue(An);
-            pending = true;
-        }
     }
-    if (!ok && pending) tc::mbar_wait_bounded(mbar, phase, kConvPolls);  // let issued UMMAs drain before the free
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+    if (warp == 0) tc::tmem_dealloc(tmem, 32 * NA);
+}
+
+// The tensor map of a BF16 plane tensor [planes_total][Hc][Wc][8] whose box
+// is one tile with its halo: 8 channels x 10 cells x 18 rows x planes_per_img
+// planes.
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+cudaError_t plane_map(CUtensorMap* m, const void* base, int nimg, int planes_per_img, int Hc, int Wc) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn) return cudaErrorNotSupported;
+    if (((uintptr_t)base & 15u) != 0u) return cudaErrorMisalignedAddress;
+    const cuuint64_t dims[4] = {8, (cuuint64_t)Wc, (cuuint64_t)Hc, (cuuint64_t)nimg * planes_per_img};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)Wc * 16, (cuuint64_t)Hc * Wc * 16};
+    const cuuint32_t box[4] = {8, (cuuint32_t)(kConvCols + 2), (cuuint32_t)(kConvRows + 2), (cuuint32_t)planes_per_img};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 template <int KS, int N, int MODE>
 cudaError_t conv_launch(const __nv_bfloat16* in, int nimg, int Hc, int Wc, const uint8_t* wpk, const float* bias,
                         const __nv_bfloat16* mask, void* out, uint32_t* flags, int num_sms, cudaStream_t st) {
     using G = ConvGeom<KS, N>;
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<KS, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         G::SMEM);
-    if (e != cudaSuccess) return e;
-    const int64_t ntiles = (int64_t)nimg * ((Hc + kConvTH - 1) / kConvTH) * ((Wc + kConvTW - 1) / kConvTW);
+    const int64_t ntiles =
+        (int64_t)nimg * ((Hc + kConvRows - 1) / kConvRows) * ((Wc + kConvCols - 1) / kConvCols);
     if (ntiles == 0) return cudaSuccess;
-    // 2 CTAs per SM (shared memory) hold 2 x 32 of the 512 TMEM columns
+    CUtensorMap tm;
+    cudaError_t e = plane_map(&tm, in, nimg, G::PLANES, Hc, Wc);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(conv3x3_kernel<KS, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    if (e != cudaSuccess) return e;
+    // persistent: at most 2 CTAs per SM, 2 x 128 of the 512 TMEM columns
+    static_assert(2 * G::SMEM <= 227 * 1024, "two CTAs per SM");
     const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms * 2);
-    conv3x3_kernel<KS, N, MODE><<<(unsigned)grid, kConvThreads, G::SMEM, st>>>(in, nimg, Hc, Wc, wpk, bias, mask,
-                                                                               out, flags);
+    conv3x3_kernel<KS, N, MODE><<<(unsigned)grid, kConvWsThreads, G::SMEM, st>>>(tm, nimg, Hc, Wc, wpk, bias, mask,
+                                                                                 out, flags);
     return cudaGetLastError();
 }
 
@@ -337,11 +369,14 @@ __global__ void cnn_input_kernel(const T* __restrict__ frames, int64_t frame_str
             if (y < H && x < W) p = __fmul_rn(__fsub_rn(load_px<T>(f, (size_t)y * W + x), mean), scale);
             v[4 * dy + dx] = p;
         }
-    uint4* o = (uint4*)(out + cell * 16);
-    o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                      pack_bf16x2(v[6], v[7]));
-    o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
-                      pack_bf16x2(v[14], v[15]));
+    // two planes of 8 channels
+    const size_t plane = (size_t)Hc * Wc;
+    uint4* o0 = (uint4*)(out + ((size_t)img * 2 * plane + rem) * 8);
+    uint4* o1 = (uint4*)(out + (((size_t)img * 2 + 1) * plane + rem) * 8);
+    *o0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                     pack_bf16x2(v[6], v[7]));
+    *o1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                     pack_bf16x2(v[14], v[15]));
 }
 
 // ---------------------------------------------------------------- labels
@@ -437,9 +472,11 @@ __global__ void cnn_loss_kernel(const float4* __restrict__ head, const float4* _
         const float ey = o.y - t.y, ex = o.z - t.z;
         lo = lambda * y * (ey * ey + ex * ex);
         const float gy = 2.0f * lambda * y * ey * inv, gx = 2.0f * lambda * y * ex * inv;
-        uint4* g = (uint4*)(grad + cell * 16);
-        g[0] = make_uint4(pack_bf16x2(gs, gy), pack_bf16x2(gx, 0.0f), 0u, 0u);
-        g[1] = make_uint4(0u, 0u, 0u, 0u);
+        // two planes of 8 channels: the three gradients, then zeros
+        const size_t plane = (size_t)CH * CW;
+        *(uint4*)(grad + ((size_t)img * 2 * plane + rem) * 8) =
+            make_uint4(pack_bf16x2(gs, gy), pack_bf16x2(gx, 0.0f), 0u, 0u);
+        *(uint4*)(grad + (((size_t)img * 2 + 1) * plane + rem) * 8) = make_uint4(0u, 0u, 0u, 0u);
     }
 #pragma unroll
     for (int d = 16; d; d >>= 1) {
@@ -463,7 +500,8 @@ __global__ void cnn_loss_kernel(const float4* __restrict__ head, const float4* _
 }
 
 // -------------------------------------------------------- weight gradient
-// dW[co][ci][t] = sum over cells of G[cell][co] * X[cell + tap t][ci], and
+// dW[co][ci][t] = sum over cells of G[cell][co] * X[cell + tap t][ci] (both
+// in 8-channel planes; G has GSTRIDE channels of which COUT are used), and
 // db[co] = sum of G[cell][co]: one thread per (t, ci) (plus one for the
 // bias) accumulating all output channels in registers over the tiles its
 // CTA owns; per-CTA partial sums go to `partial` and are added in CTA order.
@@ -494,7 +532,7 @@ cnn_wgrad_kernel(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __res
             const int gy = y0 - 1 + r, gx = x0 - 1 + j;
             float v = 0.0f;
             if (gy >= 0 && gy < Hc && gx >= 0 && gx < Wc)
-                v = __bfloat162float(X[(((size_t)img * Hc + gy) * Wc + gx) * CIN + c]);
+                v = __bfloat162float(X[((((size_t)img * (CIN / 8) + c / 8) * Hc + gy) * Wc + gx) * 8 + (c & 7)]);
             xs[i] = v;
         }
         for (int i = tid; i < kWgTH * kWgTW * COUT; i += blockDim.x) {
@@ -502,7 +540,8 @@ cnn_wgrad_kernel(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __res
             const int j = rest % kWgTW, r = rest / kWgTW;
             const int gy = y0 + r, gx = x0 + j;
             float v = 0.0f;
-            if (gy < Hc && gx < Wc) v = __bfloat162float(Gd[(((size_t)img * Hc + gy) * Wc + gx) * GSTRIDE + o]);
+            if (gy < Hc && gx < Wc)
+                v = __bfloat162float(Gd[((((size_t)img * (GSTRIDE / 8) + o / 8) * Hc + gy) * Wc + gx) * 8 + (o & 7)]);
             gs[i] = v;
         }
         __syncthreads();

@@ -89,6 +89,30 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
     return false;
 }
 
+// One plain arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(mbar)) : "memory");
+}
+
+// One arrival on the mbarrier that also expects `bytes` of asynchronous
+// (TMA) traffic before the phase can complete.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA tile load of a 4-D box (no multicast) into this CTA's shared memory;
+// completion is reported to `mbar` as transaction bytes.  c0 is the
+// innermost coordinate.
+__device__ __forceinline__ void tma_load_4d(void* smem_dst, const void* tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_addr(smem_dst)),
+        "l"((uint64_t)tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(mbar))
+        : "memory");
+}
+
 // Warp-wide loads of 32-bit TMEM cells: lane i of the warp reads TMEM lane
 // (base lane + i), columns col .. col + n - 1, into r[0..n).
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
