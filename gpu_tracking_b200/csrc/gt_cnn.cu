@@ -138,7 +138,12 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
     } else if (warp == 1) {
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_bf16_f32(128, N);
-            const uint32_t b_base = tc::smem_addr(B);
+            // descriptors of stage 0 and of the weights; a stage or a tap is a
+            // start-address offset (the low 14 bits, in 16-byte units)
+            const uint64_t a_desc0 = tc::desc_kmajor(tc::smem_addr(S0), G::PLANE, G::RS);
+            uint64_t b_desc[9 * KS];
+#pragma unroll
+            for (int j = 0; j < 9 * KS; j++) b_desc[j] = tc::desc_kmajor(tc::smem_addr(B) + j * (N / 8) * 256, 128, 256);
             int k = 0;
             for (; k < nmine; k++) {
                 const int st = k % NS, ab = k % NA;
@@ -148,17 +153,15 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
                     break;
                 }
                 tc::fence_after_sync();
-                const uint32_t a_base = tc::smem_addr(S0 + st * G::STAGE);
+                const uint64_t a_desc = a_desc0 + (uint64_t)((st * G::STAGE) >> 4);
                 uint32_t acc = 0;
 #pragma unroll
                 for (int t = 0; t < 9; t++) {
                     const int dy = t / 3, dx = t % 3;
 #pragma unroll
                     for (int kk = 0; kk < KS; kk++) {
-                        const uint64_t ad =
-                            tc::desc_kmajor(a_base + 2 * kk * G::PLANE + dy * G::RS + dx * 16, G::PLANE, G::RS);
-                        const uint64_t bd = tc::desc_kmajor(b_base + (t * KS + kk) * (N / 8) * 256, 128, 256);
-                        tc::mma_bf16(tmem + 32 * ab, ad, bd, idesc, acc);
+                        const uint64_t ad = a_desc + (uint64_t)((2 * kk * G::PLANE + dy * G::RS + dx * 16) >> 4);
+                        tc::mma_bf16(tmem + 32 * ab, ad, b_desc[t * KS + kk], idesc, acc);
                         acc = 1;
                     }
                 }
@@ -358,17 +361,48 @@ __global__ void cnn_input_kernel(const T* __restrict__ frames, int64_t frame_str
     }
     const T* f = frames + (size_t)fi * frame_stride;
     float v[16];
+    const int yb = oy + 4 * cy, xb = ox + 4 * cx;
+    if (!aug && yb + 3 < H && xb + 3 < W && (W & 3) == 0 && (frame_stride & 3) == 0) {
+        // whole block inside the frame, rows of 4 pixels aligned to 4: one load per row
 #pragma unroll
-    for (int dy = 0; dy < 4; dy++)
+        for (int dy = 0; dy < 4; dy++) {
+            const T* row = f + (size_t)(yb + dy) * W + xb;
+            float q[4];
+            if (sizeof(T) == 2) {
+                const uint2 w = __ldg((const uint2*)row);
+                q[0] = (float)(w.x & 0xFFFFu);
+                q[1] = (float)(w.x >> 16);
+                q[2] = (float)(w.y & 0xFFFFu);
+                q[3] = (float)(w.y >> 16);
+            } else if (sizeof(T) == 1) {
+                const uint32_t w = __ldg((const uint32_t*)row);
+                q[0] = (float)(w & 0xFFu);
+                q[1] = (float)((w >> 8) & 0xFFu);
+                q[2] = (float)((w >> 16) & 0xFFu);
+                q[3] = (float)(w >> 24);
+            } else {
+                const float4 w = __ldg((const float4*)row);
+                q[0] = w.x;
+                q[1] = w.y;
+                q[2] = w.z;
+                q[3] = w.w;
+            }
 #pragma unroll
-        for (int dx = 0; dx < 4; dx++) {
-            int a = 4 * cy + dy, b = 4 * cx + dx;
-            if (aug) aug_map(aug, 4 * Hc, a, b);
-            const int y = oy + a, x = ox + b;
-            float p = 0.0f;
-            if (y < H && x < W) p = __fmul_rn(__fsub_rn(load_px<T>(f, (size_t)y * W + x), mean), scale);
-            v[4 * dy + dx] = p;
+            for (int dx = 0; dx < 4; dx++) v[4 * dy + dx] = __fmul_rn(__fsub_rn(q[dx], mean), scale);
         }
+    } else {
+#pragma unroll
+        for (int dy = 0; dy < 4; dy++)
+#pragma unroll
+            for (int dx = 0; dx < 4; dx++) {
+                int a = 4 * cy + dy, b = 4 * cx + dx;
+                if (aug) aug_map(aug, 4 * Hc, a, b);
+                const int y = oy + a, x = ox + b;
+                float p = 0.0f;
+                if (y < H && x < W) p = __fmul_rn(__fsub_rn(load_px<T>(f, (size_t)y * W + x), mean), scale);
+                v[4 * dy + dx] = p;
+            }
+    }
     // two planes of 8 channels
     const size_t plane = (size_t)Hc * Wc;
     uint4* o0 = (uint4*)(out + ((size_t)img * 2 * plane + rem) * 8);

@@ -517,12 +517,20 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
 // walk or characterize circle leaves the patch asks for a patch centred
 // where it stands and resumes there.
 constexpr int kLwWarps = 4;
+constexpr int kLwSeeds = 16;  // seeds per warp (lanes 0-15); all 32 lanes build the patches
 constexpr int kLwShift = 1;   // walk steps a patch covers around its centre
 
 __host__ __device__ constexpr int lw_patch(int RI) { return 2 * (RI + kLwShift) + 1; }
 __host__ __device__ constexpr int lw_warp_floats(int RI, int R) {
-    return 32 * lw_patch(RI) * lw_patch(RI) + (lw_patch(RI) + 2 * R) * (lw_patch(RI) + 2 * R) +
+    return kLwSeeds * lw_patch(RI) * lw_patch(RI) + (lw_patch(RI) + 2 * R) * (lw_patch(RI) + 2 * R) +
            2 * (lw_patch(RI) + 2 * R) * lw_patch(RI);
+}
+
+// Division by the bandpass constants: the proven two-float reciprocal when
+// LocateConsts::fast_div is set (equal to IEEE division for every dividend
+// of integer frames), else IEEE division.
+__device__ __forceinline__ float lw_div(float x, float d, float zh, float zl, bool fast) {
+    return fast ? __fmaf_rn(x, zh, __fmul_rn(x, zl)) : __fdiv_rn(x, d);
 }
 
 // The raw pixels of a patch (clamped rows and columns) are gathered into
@@ -536,12 +544,14 @@ struct LwRaw {
     float v[NR];
 };
 
-template <typename T, int RI>
+// RC > 0: the smoothing radius as a compile-time constant (= c.R), else c.R.
+template <typename T, int RI, int RC>
 __device__ __forceinline__ void lw_raw_load(const T* __restrict__ img, const LocateConsts& c, int cu, int cv,
                                             LwRaw<RI>& reg, int lane) {
     constexpr int PS = lw_patch(RI);
-    const int H = c.H, W = c.W, RW = PS + 2 * c.R;
-    const int br = cu - RI - kLwShift - c.R, bc = cv - RI - kLwShift - c.R;
+    const int R = RC > 0 ? RC : c.R;
+    const int H = c.H, W = c.W, RW = PS + 2 * R;
+    const int br = cu - RI - kLwShift - R, bc = cv - RI - kLwShift - R;
 #pragma unroll
     for (int k = 0; k < LwRaw<RI>::NR; k++) {
         const int idx = lane + 32 * k;
@@ -553,9 +563,9 @@ __device__ __forceinline__ void lw_raw_load(const T* __restrict__ img, const Loc
     }
 }
 
-template <int RI>
+template <int RI, int RC>
 __device__ __forceinline__ void lw_raw_store(const LwRaw<RI>& reg, const LocateConsts& c, float* raw, int lane) {
-    const int RW = lw_patch(RI) + 2 * c.R;
+    const int RW = lw_patch(RI) + 2 * (RC > 0 ? RC : c.R);
 #pragma unroll
     for (int k = 0; k < LwRaw<RI>::NR; k++) {
         const int idx = lane + 32 * k;
@@ -564,25 +574,46 @@ __device__ __forceinline__ void lw_raw_store(const LwRaw<RI>& reg, const LocateC
 }
 
 // Row and column passes of a patch centred at (cu, cv) from its raw pixels.
-template <int RI>
+// A patch whose raw window lies inside the frame takes no bounds tests.
+template <int RI, int RC>
 __device__ void lw_passes(const LocateConsts& c, int cu, int cv, float* patch, const float* raw, float* xg, float* xb,
                           int lane) {
     constexpr int PS = lw_patch(RI);
-    const int H = c.H, W = c.W, R = c.R, RW = PS + 2 * R;
+    const int R = RC > 0 ? RC : c.R;
+    const int H = c.H, W = c.W, RW = PS + 2 * R;
     const int r0 = cu - RI - kLwShift, c0 = cv - RI - kLwShift;  // patch origin
-    for (int idx = lane; idx < RW * PS; idx += 32) {
-        const int rr = idx / PS, pc = idx - rr * PS;
-        const float* rowp = raw + rr * RW + pc;
-        const int gcol = c0 + pc;
-        float gs = 0.0f, cs = 0.0f;
-        for (int i = 0; i <= 2 * R; i++) {
-            const float x = rowp[i];
-            const int gc = gcol + i - R;
-            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
-            cs = __fadd_rn(cs, x);
+    const bool fast = c.fast_div != 0;
+    const bool interior = r0 - R >= 0 && r0 + PS - 1 + R < H && c0 - R >= 0 && c0 + PS - 1 + R < W;
+    if (interior) {
+        for (int idx = lane; idx < RW * PS; idx += 32) {
+            const int rr = idx / PS, pc = idx - rr * PS;
+            const float* rowp = raw + rr * RW + pc;
+            float gs = 0.0f, cs = 0.0f;
+#pragma unroll
+            for (int i = 0; i <= 2 * R; i++) {
+                const float x = rowp[i];
+                gs = __fmaf_rn(c.taps[i], x, gs);
+                cs = __fadd_rn(cs, x);
+            }
+            xg[idx] = lw_div(gs, c.gnorm, c.zh_g, c.zl_g, fast);
+            xb[idx] = cs;
         }
-        xg[idx] = __fdiv_rn(gs, c.gnorm);
-        xb[idx] = cs;
+    } else {
+        for (int idx = lane; idx < RW * PS; idx += 32) {
+            const int rr = idx / PS, pc = idx - rr * PS;
+            const float* rowp = raw + rr * RW + pc;
+            const int gcol = c0 + pc;
+            float gs = 0.0f, cs = 0.0f;
+#pragma unroll
+            for (int i = 0; i <= 2 * R; i++) {
+                const float x = rowp[i];
+                const int gc = gcol + i - R;
+                if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
+                cs = __fadd_rn(cs, x);
+            }
+            xg[idx] = lw_div(gs, c.gnorm, c.zh_g, c.zl_g, fast);
+            xb[idx] = cs;
+        }
     }
     __syncwarp();
     const float trunc_thr = 1.0f / 255.0f;
@@ -590,17 +621,18 @@ __device__ void lw_passes(const LocateConsts& c, int cu, int cv, float* patch, c
         const int pr = idx / PS, pc = idx - pr * PS;
         const int grow = r0 + pr, gcol = c0 + pc;
         float res = 0.0f;
-        if (grow >= 0 && grow < H && gcol >= 0 && gcol < W) {
+        if (interior || (grow >= 0 && grow < H && gcol >= 0 && gcol < W)) {
             // raw row (pr + i) holds row clamp(grow + i - R): the row pass of a
             // clamped row is the row pass of the edge row
             float gs = 0.0f, cs = 0.0f;
+#pragma unroll
             for (int i = 0; i <= 2 * R; i++) {
                 const int gr = grow + i - R;
                 const int xr = (pr + i) * PS + pc;
-                if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], xg[xr], gs);
+                if (interior || (gr >= 0 && gr < H)) gs = __fmaf_rn(c.taps[i], xg[xr], gs);
                 cs = __fadd_rn(cs, xb[xr]);
             }
-            res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
+            res = __fsub_rn(lw_div(gs, c.gnorm, c.zh_g, c.zl_g, fast), lw_div(cs, c.kk, c.zh_k, c.zl_k, fast));
             if (c.truncate && res < trunc_thr) res = 0.0f;
         }
         patch[idx] = res;
@@ -690,7 +722,7 @@ __device__ __forceinline__ void lw_characterize(const float* pc, int stride, con
     *ec_ = ec;
 }
 
-template <typename T, int RI>
+template <typename T, int RI, int RC>
 __global__ void __launch_bounds__(32 * kLwWarps)
 walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const LocateConsts c,
                   const uint32_t* __restrict__ cand_count, const uint32_t* __restrict__ cand_keys, uint32_t cand_cap,
@@ -700,22 +732,22 @@ walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const Loca
     extern __shared__ float lsm[];
     constexpr int PS = lw_patch(RI);
     constexpr int OFF = RI + kLwShift;
-    const int R = c.R, RW = PS + 2 * R;
+    const int R = RC > 0 ? RC : c.R, RW = PS + 2 * R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = blockIdx.y;
     const uint32_t n = min(cand_count[f], cand_cap);
-    const uint32_t first = (blockIdx.x * kLwWarps + warp) * 32u;
+    const uint32_t first = (blockIdx.x * kLwWarps + warp) * (uint32_t)kLwSeeds;
     if (first >= n) return;  // warp-uniform
     float* wbase = lsm + (size_t)warp * lw_warp_floats(RI, R);
     float* patches = wbase;
-    float* raw = wbase + 32 * PS * PS;
+    float* raw = wbase + kLwSeeds * PS * PS;
     float* xg = raw + RW * RW;
     float* xb = xg + RW * PS;
-    float* my = patches + lane * PS * PS;
+    float* my = patches + (lane < kLwSeeds ? lane : 0) * PS * PS;
     const int H = c.H, W = c.W;
     const T* img = frames + (size_t)f * frame_stride;
     const uint32_t i = first + lane;
-    const bool active = i < n;
+    const bool active = lane < kLwSeeds && i < n;
     const uint32_t key = active ? cand_keys[(size_t)f * cand_cap + i] : 0u;
     int pu = (int)(key / (uint32_t)W), pv = (int)(key % (uint32_t)W);
     int stage = active ? 0 : 2;  // 0 walk, 1 characterize, 2 done
@@ -733,15 +765,15 @@ walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const Loca
             LwRaw<RI> reg;
             int k = __ffs(needmask) - 1;
             int cu = __shfl_sync(0xffffffffu, want_u, k), cv = __shfl_sync(0xffffffffu, want_v, k);
-            lw_raw_load<T, RI>(img, c, cu, cv, reg, lane);
+            lw_raw_load<T, RI, RC>(img, c, cu, cv, reg, lane);
             for (unsigned m = needmask; m;) {
                 m &= m - 1u;
-                lw_raw_store<RI>(reg, c, raw, lane);
+                lw_raw_store<RI, RC>(reg, c, raw, lane);
                 __syncwarp();
                 const int kn = m ? __ffs(m) - 1 : 0;
                 const int nu = __shfl_sync(0xffffffffu, want_u, kn), nv = __shfl_sync(0xffffffffu, want_v, kn);
-                if (m) lw_raw_load<T, RI>(img, c, nu, nv, reg, lane);
-                lw_passes<RI>(c, cu, cv, patches + k * PS * PS, raw, xg, xb, lane);
+                if (m) lw_raw_load<T, RI, RC>(img, c, nu, nv, reg, lane);
+                lw_passes<RI, RC>(c, cu, cv, patches + k * PS * PS, raw, xg, xb, lane);
                 k = kn;
                 cu = nu;
                 cv = nv;
@@ -1366,17 +1398,26 @@ cudaError_t launch_walk_local(const T* frames, int64_t frame_stride, const Locat
     if (cand_cap == 0 || nframes == 0) return cudaSuccess;
     const int ri = (c.circle - 1) / 2;
     const size_t smem = walk_local_smem_bytes(c.circle, c.R);
-    dim3 grid((cand_cap + 32 * kLwWarps - 1) / (32 * kLwWarps), nframes);
-#define GT_WALK_LOCAL(RI)                                                                                        \
-    if (ri == RI) {                                                                                              \
-        cudaFuncSetAttribute(walk_local_kernel<T, RI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-        walk_local_kernel<T, RI><<<grid, 32 * kLwWarps, smem, st>>>(frames, frame_stride, c, cand_count,         \
-                                                                    cand_keys, cand_cap, angle_off, angles,      \
-                                                                    feats, feat_count, feat_cap, flags);          \
-        return cudaGetLastError();                                                                               \
+    dim3 grid((cand_cap + kLwSeeds * kLwWarps - 1) / (kLwSeeds * kLwWarps), nframes);
+    // the smoothing radius unrolled where it is the circle radius or one more
+    // (smoothing_size = diameter, its default), looped otherwise
+#define GT_WALK_LOCAL_RC(RI, RC)                                                                                     \
+    {                                                                                                                \
+        cudaFuncSetAttribute(walk_local_kernel<T, RI, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        walk_local_kernel<T, RI, RC><<<grid, 32 * kLwWarps, smem, st>>>(frames, frame_stride, c, cand_count,         \
+                                                                        cand_keys, cand_cap, angle_off, angles,      \
+                                                                        feats, feat_count, feat_cap, flags);          \
+        return cudaGetLastError();                                                                                   \
+    }
+#define GT_WALK_LOCAL(RI)                                \
+    if (ri == RI) {                                      \
+        if (c.R == RI) GT_WALK_LOCAL_RC(RI, RI)          \
+        if (c.R == RI + 1) GT_WALK_LOCAL_RC(RI, RI + 1)  \
+        GT_WALK_LOCAL_RC(RI, 0)                          \
     }
     GT_WALK_LOCAL(2) GT_WALK_LOCAL(3) GT_WALK_LOCAL(4) GT_WALK_LOCAL(5) GT_WALK_LOCAL(6) GT_WALK_LOCAL(7)
 #undef GT_WALK_LOCAL
+#undef GT_WALK_LOCAL_RC
     return cudaErrorInvalidValue;
 }
 
