@@ -404,6 +404,19 @@ def run_learned(args):
     kw = dict(minmass=cfg["minmass"], search_range=cfg["search_range"], memory=cfg["memory"], tqdm=False)
     score = learned.compare(gt.batch(video, cfg["diameter"], **kw),
                             learned.batch_learned(video, cfg["diameter"], net, **kw))
+    # the locate stage alone (no linking): where the seeds replace the bandpass local maxima
+    p_loc = trackpy_params(cfg["diameter"], minmass=cfg["minmass"])
+
+    def plain_loc(out):
+        return L.gt_batch(ctx.handle, ctypes.byref(p_loc), ctypes.c_void_p(video.data_ptr()), DTYPE_U16, T, S, S,
+                          None, None, 0, out)
+
+    def learned_loc(out):
+        return L.gt_batch_learned(ctx.handle, ctypes.byref(p_loc), net.handle, ctypes.c_void_p(video.data_ptr()),
+                                  DTYPE_U16, T, S, S, None, None, 0, out)
+
+    ms_pl, _, _, _, _ = timed(plain_loc, ())
+    ms_ll, _, _, _, _ = timed(learned_loc, ())
 
     pk = {}
     try:
@@ -437,6 +450,8 @@ def run_learned(args):
                         "hbm_frac_whole_step": T * bytes_per_frame_l / (ms_l / 1000.0) / 1e9 / hbm_peak,
                         "threshold": thr, "calibration": curve},
             "speedup_learned_over_plain": ms_p / ms_l,
+            "locate_only": {"plain": T / (ms_pl / 1000.0), "learned": T / (ms_ll / 1000.0), "unit": "frames/s",
+                            "speedup_learned_over_plain": ms_pl / ms_ll},
             "score_vs_plain": score,
             "training": {"steps": steps, "seconds": train_s, "loss_first": loss[:20].mean(0).tolist(),
                          "loss_last": loss[-20:].mean(0).tolist(), "setup_seconds": setup_s},

@@ -288,8 +288,12 @@ cudaError_t conv_launch(const __nv_bfloat16* in, int nimg, int Hc, int Wc, const
     CUtensorMap tm;
     cudaError_t e = plane_map(&tm, in, nimg, G::PLANES, Hc, Wc);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(conv3x3_kernel<KS, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-    if (e != cudaSuccess) return e;
+    static bool attr_set = false;  // once per instantiation (per process; one device at a time)
+    if (!attr_set) {
+        e = cudaFuncSetAttribute(conv3x3_kernel<KS, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
     // persistent: at most 2 CTAs per SM, 2 x 128 of the 512 TMEM columns
     static_assert(2 * G::SMEM <= 227 * 1024, "two CTAs per SM");
     const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms * 2);
