@@ -60,6 +60,7 @@ def parse():
                          "learned: plain vs learned-proposal seeds on 1000 frames of 2048^2 at 4000 spots/frame")
     ap.add_argument("--learned-scale", type=float, default=1.0, help="learned: fraction of the 1000 frames timed")
     ap.add_argument("--epochs", type=float, default=3.0, help="learned: passes over the 200k training crops")
+    ap.add_argument("--train-frames", type=int, default=800, help="learned: labelled frames the crops come from")
     ap.add_argument("--scale", type=float, default=0.25,
                     help="ragged: fraction of the configured 50-1000 frames per video")
     return ap.parse_args()
@@ -328,7 +329,7 @@ def run_learned(args):
 
     # training: frames of the 2000-spot generator labelled by the plain method
     t_start = time.perf_counter()
-    train = brownian_video(800, S, S, 2000, seed=101, device="cuda:0", snr_range=(3.0, 20.0), **gen)
+    train = brownian_video(args.train_frames, S, S, 2000, seed=101, device="cuda:0", snr_range=(3.0, 20.0), **gen)
     labels = gt.batch(train, cfg["diameter"], minmass=cfg["minmass"], tqdm=False)
     net = learned.ProposalNet(seed=1)
     net.fit_normalization(train)
@@ -439,7 +440,7 @@ def run_learned(args):
     line = {"metric": METRIC, "value": T / (ms_l / 1000.0), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16 network, f32 walk", "data": "synthetic",
-            "config": dict(cfg, frames=T, epochs=epochs, train_steps=steps,
+            "config": dict(cfg, frames=T, epochs=epochs, train_steps=steps, train_frames=args.train_frames,
                            l2="inputs (%.1f GB) larger than L2; no flush" % (T * S * S * 2 / 1e9)),
             "features_per_s": rows_l / (ms_l / 1000.0),
             "plain": {"value": T / (ms_p / 1000.0), "ms_per_step": ms_p, "features_per_s": rows_p / (ms_p / 1000.0),
