@@ -18,7 +18,7 @@ STATUS_NAMES = {
     1: "InvalidArgument", 2: "DimensionMismatch", 3: "EmptyIterator", 4: "NonSortedCharacterization",
     5: "FrameOutOfBounds", 6: "NonStandardArrayLayout", 7: "ArrayDimensionsError", 8: "TooDenseToLink",
     9: "Interrupted", 10: "CapacityExceeded", 11: "CudaError", 12: "NoDevice", 13: "SubnetTooExpensive",
-    14: "Internal",
+    14: "Internal", 15: "FileNotFound", 16: "ReadError",
 }
 
 _lib = None
@@ -40,6 +40,10 @@ def to_exception(status, message):
         return KeyboardInterrupt(message)
     if status == 12:
         return ConnectionError(message)
+    if status == 15:
+        return FileNotFoundError(message)
+    if status == 16:
+        return ValueError(message)
     if status in (1, 2, 3, 4, 5, 6, 7, 8, 10):
         return ValueError(message)
     return GpuTrackingError(status, message)
@@ -99,6 +103,14 @@ def lib():
                                         P(f32)]
         L.gt_proposal_maps.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(f32)]
         L.gt_batch_learned.argtypes = [vp, P(GtParams), vp, vp, i32, i64, i32, i32, P(i64), P(i64), i64, P(vp)]
+        L.gt_video_open.argtypes = [ctypes.c_char_p, i32, P(vp)]
+        L.gt_video_open.restype = i32
+        L.gt_video_info.argtypes = [vp, P(i64), P(i32), P(i32), P(i32)]
+        L.gt_video_info.restype = i32
+        L.gt_video_read.argtypes = [vp, P(i64), i64, i32, vp]
+        L.gt_video_read.restype = i32
+        L.gt_video_close.argtypes = [vp]
+        L.gt_video_last_error.restype = ctypes.c_char_p
         L.gt_last_walk_starts.argtypes = [vp]
         L.gt_last_walk_starts.restype = i64
         L.gt__proposal_loss_grad.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(i64), P(f32), P(f32), i64, P(i32), i32,

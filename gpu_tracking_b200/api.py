@@ -39,11 +39,18 @@ def _pandas():
 class _Frames:
     """A (T, H, W) video as the C ABI sees it: pointer, dtype code, shape."""
 
-    def __init__(self, obj, frames=None):
+    def __init__(self, obj, frames=None, channel=None):
         self.keep = None
         self.frame_numbers = None
         if isinstance(obj, (str, os.PathLike)):
-            obj = load(obj)
+            if os.path.splitext(os.fspath(obj))[1].lower() in _VIDEO_EXT:
+                # decoded in the file's own dtype (u8/u16 stay integers)
+                obj = _read_video(obj, frames, channel)
+                if frames is not None:
+                    self.frame_numbers = np.asarray([int(k) for k in frames], np.int64)
+                    frames = None
+            else:
+                obj = load(obj)
         if hasattr(obj, "data_ptr") and hasattr(obj, "is_cuda") and obj.is_cuda:
             self._from_tensor(obj, frames)
             return
@@ -159,7 +166,7 @@ def _table_to_frame(ctx, handle, params, has_r=None):
 
 def _locate(video, params, kw):
     ctx = _ffi.context(_DEVICE)
-    fr = _Frames(video, kw.get("frames"))
+    fr = _Frames(video, kw.get("frames"), kw.get("channel"))
     fn = None
     if fr.frame_numbers is not None:
         fn = fr.frame_numbers
@@ -344,23 +351,52 @@ def connect(to_link1, to_link2, search_range, merge=True):
     return output1.merge(output2, how="outer", on="connect particle")
 
 
-def load(path, frames=None, channel=None):
-    """Load a video as a (T, Y, X) array (lib.py:174-186).
+_VIDEO_EXT = (".tif", ".tiff", ".ets", ".vsi")
 
-    ``.npy`` files are read with numpy; the reference's TIFF and Olympus
-    .ets/.vsi decoders are not part of this engine.
+
+def _read_video(path, frames=None, channel=None, as_float=False):
+    """Decode a .tif/.tiff/.ets/.vsi video with the engine's frame providers
+    (host-side); (T, Y, X) in the file's dtype, or float32."""
+    L = _ffi.lib()
+    h = ctypes.c_void_p()
+    st = L.gt_video_open(os.fsencode(os.fspath(path)), int(channel or 0), ctypes.byref(h))
+    if st != _ffi.GT_OK:
+        raise _ffi.to_exception(st, L.gt_video_last_error().decode())
+    try:
+        T, H, W, dt = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        L.gt_video_info(h, ctypes.byref(T), ctypes.byref(H), ctypes.byref(W), ctypes.byref(dt))
+        keys = None if frames is None else np.ascontiguousarray([int(k) for k in frames], np.int64)
+        n = T.value if keys is None else len(keys)
+        code = DTYPE_F32 if as_float else dt.value
+        np_dtype = {DTYPE_U16: np.uint16, DTYPE_U8: np.uint8, DTYPE_F32: np.float32}[code]
+        out = np.empty((n, H.value, W.value), np_dtype)
+        st = L.gt_video_read(h, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)) if keys is not None else None,
+                             n, code, ctypes.c_void_p(out.ctypes.data))
+        if st != _ffi.GT_OK:
+            raise _ffi.to_exception(st, L.gt_video_last_error().decode())
+        return out
+    finally:
+        L.gt_video_close(h)
+
+
+def load(path, frames=None, channel=None):
+    """Load a video as a (T, Y, X) float32 array (lib.py:174-186, load_rust
+    python_bindings.rs:223-270).
+
+    .tif/.tiff stacks and Olympus .ets/.vsi files (``channel``, default 0)
+    are decoded by the engine's frame providers; ``.npy`` files are read with
+    numpy (kept in their dtype).  ``frames`` selects frame indices.
     """
-    del channel
     path = os.fspath(path)
     ext = os.path.splitext(path)[1].lower()
     if ext == "":
         raise ValueError("could not determine extension of file '%s'" % path)
-    if ext not in (".npy", ".tif", ".tiff", ".vsi", ".ets"):
+    if ext not in (".npy",) + _VIDEO_EXT:
         raise ValueError("unsupported file format: %s" % ext.lstrip("."))
-    if not os.path.exists(path):
+    if ext != ".vsi" and not os.path.exists(path):
         raise FileNotFoundError("could not find file '%s'" % path)
-    if ext != ".npy":
-        raise ValueError("%s decoding is not part of this engine; load the video into a numpy array" % ext)
+    if ext in _VIDEO_EXT:
+        return _read_video(path, frames, channel, as_float=True)
     arr = np.load(path, mmap_mode="r")
     if arr.ndim == 2:
         arr = arr[None]
@@ -371,8 +407,7 @@ def load(path, frames=None, channel=None):
 
 def mean_from_file(path, channel=None):
     """Mean frame of a video file (lib.py:161-172), computed on the GPU."""
-    arr = load(path, channel=channel) if isinstance(path, (str, os.PathLike)) else np.asarray(path)
-    fr = _Frames(arr)
+    fr = _Frames(path, None, channel)
     ctx = _ffi.context(_DEVICE)
     out = np.empty((fr.H, fr.W), np.float32)
     ctx.check(_ffi.lib().gt_mean_frame(ctx.handle, fr.ptr, fr.dtype, fr.T, fr.H, fr.W,

@@ -50,7 +50,9 @@ typedef enum gt_status {
     GT_ERR_CUDA = 11,                     /* ~ Error::GpuDeviceError                  (src/error.rs:11)  */
     GT_ERR_NO_DEVICE = 12,                /* ~ Error::GpuAdapterError                 (src/error.rs:8)   */
     GT_ERR_SUBNET_TOO_EXPENSIVE = 13,     /* device subnet search exceeded its step budget (no ref analogue) */
-    GT_ERR_INTERNAL = 14
+    GT_ERR_INTERNAL = 14,
+    GT_ERR_FILE_NOT_FOUND = 15,           /* Error::FileNotFound / InvalidFileName    (src/error.rs)      */
+    GT_ERR_READ = 16                      /* Error::ReadError / CastError / UnsupportedFileformat         */
 } gt_status;
 
 /* ------------------------------------------------------------- parameters */
@@ -283,6 +285,26 @@ GT_API gt_status gt_batch_learned(gt_ctx* ctx, const gt_params* params, const gt
 /* Walk starts (bandpass candidates or learned seeds) of the last gt_batch /
  * gt_batch_learned call on this context, summed over its frames. */
 GT_API int64_t gt_last_walk_starts(const gt_ctx* ctx);
+
+/* ------------------------------------------------------------ video files
+ * Frame providers of path_to_iter (src/execute_gpu.rs:1186-1270,
+ * src/decoderiter.rs:64-481): .tif/.tiff stacks (every image in IFD order;
+ * classic or BigTIFF, strips or tiles, one sample per pixel, 8/16-bit
+ * integers or 32-bit floats, uncompressed / PackBits / LZW / Deflate, with or
+ * without horizontal differencing), Olympus .ets (one channel's frames) and
+ * .vsi (the .ets at _<stem>_/stack1/frame_t_0.ets beside it).  Host-side
+ * decoding, no device needed.  u8 and u16 files keep their dtype; other
+ * sample types decode to f32.
+ */
+typedef struct gt_video gt_video;
+GT_API gt_status gt_video_open(const char* path, int32_t channel, gt_video** out);
+GT_API gt_status gt_video_info(const gt_video* v, int64_t* T, int32_t* H, int32_t* W, int32_t* dtype);
+/* Decode frames (frame indices, or the first n when frames is NULL) into dst,
+ * (n, H, W) of `dtype` (the video's own dtype or GT_DTYPE_F32). */
+GT_API gt_status gt_video_read(gt_video* v, const int64_t* frames, int64_t n, int32_t dtype, void* dst);
+GT_API void gt_video_close(gt_video* v);
+/* Message of the last failing gt_video_* call of this thread. */
+GT_API const char* gt_video_last_error(void);
 
 /* Library version string. */
 GT_API const char* gt_version(void);
