@@ -58,7 +58,7 @@ struct ConvGeom {
     static constexpr int B_BYTES = 9 * KS * (N / 8) * 256;
     static constexpr int SMEM = 128 + NSTAGE * STAGE + B_BYTES + 128 + 8 * (2 * NSTAGE + 2 * NACC) + 16;
 };
-constexpr int kConvWsThreads = 192;  // warp 0 loads, warp 1 issues, warps 2-5 drain
+constexpr int kConvWsThreads = 320;  // warp 0 loads, warp 1 issues, warps 2-5 and 6-9 drain alternate tiles
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -102,18 +102,20 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
 
+    // tile counts fit in 32 bits (conv_launch checks)
     const int ntx = (Wc + kConvCols - 1) / kConvCols, nty = (Hc + kConvRows - 1) / kConvRows;
-    const int64_t per_img = (int64_t)nty * ntx;
-    const int64_t ntiles = (int64_t)nimg * per_img;
-    const int64_t t0 = blockIdx.x, stride = gridDim.x;
+    const int per_img = nty * ntx;
+    const int ntiles = nimg * per_img;
+    const int t0 = blockIdx.x, stride = gridDim.x;
     // this CTA's tiles are t0 + k * stride, k = 0 .. nmine - 1
-    const int nmine = t0 < ntiles ? (int)((ntiles - 1 - t0) / stride) + 1 : 0;
+    const int nmine = t0 < ntiles ? (ntiles - 1 - t0) / stride + 1 : 0;
     auto tile_pos = [&](int k, int& img, int& y0, int& x0) {
-        const int64_t tile = t0 + (int64_t)k * stride;
-        img = (int)(tile / per_img);
-        const int rem = (int)(tile - (int64_t)img * per_img);
-        y0 = (rem / ntx) * kConvRows;
-        x0 = (rem % ntx) * kConvCols;
+        const int tile = t0 + k * stride;
+        img = tile / per_img;
+        const int rem = tile - img * per_img;
+        const int ty = rem / ntx;
+        y0 = ty * kConvRows;
+        x0 = (rem - ty * ntx) * kConvCols;
     };
 
     if (warp == 0) {
@@ -129,7 +131,8 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
                 int img, y0, x0;
                 tile_pos(k, img, y0, x0);
                 tc::mbar_arrive_expect_tx(full + st, G::PLANES * G::PLANE);
-                tc::tma_load_4d(S0 + st * G::STAGE, &tin, 0, x0 - 1, y0 - 1, img * G::PLANES, full + st);
+                // innermost coordinate: element (x0 - 1) * 8 of the flattened row, 16-byte aligned
+                tc::tma_load_3d(S0 + st * G::STAGE, &tin, (x0 - 1) * 8, y0 - 1, img * G::PLANES, full + st);
             }
             // no load may still be landing when the CTA leaves
             for (int j = max(0, k - NS); j < k; j++)
@@ -173,9 +176,10 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
                 tc::mbar_wait_bounded(accf + j % NA, (uint32_t)((j / NA) & 1), kConvPolls);
         }
     } else {
-        // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 = tile rows 4 * (w % 4) .. + 3
-        const int sub = warp & 3;
-        for (int k = 0; k < nmine; k++) {
+        // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 = tile rows 4 * (w % 4) .. + 3;
+        // warps 2-5 take the even tiles, warps 6-9 the odd ones
+        const int sub = warp & 3, grp = (warp - 2) >> 2;
+        for (int k = grp; k < nmine; k += 2) {
             const int ab = k % NA;
             const bool ready = tc::mbar_wait_bounded(accf + ab, (uint32_t)((k / NA) & 1), kConvPolls);
             if (!__all_sync(0xffffffffu, ready)) {
@@ -246,9 +250,10 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tin, int nimg, int Hc, int Wc
     if (warp == 0) tc::tmem_dealloc(tmem, 32 * NA);
 }
 
-// The tensor map of a BF16 plane tensor [planes_total][Hc][Wc][8] whose box
-// is one tile with its halo: 8 channels x 10 cells x 18 rows x planes_per_img
-// planes.
+// The tensor map of a BF16 plane tensor [planes_total][Hc][Wc][8] seen as
+// [planes_total][Hc][Wc * 8] (a plane row's cells and channels are one
+// contiguous run): the box is one tile with its halo, 10 cells x 8 channels
+// = 160 bytes per row, x 18 rows x planes_per_img planes.
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -268,11 +273,11 @@ cudaError_t plane_map(CUtensorMap* m, const void* base, int nimg, int planes_per
     PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
     if (!fn) return cudaErrorNotSupported;
     if (((uintptr_t)base & 15u) != 0u) return cudaErrorMisalignedAddress;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)Wc, (cuuint64_t)Hc, (cuuint64_t)nimg * planes_per_img};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)Wc * 16, (cuuint64_t)Hc * Wc * 16};
-    const cuuint32_t box[4] = {8, (cuuint32_t)(kConvCols + 2), (cuuint32_t)(kConvRows + 2), (cuuint32_t)planes_per_img};
-    const cuuint32_t es[4] = {1, 1, 1, 1};
-    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+    const cuuint64_t dims[3] = {(cuuint64_t)Wc * 8, (cuuint64_t)Hc, (cuuint64_t)nimg * planes_per_img};
+    const cuuint64_t strides[2] = {(cuuint64_t)Wc * 16, (cuuint64_t)Hc * Wc * 16};
+    const cuuint32_t box[3] = {(cuuint32_t)(kConvCols + 2) * 8, (cuuint32_t)(kConvRows + 2), (cuuint32_t)planes_per_img};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
@@ -285,6 +290,7 @@ cudaError_t conv_launch(const __nv_bfloat16* in, int nimg, int Hc, int Wc, const
     const int64_t ntiles =
         (int64_t)nimg * ((Hc + kConvRows - 1) / kConvRows) * ((Wc + kConvCols - 1) / kConvCols);
     if (ntiles == 0) return cudaSuccess;
+    if (ntiles > INT32_MAX) return cudaErrorInvalidValue;
     CUtensorMap tm;
     cudaError_t e = plane_map(&tm, in, nimg, G::PLANES, Hc, Wc);
     if (e != cudaSuccess) return e;

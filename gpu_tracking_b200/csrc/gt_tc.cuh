@@ -113,6 +113,15 @@ __device__ __forceinline__ void tma_load_4d(void* smem_dst, const void* tmap, in
         : "memory");
 }
 
+// TMA tile load of a 3-D box (no multicast); as tma_load_4d.
+__device__ __forceinline__ void tma_load_3d(void* smem_dst, const void* tmap, int c0, int c1, int c2, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_addr(smem_dst)),
+        "l"((uint64_t)tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(mbar))
+        : "memory");
+}
+
 // Warp-wide loads of 32-bit TMEM cells: lane i of the warp reads TMEM lane
 // (base lane + i), columns col .. col + n - 1, into r[0..n).
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
