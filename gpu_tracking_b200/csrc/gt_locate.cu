@@ -509,16 +509,18 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
 // evaluated with the operation order of bandpass_kernel (clamped raw rows and
 // columns, Gaussian taps skipped outside the frame, sequential sums, IEEE
 // division), so every value equals the full-frame one bit for bit.  Each lane
-// then moves its seed to the largest processed value of the 3x3 block around
-// it (inside the candidate margin; the seed itself wins ties, then row-major
-// order) -- a bandpass local maximum, the kind of pixel the plain method
-// starts its walks from -- and walks and characterizes from there with the
+// then climbs from its seed to a 3x3 local maximum of the processed image
+// (inside the candidate margin; the current pixel wins ties, then row-major
+// order; at most kLwClimb steps) -- a bandpass local maximum, the kind of
+// pixel the plain method starts its walks from -- and walks and
+// characterizes from there with the
 // operation sequence of walk_kernel_fixed, reading its patch.  A lane whose
 // walk or characterize circle leaves the patch asks for a patch centred
 // where it stands and resumes there.
 constexpr int kLwWarps = 4;
 constexpr int kLwSeeds = 16;  // seeds per warp (lanes 0-15); all 32 lanes build the patches
 constexpr int kLwShift = 1;   // walk steps a patch covers around its centre
+constexpr int kLwClimb = 4;   // hill-climbing steps of a seed before its walk
 
 __host__ __device__ constexpr int lw_patch(int RI) { return 2 * (RI + kLwShift) + 1; }
 __host__ __device__ constexpr int lw_warp_floats(int RI, int R) {
@@ -785,23 +787,29 @@ walk_local_kernel(const T* __restrict__ frames, int64_t frame_stride, const Loca
             need = false;
         }
         if (stage == 0 && !need && it == 0 && pu == cen_u && pv == cen_v && !snapped) {
+            // climb to a 3x3 local maximum of the processed image (at most
+            // kLwClimb steps, every 3x3 block inside the patch)
             snapped = true;
-            const float* pc = my + OFF * PS + OFF;
-            float best = pc[0];
-            int bu = 0, bv = 0;
-            for (int di = -1; di <= 1; di++)
-                for (int dj = -1; dj <= 1; dj++) {
-                    const int u = pu + di, v = pv + dj;
-                    if (u < c.margin || u >= H - c.margin || v < c.margin || v >= W - c.margin) continue;
-                    const float val = pc[di * PS + dj];
-                    if (val > best) {
-                        best = val;
-                        bu = di;
-                        bv = dj;
+            for (int step = 0; step < kLwClimb; step++) {
+                const float* pc = my + (pu - cen_u + OFF) * PS + (pv - cen_v + OFF);
+                float best = pc[0];
+                int bu = 0, bv = 0;
+                for (int di = -1; di <= 1; di++)
+                    for (int dj = -1; dj <= 1; dj++) {
+                        const int u = pu + di, v = pv + dj;
+                        if (u < c.margin || u >= H - c.margin || v < c.margin || v >= W - c.margin) continue;
+                        const float val = pc[di * PS + dj];
+                        if (val > best) {
+                            best = val;
+                            bu = di;
+                            bv = dj;
+                        }
                     }
-                }
-            pu += bu;
-            pv += bv;
+                if (bu == 0 && bv == 0) break;
+                if (abs(pu + bu - cen_u) > OFF - 1 || abs(pv + bv - cen_v) > OFF - 1) break;
+                pu += bu;
+                pv += bv;
+            }
         }
         if (stage == 0) {
             bool fin = false;
