@@ -1063,12 +1063,12 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     lc.snr = c.snr;
     lc.rough = c.rough;
 
-    // learned proposals: the network runs on groups of cnn_g frames, about
-    // 80 MB of activations (64 B per 4x4 cell) per layer, so most of a layer's
-    // input is still in L2 when the next layer reads it
+    // learned proposals: the network runs on groups of cnn_g frames (about
+    // 160 MB of activations per layer at 64 B per 4x4 cell): long persistent
+    // launches, part of each layer's input still in L2 for the next
     const int Hc = (H + 3) / 4, Wc = (W + 3) / 4;
     const size_t cells = (size_t)Hc * Wc;
-    const int cnn_g = net ? (int)std::max<size_t>(1, std::min<size_t>((size_t)F, (80u << 20) / (cells * 64))) : 0;
+    const int cnn_g = net ? (int)std::max<size_t>(1, std::min<size_t>((size_t)F, (160u << 20) / (cells * 64))) : 0;
     if (net) {
         CK(ctx->cnn_x.ensure((size_t)cnn_g * cells * 32));
         CK(ctx->cnn_p.ensure((size_t)cnn_g * cells * 64));
