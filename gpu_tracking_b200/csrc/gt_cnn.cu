@@ -33,6 +33,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "gt_internal.cuh"
@@ -294,11 +295,15 @@ cudaError_t conv_launch(const __nv_bfloat16* in, int nimg, int Hc, int Wc, const
     CUtensorMap tm;
     cudaError_t e = plane_map(&tm, in, nimg, G::PLANES, Hc, Wc);
     if (e != cudaSuccess) return e;
-    static bool attr_set = false;  // once per instantiation (per process; one device at a time)
-    if (!attr_set) {
+    // once per instantiation and device
+    static std::atomic<uint64_t> attr_set{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
         e = cudaFuncSetAttribute(conv3x3_kernel<KS, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set.fetch_or(bit);
     }
     // persistent: at most 2 CTAs per SM, 2 x 128 of the 512 TMEM columns
     static_assert(2 * G::SMEM <= 227 * 1024, "two CTAs per SM");
