@@ -10,7 +10,7 @@
 // Pinning.  The shader stages restated here (preprocess, extract_max, walk,
 // characterize, separable LoG, logspace_max) are pinned bit-for-bit against
 // the reference's own WGSL source executed on the CPU: oracle/wgsl2cpp.py
-// translates /root/reference/src/shaders/*.wgsl into C++ at build time
+// translates the reference checkout's src/shaders/*.wgsl into C++ at build time
 // (output only under oracle/_ref/, never committed) and tests compare both.
 // The Rust post-processing (filter_close, doughnut, prune_blobs_log) and the
 // linker cannot be executed here (no Rust toolchain); they are pinned only by
