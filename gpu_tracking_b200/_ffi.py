@@ -79,6 +79,7 @@ def lib():
         L.gt_table_nrows.restype = i64
         L.gt_table_column_f32.argtypes = [vp, i32, P(f32)]
         L.gt_table_column_i64.argtypes = [vp, i32, P(i64)]
+        L.gt_table_export.argtypes = [vp, P(i32), i32, P(vp)]
         L.gt_table_has_column.argtypes = [vp, i32]
         L.gt_table_has_column.restype = i32
         L.gt_table_free.argtypes = [vp]
@@ -116,7 +117,7 @@ def lib():
         L.gt__proposal_loss_grad.argtypes = [vp, vp, vp, i32, i64, i32, i32, P(i64), P(f32), P(f32), i64, P(i32), i32,
                                              i32, f32, f32, P(f32), P(f32)]
         for name in ("gt_create", "gt_set_interrupt", "gt_progress", "gt_table_column_f32", "gt_table_column_i64",
-                     "gt_batch", "gt_batch_videos", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
+                     "gt_table_export", "gt_batch", "gt_batch_videos", "gt_characterize_points", "gt_link", "gt_connect", "gt_mean_frame",
                      "gt_profile_enable", "gt_profile_read", "gt_proposal_create", "gt_proposal_set",
                      "gt_proposal_get", "gt_proposal_train", "gt_proposal_maps", "gt_batch_learned",
                      "gt__proposal_loss_grad"):

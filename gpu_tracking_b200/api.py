@@ -144,24 +144,17 @@ def _table_to_frame(ctx, handle, params, has_r=None):
         cols = column_names(params)
         if has_r is not None and not has_r:
             cols = [c for c in cols if c[0] != "r"]
-        data = {}
-        for name, ty in cols:
-            idx = COLUMN_INDEX[name]
-            if ty == "int":
-                v = np.empty(n, np.int64)
-                if n:
-                    ctx.check(L.gt_table_column_i64(handle, idx, v.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
-            else:
-                v32 = np.empty(n, np.float32)
-                if n:
-                    ctx.check(L.gt_table_column_f32(handle, idx,
-                                                    v32.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
-                v = v32.astype(np.float64)
-            data[name] = v
+        # the DataFrame's own dtypes (int64 / float64) filled by one library
+        # call; the frame takes the arrays as they are, without a copy
+        data = {name: np.empty(n, np.int64 if ty == "int" else np.float64) for name, ty in cols}
+        if n and cols:
+            idx = (ctypes.c_int32 * len(cols))(*[COLUMN_INDEX[name] for name, _ in cols])
+            ptrs = (ctypes.c_void_p * len(cols))(*[data[name].ctypes.data for name, _ in cols])
+            ctx.check(L.gt_table_export(handle, idx, len(cols), ptrs))
     finally:
         L.gt_table_free(handle)
     pd = _pandas()
-    return pd.DataFrame(data, columns=[c[0] for c in cols])
+    return pd.DataFrame(data, columns=[c[0] for c in cols], copy=False)
 
 
 def _locate(video, params, kw):

@@ -10,6 +10,7 @@
 //     on the device and copied out column by column on request;
 //   * capacities (candidates / detections per frame) grow and the call is
 //     replayed when a kernel reports an overflow, so nothing is truncated.
+#include <cuda.h>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -24,6 +25,7 @@
 #include <mutex>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gt_kernels.h"
@@ -500,7 +502,31 @@ LogTables log_tables(const gt_params& p) {
     return t;
 }
 
-gt_status check_frames_ptr(gt_ctx* ctx, const void* frames, bool* on_device) {
+size_t dtype_bytes(int32_t dtype) { return dtype == GT_DTYPE_F32 ? 4 : (dtype == GT_DTYPE_U16 ? 2 : 1); }
+
+// cuMemGetAddressRange through the runtime's driver entry point (no link
+// against libcuda); null when the driver does not offer it.
+typedef CUresult (*AddressRangeFn)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddressRangeFn address_range_fn() {
+    static AddressRangeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* q = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &q, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            fn = (AddressRangeFn)q;
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// Host or device frames; device frames must live on the context's device and
+// the `bytes` the call reads must lie inside the allocation that holds them
+// (a wrong dtype or shape for a device tensor is an error, not a read past
+// the end of its memory).
+gt_status check_frames_ptr(gt_ctx* ctx, const void* frames, size_t bytes, bool* on_device) {
     cudaPointerAttributes at;
     cudaError_t e = cudaPointerGetAttributes(&at, frames);
     if (e != cudaSuccess) {
@@ -513,6 +539,17 @@ gt_status check_frames_ptr(gt_ctx* ctx, const void* frames, bool* on_device) {
             return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "frames live on device %d, context is on device %d",
                            at.device, ctx->device);
         *on_device = true;
+        CUdeviceptr base = 0;
+        size_t size = 0;
+        AddressRangeFn fn = address_range_fn();
+        if (at.type == cudaMemoryTypeDevice && fn && fn(&base, &size, (CUdeviceptr)frames) == CUDA_SUCCESS) {
+            const uint64_t off = (uint64_t)(uintptr_t)frames - (uint64_t)base;
+            if (off > size || bytes > size - off)
+                return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                               "the device frames (%zu bytes from their pointer) run past the end of their "
+                               "allocation (%zu bytes left): check the dtype and shape",
+                               bytes, (size_t)(size - std::min<uint64_t>(off, size)));
+        }
     } else {
         *on_device = false;
     }
@@ -1703,7 +1740,7 @@ gt_status batch_videos_impl(gt_ctx* ctx, const gt_params& p, int32_t n_videos, c
     std::vector<std::vector<int64_t>> row_off((size_t)n_videos);
     for (int32_t v = 0; v < n_videos; v++) {
         bool on_device = false;
-        CKS(check_frames_ptr(ctx, frames[v], &on_device));
+        CKS(check_frames_ptr(ctx, frames[v], (size_t)T_[v] * H_[v] * W_[v] * sizeof(T), &on_device));
         const int64_t NT = T_[v];
         gt_status st = batch_impl<T>(ctx, pl, (const T*)frames[v], on_device, NT, H_[v], W_[v], nullptr, nullptr, 0,
                                      tabs[v]);
@@ -1948,6 +1985,135 @@ gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst) {
     return GT_OK;
 }
 
+namespace {
+
+// Table export: each lane (one host thread) owns two pinned slots and a
+// stream; it copies its share of the rows chunk by chunk into one slot while
+// it widens the previous chunk from the other into the destination.
+constexpr int kExportLanes = 8;
+constexpr size_t kExportSlot = (size_t)1 << 20;
+constexpr int kExportMaxDevices = 64;
+
+struct ExportLane {
+    char* slot[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+struct ExportPool {
+    std::mutex mu;
+    bool ready = false;
+    ExportLane lane[kExportLanes];
+};
+
+// One pool per device for the life of the process (never destroyed: no CUDA
+// call runs from a static destructor after the runtime has shut down).
+ExportPool* export_pool(int device) {
+    static ExportPool* pools = new ExportPool[kExportMaxDevices];
+    return device >= 0 && device < kExportMaxDevices ? &pools[device] : nullptr;
+}
+
+cudaError_t export_pool_init(ExportPool& p) {
+    if (p.ready) return cudaSuccess;
+    char* block = nullptr;
+    cudaError_t e = cudaHostAlloc((void**)&block, 2 * kExportLanes * kExportSlot, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    for (int l = 0; l < kExportLanes; l++) {
+        ExportLane& L = p.lane[l];
+        L.slot[0] = block + (2 * l) * kExportSlot;
+        L.slot[1] = block + (2 * l + 1) * kExportSlot;
+        if ((e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        for (int s = 0; s < 2; s++)
+            if ((e = cudaEventCreateWithFlags(&L.ev[s], cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    p.ready = true;
+    return cudaSuccess;
+}
+
+struct ExportItem {
+    const char* src;   // device rows
+    char* dst;         // host rows
+    int64_t rows;
+    bool widen;        // float32 -> double; otherwise int64 copied as is
+};
+
+cudaError_t export_lane(int device, ExportLane& L, const std::vector<ExportItem>& items) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    auto issue = [&](size_t i) {
+        const ExportItem& it = items[i];
+        const size_t bytes = (size_t)it.rows * (it.widen ? 4 : 8);
+        cudaError_t r = cudaMemcpyAsync(L.slot[i & 1], it.src, bytes, cudaMemcpyDeviceToHost, L.st);
+        return r != cudaSuccess ? r : cudaEventRecord(L.ev[i & 1], L.st);
+    };
+    if (items.empty()) return cudaSuccess;
+    if ((e = issue(0)) != cudaSuccess) return e;
+    for (size_t i = 0; i < items.size(); i++) {
+        // slot (i + 1) & 1 held item i - 1, already widened by this thread
+        if (i + 1 < items.size() && (e = issue(i + 1)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(L.ev[i & 1])) != cudaSuccess) break;
+        const ExportItem& it = items[i];
+        if (it.widen) {
+            const float* s = (const float*)L.slot[i & 1];
+            double* d = (double*)it.dst;
+            for (int64_t j = 0; j < it.rows; j++) d[j] = (double)s[j];
+        } else {
+            memcpy(it.dst, L.slot[i & 1], (size_t)it.rows * 8);
+        }
+    }
+    // nothing may still land in the slots once the pool is handed on
+    cudaError_t e2 = cudaStreamSynchronize(L.st);
+    return e != cudaSuccess ? e : e2;
+}
+
+}  // namespace
+
+gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
+    if (!t || ncolumns < 0 || (ncolumns > 0 && (!columns || !dst))) return GT_ERR_INVALID_ARGUMENT;
+    for (int32_t k = 0; k < ncolumns; k++) {
+        const int32_t c = columns[k];
+        if (c < 0 || c >= GT_NUM_COLUMNS || !t->has[c] || !dst[k]) return GT_ERR_INVALID_ARGUMENT;
+    }
+    const int64_t N = t->n;
+    if (N == 0 || ncolumns == 0) return GT_OK;
+    ExportPool* pool = export_pool(t->device);
+    if (!pool) return GT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(pool->mu);
+    if (cudaSetDevice(t->device) != cudaSuccess || export_pool_init(*pool) != cudaSuccess) return GT_ERR_CUDA;
+    // lanes: one per 256k rows, at most kExportLanes and half the host threads
+    const int hw = std::max(1, (int)std::thread::hardware_concurrency() / 2);
+    const int lanes = (int)std::max<int64_t>(1, std::min<int64_t>({kExportLanes, hw, (N + (1 << 18) - 1) >> 18}));
+    std::vector<std::vector<ExportItem>> work(lanes);
+    for (int l = 0; l < lanes; l++) {
+        const int64_t r0 = N * l / lanes, r1 = N * (l + 1) / lanes;
+        for (int32_t k = 0; k < ncolumns; k++) {
+            const int32_t c = columns[k];
+            const bool integer = c == GT_COL_FRAME || c == GT_COL_PARTICLE || c == GT_COL_DURATION;
+            const TBuf& b = c == GT_COL_FRAME ? t->frame
+                                              : (c == GT_COL_PARTICLE ? t->particle
+                                                                      : (c == GT_COL_DURATION ? t->duration : t->col[c]));
+            const int64_t chunk = (int64_t)(kExportSlot / (integer ? 8 : 4));
+            for (int64_t r = r0; r < r1; r += chunk) {
+                ExportItem it;
+                it.rows = std::min(chunk, r1 - r);
+                it.src = (const char*)b.p + (size_t)r * (integer ? 8 : 4);
+                it.dst = (char*)dst[k] + (size_t)r * 8;
+                it.widen = !integer;
+                work[l].push_back(it);
+            }
+        }
+    }
+    std::vector<cudaError_t> err(lanes, cudaSuccess);
+    std::vector<std::thread> th;
+    for (int l = 1; l < lanes; l++)
+        th.emplace_back([&, l] { err[l] = export_lane(t->device, pool->lane[l], work[l]); });
+    err[0] = export_lane(t->device, pool->lane[0], work[0]);
+    for (auto& x : th) x.join();
+    for (cudaError_t e : err)
+        if (e != cudaSuccess) return GT_ERR_CUDA;
+    return GT_OK;
+}
+
 void gt_table_free(gt_table* t) {
     if (!t) return;
     cudaSetDevice(t->device);
@@ -1961,7 +2127,7 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
     *out = nullptr;
     CKS(validate(ctx, params, frames, dtype, T, H, W));
     bool on_device = false;
-    CKS(check_frames_ptr(ctx, frames, &on_device));
+    CKS(check_frames_ptr(ctx, frames, (size_t)T * H * W * dtype_bytes(dtype), &on_device));
     std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
     gt_status st;
     if (dtype == GT_DTYPE_U16)
@@ -2000,7 +2166,7 @@ gt_status gt_batch_learned(gt_ctx* ctx, const gt_params* params, const gt_propos
                        "snr, minmass_snr, adaptive_background and illumination correction are not supported with "
                        "learned proposals");
     bool on_device = false;
-    CKS(check_frames_ptr(ctx, frames, &on_device));
+    CKS(check_frames_ptr(ctx, frames, (size_t)T * H * W * dtype_bytes(dtype), &on_device));
     std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
     gt_status st;
     if (dtype == GT_DTYPE_U16)
@@ -2058,7 +2224,7 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const voi
     CKS(validate(ctx, params, frames, dtype, T, H, W));
     if (n_points > 0 && !points) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null points");
     bool on_device = false;
-    CKS(check_frames_ptr(ctx, frames, &on_device));
+    CKS(check_frames_ptr(ctx, frames, (size_t)T * H * W * dtype_bytes(dtype), &on_device));
     std::unique_ptr<gt_table> tab(new gt_table(ctx->device, ctx->st));
     gt_status st;
     if (dtype == GT_DTYPE_U16)
@@ -2236,7 +2402,7 @@ gt_status gt_mean_frame(gt_ctx* ctx, const void* frames, int32_t dtype, int64_t 
     CKS(validate(ctx, &p, frames, dtype, T, H, W));
     if (!out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null output");
     bool on_device = false;
-    CKS(check_frames_ptr(ctx, frames, &on_device));
+    CKS(check_frames_ptr(ctx, frames, (size_t)T * H * W * dtype_bytes(dtype), &on_device));
     if (dtype == GT_DTYPE_U16) return mean_impl<uint16_t>(ctx, (const uint16_t*)frames, on_device, T, H, W, out);
     if (dtype == GT_DTYPE_F32) return mean_impl<float>(ctx, (const float*)frames, on_device, T, H, W, out);
     return mean_impl<uint8_t>(ctx, (const uint8_t*)frames, on_device, T, H, W, out);

@@ -64,6 +64,8 @@ struct StripGeom {
     static_assert(RWp >= PWp, "vertical maxima fit in the staging rows");
     static_assert(4 * 31 + 4 * NV4 <= PWp, "dilation row reads stay in the row");
     static_assert(4 * 31 + KD + 2 <= PW - 1 && SH4 + O + kStripTW <= PWp, "dilation windows inside the row");
+    static_assert(KD >= kStepRows && kStepRows == 8, "vertical maxima: 8 rows share the window rows 7 .. KD-1");
+    static_assert(PWp <= kStripThreads, "one thread per column in the column pass and vertical maxima");
 };
 
 template <typename T>
@@ -143,6 +145,8 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     const int tid = threadIdx.x;
     const bool edge_cols = (xa < 0) || (xa + RWp > W);
     const bool vec = vec_ok && !edge_cols;
+    // 16-byte stores of processed rows: every row start is a multiple of 4 floats
+    const bool st4 = (W % 4 == 0) && ((uintptr_t)proc % 16 == 0);
     // steps until the dilation rows reach R1: x0 + 8s - R - E + 8 >= R1
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
@@ -267,106 +271,98 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
         }
         __syncthreads();
 
-        // ---- C: column pass (preprocess_cols.wgsl) for processed rows q = x0 + 8s - R + jj
-        {
-            const int qbase = x0 + kStepRows * s - R;
-            for (int t = tid; t < 2 * PWp; t += kStripThreads) {
-                const int h = t / PWp, pc = t - h * PWp;
-                const int q0 = qbase + 4 * h;       // first of 4 processed rows
-                const int gcol = ps + pc;
-                // row-pass rows q0 - R .. q0 + 3 + R: relative index 8s - 2R + 4h + i
-                const int w0 = (kStepRows * s + 4 * h + (XR - 2 * R)) % XR;
-                const float* pg = xg + w0 * PWp + pc;
-                const float* pb = xb + w0 * PWp + pc;
-                float vg[4 + 2 * R], vbx[4 + 2 * R];
+        // ---- C: column pass (preprocess_cols.wgsl) for the step's 8 processed
+        // rows q = x0 + 8s - R + k, one column per thread
+        if (tid < PWp) {
+            const int pc = tid;
+            const int q0 = x0 + kStepRows * s - R;
+            const int gcol = ps + pc;
+            // row-pass rows q0 - R .. q0 + 7 + R: relative index 8s - 2R + i
+            const int w0 = (kStepRows * s + (XR - 2 * R)) % XR;
+            const float* pg = xg + w0 * PWp + pc;
+            const float* pb = xb + w0 * PWp + pc;
+            float vg[kStepRows + 2 * R], vbx[kStepRows + 2 * R];
 #pragma unroll
-                for (int i = 0; i < 4 + 2 * R; i++) {
-                    vg[i] = pg[i * PWp];
-                    vbx[i] = pb[i * PWp];
-                }
-                const bool col_in = (gcol >= 0 && gcol < W);
-                const bool rows_in = (q0 >= R && q0 + 3 < H - R);
-                float cs = 0.0f;
-                float res[4];
+            for (int i = 0; i < kStepRows + 2 * R; i++) {
+                vg[i] = pg[i * PWp];
+                vbx[i] = pb[i * PWp];
+            }
+            const bool col_in = (gcol >= 0 && gcol < W);
+            const bool rows_in = (q0 >= R && q0 + kStepRows - 1 < H - R);
+            float cs = 0.0f;
+            // processed row q has relative index q - (x0 - R) = 8s + k
+            const int p0 = (kStepRows * s) % PR;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int q = q0 + k;
-                    float gs = 0.0f;
-                    if (rows_in) {
+            for (int k = 0; k < kStepRows; k++) {
+                const int q = q0 + k;
+                float gs = 0.0f;
+                if (rows_in) {
 #pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
-                    } else {
+                    for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
+                } else {
 #pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) {
-                            const int gr = q + i - R;
-                            if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
-                        }
+                    for (int i = 0; i <= 2 * R; i++) {
+                        const int gr = q + i - R;
+                        if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
                     }
-                    if (kInt) {
-                        if (k == 0) {
+                }
+                if (kInt) {
+                    if (k == 0) {
 #pragma unroll
-                            for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[i]);
-                        } else {
-                            cs = __fsub_rn(__fadd_rn(cs, vbx[k + 2 * R]), vbx[k - 1]);
-                        }
+                        for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[i]);
                     } else {
-                        cs = 0.0f;
-#pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[k + i]);
+                        cs = __fsub_rn(__fadd_rn(cs, vbx[k + 2 * R]), vbx[k - 1]);
                     }
-                    float r = __fsub_rn(div_gnorm<FAST>(gs, c), div_kk<FAST>(cs, c));
-                    if (c.truncate && r < trunc_thr) r = 0.0f;
-                    res[k] = r;
-                }
-                // processed row q has relative index q - (x0 - R) = 8s + 4h + k
-                const int p0 = (kStepRows * s + 4 * h) % PR;
-                const int vcol = pc - SH4;   // pc0-relative column
+                } else {
+                    cs = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int q = q0 + k;
-                    const bool in = col_in && q >= 0 && q < H;
-                    const float v = in ? res[k] : -INFINITY;
-                    int pp = p0 + k;
-                    if (pp >= PR) pp -= PR;
-                    pr[pp * PWp + pc] = v;
-                    pr[(pp + PR) * PWp + pc] = v;
-                    // the segment's own rows and the strip's own columns go to HBM
-                    if (in && q >= R0 && q < R1 && vcol >= O && vcol < O + kStripTW) proc[(size_t)q * W + gcol] = v;
+                    for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[k + i]);
                 }
+                float r = __fsub_rn(div_gnorm<FAST>(gs, c), div_kk<FAST>(cs, c));
+                if (c.truncate && r < trunc_thr) r = 0.0f;
+                const float v = (col_in && q >= 0 && q < H) ? r : -INFINITY;
+                int pp = p0 + k;
+                if (pp >= PR) pp -= PR;
+                pr[pp * PWp + pc] = v;
+                pr[(pp + PR) * PWp + pc] = v;
             }
         }
         __syncthreads();
 
-        // ---- D: vertical maximum over KD processed rows for dilation rows d = x0 + 8s - R - E + jj
+        // ---- D: vertical maximum over KD processed rows for the step's 8
+        // dilation rows d = x0 + 8s - R - E + k, one column per thread
         const int dbase = x0 + kStepRows * s - R - E;
-        {
-            for (int t = tid; t < 2 * PWp; t += kStripThreads) {
-                const int h = t / PWp, pc = t - h * PWp;
-                const int vcol = pc - SH4;
-                if (vcol < 0) continue;
-                // output k of this thread: processed rows d0 + k - O .. d0 + k + E,
-                // relative index 8s - (KD - 1) + 4h + k + i
-                const int w0 = (kStepRows * s + 4 * h + (2 * PR - (KD - 1))) % PR;
-                const float* pp = pr + w0 * PWp + pc;
-                float a[KD + 3];
+        if (tid < PWp - SH4) {
+            const int pc = tid + SH4;
+            const int vcol = tid;   // pc0-relative column
+            // output k: processed rows d + k - O .. d + k + E, relative index
+            // 8s - (KD - 1) + k + i
+            const int w0 = (kStepRows * s + (2 * PR - (KD - 1))) % PR;
+            const float* pp = pr + w0 * PWp + pc;
+            float a[KD + kStepRows - 1];
 #pragma unroll
-                for (int i = 0; i < KD + 3; i++) a[i] = pp[i * PWp];
-                float mid = a[3];
+            for (int i = 0; i < KD + kStepRows - 1; i++) a[i] = pp[i * PWp];
+            // out k = max(a[k..6], mid = a[7..KD-1], a[KD..KD+k-1])
+            float mid = a[7];
 #pragma unroll
-                for (int i = 4; i < KD; i++) mid = fmaxf(mid, a[i]);
-                // out k = max(a[k..2], mid(a[3..KD-1]), a[KD..KD+k-1])
-                float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
-                float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
-                const int vr = 4 * h;
-                vb[(vr + 0) * PWp + vcol] = fmaxf(s0, mid);
-                vb[(vr + 1) * PWp + vcol] = fmaxf(fmaxf(s1, mid), p1);
-                vb[(vr + 2) * PWp + vcol] = fmaxf(fmaxf(s2, mid), p2);
-                vb[(vr + 3) * PWp + vcol] = fmaxf(mid, p3);
-            }
+            for (int i = 8; i < KD; i++) mid = fmaxf(mid, a[i]);
+            float sfx[7], pfx[8];
+            sfx[6] = a[6];
+#pragma unroll
+            for (int k = 5; k >= 0; k--) sfx[k] = fmaxf(a[k], sfx[k + 1]);
+            pfx[1] = a[KD];
+#pragma unroll
+            for (int k = 2; k < 8; k++) pfx[k] = fmaxf(pfx[k - 1], a[KD + k - 1]);
+            vb[vcol] = fmaxf(sfx[0], mid);
+#pragma unroll
+            for (int k = 1; k < 7; k++) vb[k * PWp + vcol] = fmaxf(fmaxf(sfx[k], mid), pfx[k]);
+            vb[7 * PWp + vcol] = fmaxf(mid, pfx[7]);
         }
         __syncthreads();
 
-        // ---- E: horizontal maximum and the candidate test (extract_max.wgsl)
+        // ---- E: horizontal maximum and the candidate test (extract_max.wgsl);
+        // the processed rows of the segment go to HBM from here, 4 columns
+        // per thread
         {
             const int t = tid;
             int cnt = 0;
@@ -396,13 +392,30 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                                   fmaxf(mid, p3)};
                     int prow = (kStepRows * s + jj + (PR - E)) % PR;   // relative index of row d: 8s + jj - E
                     const float* cen = pr + prow * PWp + SH4 + O + cc;
-                    const bool rows_ok = d >= c.margin && d < H - c.margin;
+                    float cv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) cv[k] = cen[k];
+                    const int gc0 = c0 + cc;
+                    float* dst = proc + (size_t)d * W + gc0;
+                    if (st4 && gc0 + 3 < W) {
+                        *(float4*)dst = make_float4(cv[0], cv[1], cv[2], cv[3]);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if (gc0 + k < W) dst[k] = cv[k];
+                    }
+                    // columns and rows inside the margin need no per-column test
+                    const bool inner = d >= c.margin && d < H - c.margin && gc0 >= c.margin &&
+                                       gc0 + 3 < W - c.margin;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        const int gc = c0 + cc + k;
-                        if (gc >= W) continue;
-                        if (!rows_ok || gc < c.margin || gc >= W - c.margin) continue;
-                        const float center = cen[k];
+                        if (!inner) {
+                            const int gc = gc0 + k;
+                            if (gc >= W || d < c.margin || d >= H - c.margin || gc < c.margin ||
+                                gc >= W - c.margin)
+                                continue;
+                        }
+                        const float center = cv[k];
                         if (center < thr) continue;
                         if (c.skip_zero && center == 0.0f) continue;
                         if (m[k] > center) continue;
@@ -410,7 +423,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                         cnt++;
                     }
                     cd = d;
-                    ccol = c0 + cc;
+                    ccol = gc0;
                 }
             }
             // warp-aggregated reservation of output slots

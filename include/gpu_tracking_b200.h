@@ -138,6 +138,16 @@ GT_API int64_t gt_table_nrows(const gt_table* t);
 GT_API gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst);
 /* Copy an integer column (frame / particle / duration) as int64. */
 GT_API gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst);
+/* Copy several columns at once in the dtypes of the reference's DataFrame
+ * (the `astype` of the column types after `pandas.DataFrame(array)`,
+ * gpu_tracking_macros/src/lib.rs:138-147: "int" -> int64, "float" ->
+ * float64).  dst[k] receives column columns[k]: int64_t values for
+ * GT_COL_FRAME / GT_COL_PARTICLE / GT_COL_DURATION, double for every other
+ * column (the float32 value widened exactly).  The rows cross PCIe through
+ * pinned staging buffers and are widened on several host threads, so the
+ * destinations may be ordinary pageable memory.  Returns
+ * GT_ERR_INVALID_ARGUMENT for a column the table does not have. */
+GT_API gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst);
 /* 1 if the column was computed for this table (e.g. GT_COL_PARTICLE only
  * when linking ran). */
 GT_API int32_t gt_table_has_column(const gt_table* t, int32_t column);
