@@ -16,9 +16,10 @@
 // contiguous and every read in the tap loops is a constant offset from one
 // base address.  The tap loops are unrolled for the compile-time radius.
 // The floating-point operation sequence of every output is the oracle's:
-// sequential fused multiply-adds over the taps, sequential boxcar sums (a
-// sliding sum for integer inputs, where every partial sum is an exactly
-// representable integer), and division by the constants gnorm and kk either
+// sequential fused multiply-adds over the taps, sequential boxcar sums (for
+// integer inputs a pairwise window sum and sliding differences instead: every
+// partial sum is an exactly representable integer, so any order gives the
+// same value), and division by the constants gnorm and kk either
 // as IEEE division or, where proven equal to it (LocateConsts::fast_div), as
 // fma(x, zh, x*zl).
 #include <math.h>
@@ -104,6 +105,24 @@ struct Quad<float> {
     using V = float4;
     __device__ static V load(const float* p) { return __ldg((const float4*)p); }
     __device__ static float4 cvt(V v) { return v; }
+};
+
+// Pairwise reductions with a short dependency chain.  Both are exact in any
+// order here: the maximum always, the sum because it only adds integer pixel
+// values (or integer row sums) whose partial sums stay below 2^24.
+template <int N>
+struct Tree {
+    __device__ __forceinline__ static float max(const float* a) {
+        return fmaxf(Tree<N / 2>::max(a), Tree<N - N / 2>::max(a + N / 2));
+    }
+    __device__ __forceinline__ static float sum(const float* a) {
+        return __fadd_rn(Tree<N / 2>::sum(a), Tree<N - N / 2>::sum(a + N / 2));
+    }
+};
+template <>
+struct Tree<1> {
+    __device__ __forceinline__ static float max(const float* a) { return a[0]; }
+    __device__ __forceinline__ static float sum(const float* a) { return a[0]; }
 };
 
 template <bool FAST>
@@ -246,12 +265,9 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                         }
                     }
                     if (kInt) {
-                        if (k == 0) {
-#pragma unroll
-                            for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, x[i]);
-                        } else {
-                            cs = __fsub_rn(__fadd_rn(cs, x[k + 2 * R]), x[k - 1]);
-                        }
+                        // exact integers: the window sum, then sliding differences
+                        if (k == 0) cs = Tree<2 * R + 1>::sum(x);
+                        else cs = __fadd_rn(cs, __fsub_rn(x[k + 2 * R], x[k - 1]));
                     } else {
                         cs = 0.0f;
 #pragma unroll
@@ -307,12 +323,8 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                     }
                 }
                 if (kInt) {
-                    if (k == 0) {
-#pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[i]);
-                    } else {
-                        cs = __fsub_rn(__fadd_rn(cs, vbx[k + 2 * R]), vbx[k - 1]);
-                    }
+                    if (k == 0) cs = Tree<2 * R + 1>::sum(vbx);
+                    else cs = __fadd_rn(cs, __fsub_rn(vbx[k + 2 * R], vbx[k - 1]));
                 } else {
                     cs = 0.0f;
 #pragma unroll
@@ -343,9 +355,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
 #pragma unroll
             for (int i = 0; i < KD + kStepRows - 1; i++) a[i] = pp[i * PWp];
             // out k = max(a[k..6], mid = a[7..KD-1], a[KD..KD+k-1])
-            float mid = a[7];
-#pragma unroll
-            for (int i = 8; i < KD; i++) mid = fmaxf(mid, a[i]);
+            const float mid = Tree<KD - 7>::max(a + 7);
             float sfx[7], pfx[8];
             sfx[6] = a[6];
 #pragma unroll
@@ -383,9 +393,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
                         a[4 * i + 2] = v.z;
                         a[4 * i + 3] = v.w;
                     }
-                    float mid = a[3];
-#pragma unroll
-                    for (int i = 4; i < KD; i++) mid = fmaxf(mid, a[i]);
+                    const float mid = Tree<KD - 3>::max(a + 3);
                     float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
                     float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
                     float m[4] = {fmaxf(s0, mid), fmaxf(fmaxf(s1, mid), p1), fmaxf(fmaxf(s2, mid), p2),
