@@ -660,6 +660,7 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     L.b_pts = ctx->l_bpts.as<int32_t>();
     L.b_dist = ctx->l_bdist.as<float>();
     L.srt = ctx->l_srt.as<uint32_t>();
+    L.f_entries = ftot;
     {
         Prof pf(ctx, "link_lists");
         CK(link_fill_lists(in, L, ctx->st));

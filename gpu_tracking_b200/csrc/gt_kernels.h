@@ -212,6 +212,7 @@ struct LinkLists {
     uint32_t* srt = nullptr;      // per group: points sorted by row key
     int64_t pbase = 0;            // first point the offset arrays cover
     int64_t f_cap = -1, b_cap = -1;  // entries f_pts / b_pts hold (-1: sized exactly)
+    int64_t f_entries = -1;          // forward entries of lists sized exactly (-1: not known)
 };
 
 struct LinkScratch {

@@ -27,13 +27,27 @@ constexpr int kSortSmem = 4096;
 constexpr long long kSubnetBudget = 1ll << 28;
 constexpr int kLagRegs = 4;     // backward-list offsets of up to 4 lags held in registers
 constexpr int kRingSmem = 64;   // memory ring bookkeeping in shared memory up to memory = 64
-// A frame with at most kLinkSmemD detections and kLinkSmemS sources keeps its
-// per-destination and per-source working arrays in shared memory; larger
-// frames use the same arrays in the global scratch.
-constexpr int kLinkSmemD = 2048;
-constexpr int kLinkSmemS = 2560;
-constexpr size_t kLinkSmemBytes = (size_t)(kLinkSmemD + 1) * 4 * 10 + (size_t)kLinkSmemS * (8 + 8 + 4 + 1);
-static_assert(((kLinkSmemD + 1) * 4 * 10) % 8 == 0, "source block stays 8-byte aligned");
+// A frame with at most LinkSmem<SF>::D detections and LinkSmem<SF>::S sources
+// keeps its per-destination and per-source working arrays in shared memory;
+// larger frames use the same arrays in the global scratch.  SF is the type of
+// the per-source forward-list offsets: int32 when every offset of the lists
+// fits (a larger working set in the same shared memory), int64 otherwise.
+template <typename SF>
+struct LinkSmem;
+template <>
+struct LinkSmem<int64_t> {
+    static constexpr int D = 2048, S = 2560;
+};
+template <>
+struct LinkSmem<int32_t> {
+    static constexpr int D = 3840, S = 4608;
+};
+template <typename SF>
+constexpr size_t link_smem_bytes() {
+    return (size_t)(LinkSmem<SF>::D + 1) * 4 * 10 + (size_t)LinkSmem<SF>::S * (2 * sizeof(SF) + 4 + 1);
+}
+static_assert(((LinkSmem<int64_t>::D + 1) * 4 * 10) % 8 == 0, "source block stays 8-byte aligned");
+static_assert(link_smem_bytes<int32_t>() + 4096 <= 227 * 1024, "the int32 working set fits with the static arrays");
 
 // ------------------------------------------------------- point addressing
 __device__ __forceinline__ int64_t gbase(const LinkInput& in, int g) {
@@ -271,8 +285,10 @@ __device__ __forceinline__ void uf_union(volatile int* parent, int a, int b) {
     }
 }
 
+template <typename SF>
 __global__ void __launch_bounds__(kLinkThreads)
 link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, LinkWindow W) {
+    constexpr int kLinkSmemD = LinkSmem<SF>::D, kLinkSmemS = LinkSmem<SF>::S;
     __shared__ int wsum[33];
     __shared__ long long wsum64[33];
     __shared__ int sh_ring_n[kRingSmem + 1], sh_ringpre[kRingSmem + 2];
@@ -382,8 +398,8 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
         const int sstr = fast ? kLinkSmemS : Smax;
         int32_t* const dblk = fast ? s_dblk : g_dblk;
         uint8_t* const sblk = fast ? s_sblk : g_sblk;
-        int64_t* const sf0 = (int64_t*)sblk;
-        int64_t* const sf1 = sf0 + sstr;
+        SF* const sf0 = (SF*)sblk;
+        SF* const sf1 = sf0 + sstr;
         int32_t* const src_pt = (int32_t*)(sf1 + sstr);
         uint8_t* const srcUsed = (uint8_t*)(src_pt + sstr);
         int32_t* const d_off = dblk;
@@ -525,8 +541,8 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
             const int64_t pt = P0 + src_pt[s];
             const int64_t l = lix(L, pt, K, g - ggroup(in, pt) - 1);
             const int64_t f0 = L.f_off[l], f1 = L.f_off[l + 1];
-            sf0[s] = f0;
-            sf1[s] = f1;
+            sf0[s] = (SF)f0;
+            sf1[s] = (SF)f1;
             srcUsed[s] = 0;
         }
         __syncthreads();
@@ -954,8 +970,17 @@ cudaError_t link_run_window(const LinkInput& in, const LinkLists& L, const LinkS
                             const LinkWindow& w, cudaStream_t st) {
     if (in.nvideos == 0) return cudaSuccess;
     if (w.g0 >= 0 && (in.nvideos != 1 || !w.state)) return cudaErrorInvalidValue;
-    cudaFuncSetAttribute(link_video_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLinkSmemBytes);
-    link_video_kernel<<<in.nvideos, kLinkThreads, kLinkSmemBytes, st>>>(in, L, S, out, w);
+    // narrow offsets when the forward lists hold fewer than 2^31 entries
+    const int64_t fmax = L.f_cap >= 0 ? L.f_cap : L.f_entries;
+    if (fmax >= 0 && fmax < (int64_t)INT32_MAX) {
+        constexpr size_t bytes = link_smem_bytes<int32_t>();
+        cudaFuncSetAttribute(link_video_kernel<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        link_video_kernel<int32_t><<<in.nvideos, kLinkThreads, bytes, st>>>(in, L, S, out, w);
+    } else {
+        constexpr size_t bytes = link_smem_bytes<int64_t>();
+        cudaFuncSetAttribute(link_video_kernel<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        link_video_kernel<int64_t><<<in.nvideos, kLinkThreads, bytes, st>>>(in, L, S, out, w);
+    }
     return cudaGetLastError();
 }
 
