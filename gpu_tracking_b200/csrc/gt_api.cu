@@ -2014,18 +2014,29 @@ ExportPool* export_pool(int device) {
     return device >= 0 && device < kExportMaxDevices ? &pools[device] : nullptr;
 }
 
+// All or nothing: on a failure everything created so far is released and the
+// next call tries again.
 cudaError_t export_pool_init(ExportPool& p) {
     if (p.ready) return cudaSuccess;
     char* block = nullptr;
     cudaError_t e = cudaHostAlloc((void**)&block, 2 * kExportLanes * kExportSlot, cudaHostAllocDefault);
     if (e != cudaSuccess) return e;
-    for (int l = 0; l < kExportLanes; l++) {
+    for (int l = 0; l < kExportLanes && e == cudaSuccess; l++) {
         ExportLane& L = p.lane[l];
         L.slot[0] = block + (2 * l) * kExportSlot;
         L.slot[1] = block + (2 * l + 1) * kExportSlot;
-        if ((e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess) return e;
-        for (int s = 0; s < 2; s++)
-            if ((e = cudaEventCreateWithFlags(&L.ev[s], cudaEventDisableTiming)) != cudaSuccess) return e;
+        e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
+        for (int s = 0; s < 2 && e == cudaSuccess; s++) e = cudaEventCreateWithFlags(&L.ev[s], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        for (ExportLane& L : p.lane) {
+            for (cudaEvent_t& ev : L.ev)
+                if (ev) cudaEventDestroy(ev), ev = nullptr;
+            if (L.st) cudaStreamDestroy(L.st), L.st = nullptr;
+            L.slot[0] = L.slot[1] = nullptr;
+        }
+        cudaFreeHost(block);
+        return e;
     }
     p.ready = true;
     return cudaSuccess;
@@ -2069,7 +2080,9 @@ cudaError_t export_lane(int device, ExportLane& L, const std::vector<ExportItem>
 
 }  // namespace
 
-gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
+namespace {
+
+gt_status table_export_impl(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
     if (!t || ncolumns < 0 || (ncolumns > 0 && (!columns || !dst))) return GT_ERR_INVALID_ARGUMENT;
     for (int32_t k = 0; k < ncolumns; k++) {
         const int32_t c = columns[k];
@@ -2106,13 +2119,29 @@ gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t nco
     }
     std::vector<cudaError_t> err(lanes, cudaSuccess);
     std::vector<std::thread> th;
-    for (int l = 1; l < lanes; l++)
-        th.emplace_back([&, l] { err[l] = export_lane(t->device, pool->lane[l], work[l]); });
+    // lanes whose thread cannot be started run on the calling thread
+    for (int l = 1; l < lanes; l++) {
+        try {
+            th.emplace_back([&, l] { err[l] = export_lane(t->device, pool->lane[l], work[l]); });
+        } catch (...) {
+            err[l] = export_lane(t->device, pool->lane[l], work[l]);
+        }
+    }
     err[0] = export_lane(t->device, pool->lane[0], work[0]);
     for (auto& x : th) x.join();
     for (cudaError_t e : err)
         if (e != cudaSuccess) return GT_ERR_CUDA;
     return GT_OK;
+}
+
+}  // namespace
+
+gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
+    try {
+        return table_export_impl(t, columns, ncolumns, dst);
+    } catch (...) {
+        return GT_ERR_INTERNAL;   // no C++ exception crosses the C ABI
+    }
 }
 
 void gt_table_free(gt_table* t) {

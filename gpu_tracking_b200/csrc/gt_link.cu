@@ -26,6 +26,7 @@ constexpr int kLinkThreads = 1024;
 constexpr int kSortSmem = 4096;
 constexpr long long kSubnetBudget = 1ll << 28;
 constexpr int kLagRegs = 4;     // backward-list offsets of up to 4 lags held in registers
+constexpr int kEdgeRegs = 2;    // backward edges per lag gathered in registers before they are written
 constexpr int kRingSmem = 64;   // memory ring bookkeeping in shared memory up to memory = 64
 // A frame with at most LinkSmem<SF>::D detections and LinkSmem<SF>::S sources
 // keeps its per-destination and per-source working arrays in shared memory;
@@ -497,11 +498,69 @@ link_video_kernel(LinkInput in, LinkLists L, LinkScratch S, LinkOutput out, Link
             int64_t bo[kLagRegs + 1];
             const bool regs = K <= kLagRegs;
 #pragma unroll
-            for (int i = 0; i <= kLagRegs; i++)
-                if (regs && i <= K) bo[i] = L.b_off[lb + i];
+            for (int i = 0; i <= kLagRegs; i++) bo[i] = (regs && i <= K) ? L.b_off[lb + i] : 0;
             const int64_t b0 = regs ? bo[0] : L.b_off[lb];
             int w = (int)(b0 - fb);
             d_off[j] = w;
+            // When every lag has at most kEdgeRegs edges, all list reads are
+            // issued before any write (the writes could alias them for the
+            // compiler), so their latencies overlap: three dependent levels
+            // instead of one chain per edge.  Same edges, same order.
+            bool fits = regs;
+#pragma unroll
+            for (int k = 1; k <= kLagRegs; k++)
+                if (k <= K && bo[k] - bo[k - 1] > kEdgeRegs) fits = false;
+            if (fits) {
+                int32_t ep[kLagRegs][kEdgeRegs], es[kLagRegs][kEdgeRegs];
+                float ed[kLagRegs][kEdgeRegs];
+#pragma unroll
+                for (int k = 1; k <= kLagRegs; k++) {
+                    const bool lag_on = k <= K && (k == 1 ? S0 > 0 : g - k >= gb);
+#pragma unroll
+                    for (int u = 0; u < kEdgeRegs; u++) {
+                        const int64_t e = bo[k - 1] + u;
+                        const bool on = lag_on && e < bo[k];
+                        ep[k - 1][u] = on ? L.b_pts[e] : -1;
+                        ed[k - 1][u] = on ? L.b_dist[e] : 0.0f;
+                    }
+                }
+                // lags 2..K: the source's index in this step's source list,
+                // or -1 when it is not a source of this step
+#pragma unroll
+                for (int k = 2; k <= kLagRegs; k++) {
+                    const int64_t ta = (k <= K && g - k >= gb) ? gbase(in, g - k) - P0 : 0;
+#pragma unroll
+                    for (int u = 0; u < kEdgeRegs; u++) {
+                        es[k - 1][u] = -1;
+                        if (ep[k - 1][u] >= 0) {
+                            const int64_t lp = ta + ep[k - 1][u];
+                            const int32_t stamp = srcstamp[lp], idx = srcidx[lp];
+                            es[k - 1][u] = (stamp == step) ? idx : -1;
+                        }
+                    }
+                }
+                // lag 1 (index within group g-1 == source index), then lags K..2
+#pragma unroll
+                for (int u = 0; u < kEdgeRegs; u++)
+                    if (ep[0][u] >= 0) {
+                        e_src[w] = ep[0][u];
+                        e_dist[w] = ed[0][u];
+                        w++;
+                    }
+#pragma unroll
+                for (int k = kLagRegs; k >= 2; k--)
+#pragma unroll
+                    for (int u = 0; u < kEdgeRegs; u++)
+                        if (es[k - 1][u] >= 0) {
+                            e_src[w] = es[k - 1][u];
+                            e_dist[w] = ed[k - 1][u];
+                            w++;
+                        }
+                d_end[j] = w;
+                parent[j] = j;
+                out_src[j] = -2;
+                continue;
+            }
             if (S0 > 0) {
                 const int64_t o1 = regs ? bo[1] : L.b_off[lb + 1];
                 for (int64_t e = b0; e < o1; e++) {
