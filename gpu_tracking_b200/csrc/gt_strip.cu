@@ -7,10 +7,11 @@
 //   A  the step's raw rows are staged in shared memory (4 pixels per load,
 //      converted exactly to float), the next step's are prefetched;
 //   B  row pass: each thread makes 4 adjacent columns from float4 loads;
-//   C  column pass: each thread makes 4 rows of one column;
-//   D  vertical dilation maximum, 4 rows per thread;
-//   E  horizontal dilation maximum and the candidate test, 4 columns per
-//      thread, slots reserved once per warp.
+//   C  column pass: each thread makes the step's 8 rows of one column;
+//   D  vertical dilation maximum, 8 rows of one column per thread;
+//   E  horizontal dilation maximum, the candidate test and the store of the
+//      segment's processed rows, 4 columns per thread, slots reserved once
+//      per warp.
 // The row-pass rows and the processed rows live in ring buffers that hold
 // every row twice (at r and r + ring), so any window of consecutive rows is
 // contiguous and every read in the tap loops is a constant offset from one
