@@ -184,6 +184,16 @@ def test_link_dense_subnets(oracle, n, size, R):
     assert np.array_equal(ids, oracle.link(rows, R, 1))
 
 
+@pytest.mark.parametrize("n", [3000, 5000])
+def test_link_large_frames(oracle, n):
+    """Frames of 3000 detections keep the linker's per-frame working arrays in
+    shared memory only with 32-bit list offsets; frames of 5000 exceed it and
+    use the global scratch.  Both give the oracle's ids."""
+    rows = random_detections(7, T=6, n=n, R=5.0, size=1500.0)
+    ids = gt.link(rows, 5.0, 2)
+    assert np.array_equal(ids, oracle.link(rows, 5.0, 2))
+
+
 def test_link_load_guard_agrees_with_oracle(oracle):
     rows = random_detections(5, T=10, n=150, R=6.0, size=60.0)
     with pytest.raises(oracle.OracleError):
