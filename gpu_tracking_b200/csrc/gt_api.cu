@@ -7,7 +7,9 @@
 //     copy of chunk c+1 overlaps the kernels of chunk c;
 //   * every per-frame result stays in HBM until the whole video is done
 //     (filter, doughnut and linking included), then one table is assembled
-//     on the device and copied out column by column on request;
+//     on the device; gt_table_export copies any set of its columns out in one
+//     call (pinned staging lanes, widened to the DataFrame's dtypes on host
+//     threads), gt_table_column_* one column at a time;
 //   * capacities (candidates / detections per frame) grow and the call is
 //     replayed when a kernel reports an overflow, so nothing is truncated.
 #include <cuda.h>
