@@ -425,7 +425,8 @@ def run_learned(args):
             pk = json.load(f)
     except Exception:
         pass
-    tc_peak = float(pk.get("bf16_tflops", 1590.0))
+    # the network runs inside a long step: the sustained GEMM figure when measured
+    tc_peak = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops", 1590.0)))
     net_ms = kern_l.get("proposal_net", {}).get("ms")
     flops = cnn_flops_per_cell() * ((S + 3) // 4) ** 2 * T
     tensor = None
