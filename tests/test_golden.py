@@ -1,0 +1,78 @@
+"""Golden vectors from the reference's own shaders (tests/golden/make_golden.py:
+preprocess_rows/cols, max_rows + extract_max, walk + characterize, translated
+from the reference's WGSL and run on the CPU).  They need no reference
+checkout, so they pin the oracle and the GPU path on any machine:
+
+* the oracle's restatement reproduces every processed value, candidate and
+  walked row bit for bit;
+* the engine's table (filter_close and the doughnut off, so that only the
+  shader stages shape it) holds the same rows bit for bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from gpu_tracking_b200._params import trackpy_params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "trackpy_ref_64x96.npz")
+# the generator's cases (tests/golden/make_golden.py)
+CASES = [
+    dict(diameter=9, minmass=300.0, separation=9),
+    dict(diameter=11, minmass=200.0),
+    dict(diameter=7, minmass=0.0, truncate_preprocessed=False),
+]
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def same_floats(got, want):
+    """Bit-identical float32 values; a NaN equals any NaN (the GPU and the
+    host write different NaN payloads, e.g. for Rg of a zero-mass row)."""
+    g = np.ascontiguousarray(got, np.float32)
+    w = np.ascontiguousarray(want, np.float32)
+    return bool(np.all((bits(g) == bits(w)) | (np.isnan(g) & np.isnan(w))))
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with np.load(GOLDEN) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_oracle_reproduces_reference_shaders(oracle, golden, case):
+    p = trackpy_params(**CASES[case])
+    frames = golden["c%d_frames" % case]
+    assert len(golden["c%d_t0_rows" % case]) + len(golden["c%d_t1_rows" % case]) > 0
+    for t in range(frames.shape[0]):
+        f = frames[t].astype(np.float32)
+        proc = oracle.preprocess(p, f)
+        if t == 0:
+            assert np.array_equal(bits(proc), bits(golden["c%d_t0_processed" % case]))
+        cands = oracle.candidates(p, proc)
+        assert np.array_equal(cands, golden["c%d_t%d_candidates" % (case, t)])
+        rows, keep = oracle.walk(p, proc, f, cands)
+        assert np.array_equal(bits(rows[keep]), bits(golden["c%d_t%d_rows" % (case, t)]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_engine_reproduces_reference_shaders(golden, case):
+    import gpu_tracking_b200 as gt
+    kw = dict(CASES[case])
+    diameter = kw.pop("diameter")
+    frames = golden["c%d_frames" % case]
+    df = gt.batch(frames, diameter, filter_close=False, doughnut_correction=False, characterize=True, tqdm=False,
+                  **kw)
+    # walked rows: x (row), y (column), mass, r, max, Rg, raw, signal, ecc, count
+    cols = [("y", 0), ("x", 1), ("mass", 2), ("Rg", 5), ("raw", 6), ("signal", 7), ("ecc", 8)]
+    for t in range(frames.shape[0]):
+        want = golden["c%d_t%d_rows" % (case, t)]
+        got = df[df["frame"] == t]
+        assert len(got) == len(want), (t, len(got), len(want))
+        for name, field in cols:
+            assert same_floats(got[name].to_numpy(), want[:, field]), (t, name)
