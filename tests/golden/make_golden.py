@@ -1,6 +1,7 @@
-"""Writes tests/golden/trackpy_ref_64x96.npz: outputs of the reference's own
-WGSL shaders (preprocess_rows/cols, max_rows + extract_max, walk +
-characterize), translated to C++ by oracle/wgsl2cpp.py and built into
+"""Writes tests/golden/trackpy_ref_64x96.npz and tests/golden/log_ref_48x56.npz:
+outputs of the reference's own WGSL shaders (preprocess_rows/cols, max_rows +
+extract_max, walk + characterize; separable_log, logspace_max; the frame std
+reduction), translated to C++ by oracle/wgsl2cpp.py and built into
 oracle/_ref/ from the reference checkout, on small seeded synthetic frames.
 
 The fixtures let the oracle and the GPU path be checked against the
@@ -19,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-from gpu_tracking_b200._params import trackpy_params  # noqa: E402
+from gpu_tracking_b200._params import log_params, trackpy_params  # noqa: E402
 from oracle import loader  # noqa: E402
 from synth import video  # noqa: E402
 
@@ -49,7 +50,34 @@ def main():
                 out["c%d_t%d_processed" % (c, t)] = proc
             out["c%d_t%d_candidates" % (c, t)] = cands
             out["c%d_t%d_rows" % (c, t)] = rows
+        # the reference's frame std (snr / minmass_snr thresholds)
+        out["c%d_std" % c] = np.array([loader.ref_frame_std(frames[t].astype(np.float32)) for t in range(T)],
+                                      np.float32)
     path = os.path.join(HERE, "trackpy_ref_64x96.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+    # LoG: the scale planes of every radius, the scale-space maxima and their walks
+    out = {}
+    frames, _ = video(1, 48, 56, 10, seed=7, dtype=np.float32, read_noise=5.0, bg=50.0)
+    f = frames[0]
+    out["frame"] = f
+    for s_, spacing in enumerate((False, True)):
+        p = log_params(2.0, 6.0, n_radii=4, log_spacing=spacing)
+        planes, radii = loader.log_planes(p, f)   # radii only: the planes below are the reference's
+        proc = loader.ref_preprocess(p, f)
+        ref_planes = np.stack([loader.ref_laplace(p, f, np.float32(r) / np.sqrt(np.float32(2.0))) for r in radii])
+        out["s%d_radii" % s_] = radii
+        out["s%d_planes" % s_] = ref_planes
+        n = len(radii)
+        for i in range(n):
+            edge = -1 if i == 0 else (1 if i == n - 1 else 0)
+            bottom = ref_planes[i - 1] if i > 0 else np.zeros_like(f)
+            top = ref_planes[i + 1] if i < n - 1 else np.zeros_like(f)
+            cands = loader.ref_logspace_max(p, bottom, ref_planes[i], top, proc, edge, radii[i])
+            out["s%d_r%d_candidates" % (s_, i)] = cands
+            out["s%d_r%d_rows" % (s_, i)] = loader.ref_walk(p, proc, f, cands, r=float(radii[i]), characterize=False)
+    path = os.path.join(HERE, "log_ref_48x56.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")
 

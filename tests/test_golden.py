@@ -76,3 +76,38 @@ def test_engine_reproduces_reference_shaders(golden, case):
         assert len(got) == len(want), (t, len(got), len(want))
         for name, field in cols:
             assert same_floats(got[name].to_numpy(), want[:, field]), (t, name)
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_oracle_frame_std_matches_reference(oracle, golden, case):
+    frames = golden["c%d_frames" % case]
+    want = golden["c%d_std" % case]
+    got = np.array([oracle.frame_std(f.astype(np.float32)) for f in frames], np.float32)
+    assert np.array_equal(bits(got), bits(want))
+
+
+@pytest.fixture(scope="module")
+def golden_log():
+    with np.load(os.path.join(HERE, "golden", "log_ref_48x56.npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("spacing", [0, 1])
+def test_oracle_log_matches_reference(oracle, golden_log, spacing):
+    """Scale planes of every radius bit for bit, and the walks from the
+    reference's scale-space maxima (position, mass, radius, max)."""
+    from gpu_tracking_b200._params import log_params
+    f = golden_log["frame"]
+    p = log_params(2.0, 6.0, n_radii=4, log_spacing=bool(spacing))
+    planes, radii = oracle.log_planes(p, f)
+    assert np.array_equal(bits(radii), bits(golden_log["s%d_radii" % spacing]))
+    assert np.array_equal(bits(planes), bits(golden_log["s%d_planes" % spacing]))
+    proc = oracle.preprocess(p, f)
+    n_rows = 0
+    for i, r in enumerate(radii):
+        cands = golden_log["s%d_r%d_candidates" % (spacing, i)]
+        want = golden_log["s%d_r%d_rows" % (spacing, i)]
+        mine, keep = oracle.walk(p, proc, f, cands, r=float(r))
+        assert np.array_equal(bits(mine[keep][:, :5]), bits(want[:, :5])), i
+        n_rows += len(want)
+    assert n_rows > 0
