@@ -111,3 +111,23 @@ def test_oracle_log_matches_reference(oracle, golden_log, spacing):
         assert np.array_equal(bits(mine[keep][:, :5]), bits(want[:, :5])), i
         n_rows += len(want)
     assert n_rows > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spacing", [0, 1])
+def test_engine_log_matches_reference(golden_log, spacing):
+    """The engine's LoG detections (no pruning, no characterization) are the
+    walks from the reference's scale-space maxima: position, mass and radius
+    bit for bit."""
+    import gpu_tracking_b200 as gt
+    f = golden_log["frame"]
+    df = gt.LoG(f[None], 2.0, 6.0, n_radii=4, log_spacing=bool(spacing), overlap_threshold=1.0,
+                characterize=False, doughnut_correction=False, tqdm=False)
+    radii = golden_log["s%d_radii" % spacing]
+    want = np.concatenate([golden_log["s%d_r%d_rows" % (spacing, i)] for i in range(len(radii))])
+    got = np.stack([df[c].to_numpy(np.float32) for c in ("y", "x", "mass", "r")], axis=1)
+    assert len(got) == len(want) > 0
+    # the same set of rows: order both by radius, then position
+    g = got[np.lexsort((got[:, 1], got[:, 0], got[:, 3]))]
+    w = want[:, :4][np.lexsort((want[:, 1], want[:, 0], want[:, 3]))]
+    assert same_floats(g, w)
