@@ -29,6 +29,8 @@ CASES = [
     (dict(diameter=9, minmass=300.0, separation=9), 11),
     (dict(diameter=11, minmass=200.0), 12),
     (dict(diameter=7, minmass=0.0, truncate_preprocessed=False), 13),
+    # thresholds from the frame std: extract_max.wgsl:37 and walk.wgsl:200-205
+    (dict(diameter=9, snr=1.2, minmass_snr=0.3), 14),
 ]
 T, H, W = 2, 64, 96
 
@@ -44,8 +46,9 @@ def main():
         for t in range(T):
             f = frames[t].astype(np.float32)
             proc = loader.ref_preprocess(p, f)
-            cands = loader.ref_candidates(p, proc)
-            rows = loader.ref_walk(p, proc, f, cands, characterize=True)
+            std = loader.ref_frame_std(f) if ("snr" in kw or "minmass_snr" in kw) else 0.0
+            cands = loader.ref_candidates(p, proc, pic_std=std)
+            rows = loader.ref_walk(p, proc, f, cands, characterize=True, pic_std=std)
             if t == 0:
                 out["c%d_t%d_processed" % (c, t)] = proc
             out["c%d_t%d_candidates" % (c, t)] = cands

@@ -22,6 +22,7 @@ CASES = [
     dict(diameter=9, minmass=300.0, separation=9),
     dict(diameter=11, minmass=200.0),
     dict(diameter=7, minmass=0.0, truncate_preprocessed=False),
+    dict(diameter=9, snr=1.2, minmass_snr=0.3),
 ]
 
 
@@ -53,9 +54,10 @@ def test_oracle_reproduces_reference_shaders(oracle, golden, case):
         proc = oracle.preprocess(p, f)
         if t == 0:
             assert np.array_equal(bits(proc), bits(golden["c%d_t0_processed" % case]))
-        cands = oracle.candidates(p, proc)
+        std = golden["c%d_std" % case][t] if ("snr" in CASES[case] or "minmass_snr" in CASES[case]) else 0.0
+        cands = oracle.candidates(p, proc, pic_std=std)
         assert np.array_equal(cands, golden["c%d_t%d_candidates" % (case, t)])
-        rows, keep = oracle.walk(p, proc, f, cands)
+        rows, keep = oracle.walk(p, proc, f, cands, pic_std=std)
         assert np.array_equal(bits(rows[keep]), bits(golden["c%d_t%d_rows" % (case, t)]))
 
 
