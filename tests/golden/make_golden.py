@@ -31,6 +31,8 @@ CASES = [
     (dict(diameter=7, minmass=0.0, truncate_preprocessed=False), 13),
     # thresholds from the frame std: extract_max.wgsl:37 and walk.wgsl:200-205
     (dict(diameter=9, snr=1.2, minmass_snr=0.3), 14),
+    # per-frame illumination correction: every stage sees frame / smoothed frame
+    (dict(diameter=9, minmass=0.05, illumination_sigma=4.0, illumination_correction_per_frame=True), 15),
 ]
 T, H, W = 2, 64, 96
 
@@ -45,6 +47,8 @@ def main():
         p = trackpy_params(**kw)
         for t in range(T):
             f = frames[t].astype(np.float32)
+            if kw.get("illumination_correction_per_frame"):
+                f = loader.ref_illumination(p, f, np.float32(kw["illumination_sigma"]), f)[1]
             proc = loader.ref_preprocess(p, f)
             std = loader.ref_frame_std(f) if ("snr" in kw or "minmass_snr" in kw) else 0.0
             cands = loader.ref_candidates(p, proc, pic_std=std)

@@ -23,6 +23,7 @@ CASES = [
     dict(diameter=11, minmass=200.0),
     dict(diameter=7, minmass=0.0, truncate_preprocessed=False),
     dict(diameter=9, snr=1.2, minmass_snr=0.3),
+    dict(diameter=9, minmass=0.05, illumination_sigma=4.0, illumination_correction_per_frame=True),
 ]
 
 
@@ -51,6 +52,8 @@ def test_oracle_reproduces_reference_shaders(oracle, golden, case):
     assert len(golden["c%d_t0_rows" % case]) + len(golden["c%d_t1_rows" % case]) > 0
     for t in range(frames.shape[0]):
         f = frames[t].astype(np.float32)
+        if CASES[case].get("illumination_correction_per_frame"):
+            f = f / oracle.smooth_profile(f, np.float32(CASES[case]["illumination_sigma"]))
         proc = oracle.preprocess(p, f)
         if t == 0:
             assert np.array_equal(bits(proc), bits(golden["c%d_t0_processed" % case]))
