@@ -1,7 +1,7 @@
 """Writes tests/golden/trackpy_ref_64x96.npz and tests/golden/log_ref_48x56.npz:
 outputs of the reference's own WGSL shaders (preprocess_rows/cols, max_rows +
 extract_max, walk + characterize; separable_log, logspace_max; the frame std
-reduction), translated to C++ by oracle/wgsl2cpp.py and built into
+reduction; correct_illumination), translated to C++ by oracle/wgsl2cpp.py and built into
 oracle/_ref/ from the reference checkout, on small seeded synthetic frames.
 
 The fixtures let the oracle and the GPU path be checked against the
