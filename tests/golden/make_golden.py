@@ -1,7 +1,7 @@
 """Writes tests/golden/trackpy_ref_64x96.npz and tests/golden/log_ref_48x56.npz:
 outputs of the reference's own WGSL shaders (preprocess_rows/cols, max_rows +
 extract_max, walk + characterize; separable_log, logspace_max; the frame std
-reduction; correct_illumination), translated to C++ by oracle/wgsl2cpp.py and built into
+reduction; correct_illumination; adaptive_filter), translated to C++ by oracle/wgsl2cpp.py and built into
 oracle/_ref/ from the reference checkout, on small seeded synthetic frames.
 
 The fixtures let the oracle and the GPU path be checked against the
@@ -33,6 +33,8 @@ CASES = [
     (dict(diameter=9, snr=1.2, minmass_snr=0.3), 14),
     # per-frame illumination correction: every stage sees frame / smoothed frame
     (dict(diameter=9, minmass=0.05, illumination_sigma=4.0, illumination_correction_per_frame=True), 15),
+    # adaptive_background: two adaptive_filter passes over the walked rows
+    (dict(diameter=9, adaptive_background=2, snr=0.3, minmass_snr=1.0), 16),
 ]
 T, H, W = 2, 64, 96
 
@@ -53,6 +55,8 @@ def main():
             std = loader.ref_frame_std(f) if ("snr" in kw or "minmass_snr" in kw) else 0.0
             cands = loader.ref_candidates(p, proc, pic_std=std)
             rows = loader.ref_walk(p, proc, f, cands, characterize=True, pic_std=std)
+            if kw.get("adaptive_background"):
+                rows = loader.ref_adaptive(p, f, rows, kw["adaptive_background"], std)
             if t == 0:
                 out["c%d_t%d_processed" % (c, t)] = proc
             out["c%d_t%d_candidates" % (c, t)] = cands
