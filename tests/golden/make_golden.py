@@ -1,7 +1,7 @@
 """Writes tests/golden/trackpy_ref_64x96.npz and tests/golden/log_ref_48x56.npz:
 outputs of the reference's own WGSL shaders (preprocess_rows/cols, max_rows +
 extract_max, walk + characterize; separable_log, logspace_max; the frame std
-reduction; correct_illumination; adaptive_filter), translated to C++ by oracle/wgsl2cpp.py and built into
+reduction; correct_illumination; adaptive_filter; characterize at given points), translated to C++ by oracle/wgsl2cpp.py and built into
 oracle/_ref/ from the reference checkout, on small seeded synthetic frames.
 
 The fixtures let the oracle and the GPU path be checked against the
@@ -64,6 +64,14 @@ def main():
         # the reference's frame std (snr / minmass_snr thresholds)
         out["c%d_std" % c] = np.array([loader.ref_frame_std(frames[t].astype(np.float32)) for t in range(T)],
                                       np.float32)
+    # characterize_points: the reference's characterize shader at given points
+    f = out["c1_frames"][0].astype(np.float32)
+    p = trackpy_params(9)
+    rng = np.random.default_rng(3)
+    pts = np.c_[rng.uniform(0, 63, 25), rng.uniform(0, 95, 25)].astype(np.float32)
+    pts[:3] = [[10.5, 20.5], [11.5, 21.5], [0.0, 0.0]]   # half-way rounding and a corner
+    out["cp_points"] = pts
+    out["cp_rows"] = loader.ref_characterize_points(p, loader.ref_preprocess(p, f), f, pts)
     path = os.path.join(HERE, "trackpy_ref_64x96.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")

@@ -151,3 +151,29 @@ def test_engine_log_matches_reference(golden_log, spacing):
     g = got[np.lexsort((got[:, 1], got[:, 0], got[:, 3]))]
     w = want[:, :4][np.lexsort((want[:, 1], want[:, 0], want[:, 3]))]
     assert same_floats(g, w)
+
+
+# characterize_points: oracle table columns / engine columns and the
+# reference's ResultRow fields (mass, Rg, raw, signal, ecc)
+CP_FIELDS = [("mass", 3, 2), ("Rg", 5, 5), ("raw", 6, 6), ("signal", 7, 7), ("ecc", 8, 8)]
+
+
+def test_oracle_characterize_points_matches_reference(oracle, golden):
+    f = golden["c1_frames"][:1].astype(np.float32)
+    pts, want = golden["cp_points"], golden["cp_rows"]
+    tab = oracle.characterize_points(trackpy_params(9), f, pts, False, False)
+    assert len(tab) == len(want) == len(pts)
+    for _, col, field in CP_FIELDS:
+        assert same_floats(tab[:, col], want[:, field]), col
+
+
+@pytest.mark.gpu
+def test_engine_characterize_points_matches_reference(golden):
+    import pandas as pd
+    import gpu_tracking_b200 as gt
+    f = golden["c1_frames"][:1]
+    pts, want = golden["cp_points"], golden["cp_rows"]
+    df = gt.characterize_points(f, pd.DataFrame({"y": pts[:, 0], "x": pts[:, 1]}), diameter=9, tqdm=False)
+    assert len(df) == len(want)
+    for name, _, field in CP_FIELDS:
+        assert same_floats(df[name].to_numpy(), want[:, field]), name
