@@ -55,9 +55,10 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="frames in the CPU-baseline sample (0: auto)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="headline", choices=["headline", "ragged", "learned"],
+    ap.add_argument("--workload", default="headline", choices=["headline", "ragged", "learned", "log"],
                     help="headline: the 2000-frame 2048^2 video; ragged: 64 videos of uneven size and length; "
-                         "learned: plain vs learned-proposal seeds on 1000 frames of 2048^2 at 4000 spots/frame")
+                         "learned: plain vs learned-proposal seeds on 1000 frames of 2048^2 at 4000 spots/frame; "
+                         "log: multi-scale LoG on 500 frames of 1024^2 float32")
     ap.add_argument("--learned-scale", type=float, default=1.0, help="learned: fraction of the 1000 frames timed")
     ap.add_argument("--epochs", type=float, default=3.0, help="learned: passes over the 200k training crops")
     ap.add_argument("--train-frames", type=int, default=800, help="learned: labelled frames the crops come from")
@@ -463,6 +464,116 @@ def run_learned(args):
     return 0
 
 
+LOG = dict(workload="multi-scale LoG detect+characterize+link, 500 frames 1024x1024 float32, 1500 blobs/frame",
+           frames=500, height=1024, width=1024, blobs_per_frame=1500, radius_px=[2.0, 8.0], read_noise=5.0,
+           background=50.0, snr=[3, 20], D=1.0, births_deaths=0.02, min_radius=2.0, max_radius=8.0, n_radii=10,
+           log_spacing=True, minmass=150.0, characterize=True, doughnut_correction=True, search_range=6.0,
+           memory=0, style="log", seed=3)
+
+
+def log_taps_per_pixel(p):
+    """Taps of the four separable passes of every radius, per pixel: each
+    radius r filters with 2*rint+1 taps, rint = int(4 r / sqrt(2) + 0.5)
+    (separable_log.wgsl), in each of its four passes."""
+    import math
+    import numpy as np
+    n = int(p.n_radii)
+    if p.log_spacing:
+        radii = np.logspace(math.log10(p.min_radius), math.log10(p.max_radius), n).astype(np.float32)
+    else:
+        radii = np.linspace(p.min_radius, p.max_radius, n).astype(np.float32)
+    return sum(4 * (2 * int(4.0 * float(r / np.float32(math.sqrt(2.0))) + 0.5) + 1) for r in radii)
+
+
+def run_log(args):
+    """Frames/s of the LoG workload, video resident in HBM, with an FP32
+    roofline of the scale-space kernel (its tap multiply-adds per frame)."""
+    import ctypes
+
+    import torch
+    from gpu_tracking_b200 import _ffi
+    from gpu_tracking_b200._params import DTYPE_F32, log_params
+    from gpu_tracking_b200.synth import blob_video
+    torch.cuda.set_device(0)
+    cfg = LOG
+    T = args.frames if args.frames != CONFIG["frames"] else cfg["frames"]
+    H = W = args.size if args.size != CONFIG["height"] else cfg["height"]
+    video = blob_video(T, H, W, cfg["blobs_per_frame"], seed=cfg["seed"], device="cuda:0",
+                       radius_range=tuple(cfg["radius_px"]), read_noise=cfg["read_noise"], bg=cfg["background"],
+                       snr_range=tuple(cfg["snr"]), D=cfg["D"], turnover=cfg["births_deaths"])
+    torch.cuda.synchronize()
+    p = log_params(cfg["min_radius"], cfg["max_radius"], n_radii=cfg["n_radii"], log_spacing=cfg["log_spacing"],
+                   minmass=cfg["minmass"], search_range=cfg["search_range"])
+    ctx = _ffi.context(0)
+    L = _ffi.lib()
+
+    def step():
+        out = ctypes.c_void_p()
+        ctx.check(L.gt_batch(ctx.handle, ctypes.byref(p), ctypes.c_void_p(video.data_ptr()), DTYPE_F32, T, H, W,
+                             None, None, 0, ctypes.byref(out)))
+        n = L.gt_table_nrows(out)
+        L.gt_table_free(out)
+        return n
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    ctx.profile(True)
+    l0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    rows = 0
+    for _ in range(args.steps):
+        rows += step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count() - l0
+    kernels = {}
+    for name in ("bandpass", "laplace", "logspace_max", "walk_characterize", "finalize", "scatter", "link_sort",
+                 "link_lists", "link_video", "link_rows"):
+        n, kms = ctx.profile_read(name)
+        if n:
+            kernels[name] = (n, kms)
+    ctx.profile(False)
+    clk = clocks.stop()
+    frames = T * args.steps
+    taps = log_taps_per_pixel(p)
+    flops_per_frame = 2.0 * taps * H * W
+    # FP32 peak: no measured figure exists for CUDA-core FP32, so the nominal
+    # one at the sampled SM clock: 148 SMs x 128 FP32 lanes x 2 flops
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    lap = kernels.get("laplace") or kernels.get("log_scale_space")
+    roofline = None
+    if lap:
+        achieved = flops_per_frame * frames / (lap[1] / 1000.0) / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak, "kernel": "laplace (+ logspace_max)",
+                    "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x 2 flops at the sampled SM clock",
+                    "flops_per_frame": flops_per_frame, "taps_per_pixel": taps, "traffic": None}
+    hbm_peak, hbm_kind = load_peaks()
+    total_k = sum(v[1] for v in kernels.values()) or 1.0
+    line = {"metric": "frames/s, multi-scale LoG 1024x1024 float32 (10 radii), detect+characterize+link",
+            "value": frames / (ms / 1000.0), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(cfg, frames=T, height=H, width=W,
+                           l2="inputs (%.1f GB) larger than L2; no flush" % (T * H * W * 4 / 1e9)),
+            "features_per_s": rows / (ms / 1000.0), "features_per_frame": rows / frames,
+            "gpu_launches": int(launches), "roofline": roofline,
+            "hbm": {"algorithmic_bytes_per_frame": H * W * 4 + rows / frames * 52.0, "peak": hbm_peak,
+                    "peak_kind": hbm_kind,
+                    "whole_step_frac": frames * (H * W * 4 + rows / frames * 52.0) / (ms / 1000.0) / 1e9 / hbm_peak},
+            "kernel_ms_per_frame": {k: v[1] / frames for k, v in kernels.items()},
+            "kernel_share": {k: round(v[1] / total_k, 4) for k, v in kernels.items()},
+            "clocks": clk}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -471,6 +582,8 @@ def main():
         return run_ragged(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "log":
+        return run_log(args)
     import ctypes
 
     import numpy as np

@@ -1829,6 +1829,24 @@ extern "C" {
 
 // internal accessors for the other translation units (not exported)
 int gt__ctx_device(const gt_ctx* ctx) { return ctx->device; }
+// GT_OK when `bytes` bytes from device pointer p lie inside the allocation
+// that holds p (cuMemGetAddressRange), or when the driver cannot tell;
+// GT_ERR_INVALID_ARGUMENT, with the context's message set, when they run past it.
+gt_status gt__device_span_check(gt_ctx* ctx, const void* p, size_t bytes, const char* what) {
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    AddressRangeFn fn = address_range_fn();
+    if (!fn || fn(&base, &size, (CUdeviceptr)p) != CUDA_SUCCESS) {
+        cudaGetLastError();
+        return GT_OK;
+    }
+    const uint64_t off = (uint64_t)(uintptr_t)p - (uint64_t)base;
+    if (off > size || bytes > size - off)
+        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
+                       "%s: %zu bytes from the pointer run past the end of its allocation (%zu bytes left)", what,
+                       bytes, (size_t)(size - std::min<uint64_t>(off, size)));
+    return GT_OK;
+}
 cudaStream_t gt__ctx_stream(const gt_ctx* ctx) { return ctx->st; }
 void gt__ctx_set_error(gt_ctx* ctx, const char* msg) { ctx->err = msg; }
 
@@ -1840,6 +1858,26 @@ GT_API gt_status gt__set_link_window_caps(gt_ctx* ctx, int64_t list_entries, int
     if (!ctx) return GT_ERR_INVALID_ARGUMENT;
     ctx->w_list_cap = list_entries;
     ctx->w_edge_cap = edges_per_frame;
+    return GT_OK;
+}
+
+// Test hook (exported, not part of the public header): the per-frame
+// candidate and detection capacities the next gt_batch starts from (values
+// <= 0 keep the current ones).  Small values make the kernels report overflow
+// and the call replay with grown capacities, the path that replaces the
+// reference's silent truncation (src/gpu_setup.rs:246-253).
+GT_API gt_status gt__set_capacities(gt_ctx* ctx, int64_t cand_cap, int64_t feat_cap) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    if (cand_cap > 0) ctx->cand_cap = (uint32_t)std::min<int64_t>(cand_cap, 1LL << 30);
+    if (feat_cap > 0) ctx->feat_cap = (uint32_t)std::min<int64_t>(feat_cap, 1LL << 24);
+    return GT_OK;
+}
+
+// Test hook: the capacities the last call ended with.
+GT_API gt_status gt__get_capacities(const gt_ctx* ctx, int64_t* cand_cap, int64_t* feat_cap) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    if (cand_cap) *cand_cap = ctx->cand_cap;
+    if (feat_cap) *feat_cap = ctx->feat_cap;
     return GT_OK;
 }
 

@@ -23,7 +23,12 @@
 //
 // The device address of the array is looked up with cudaGetSymbolAddress
 // once per device, on the first call made with that device current; make
-// that first call before any stream capture begins.
+// that first call before any stream capture begins.  The address stays valid
+// for the life of the process's CUDA context on that device: a
+// cudaDeviceReset (which also ends this library's contexts) is not supported
+// while the library is in use.  Every call reads sizes back to the host and
+// synchronises the context's stream before it returns.  The caller's current
+// device is restored on return.
 #include <mutex>
 
 #include "gt_kernels.h"
@@ -206,6 +211,23 @@ using namespace gt;
 extern "C" int gt__ctx_device(const gt_ctx* ctx);
 extern "C" cudaStream_t gt__ctx_stream(const gt_ctx* ctx);
 extern "C" void gt__ctx_set_error(gt_ctx* ctx, const char* msg);
+extern "C" gt_status gt__device_span_check(gt_ctx* ctx, const void* p, size_t bytes, const char* what);
+
+namespace {
+// Restores the calling thread's current device when the call returns.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+}  // namespace
 
 static gt_status noalloc_fail(gt_ctx* ctx, gt_status st, const char* msg) {
     gt__ctx_set_error(ctx, msg);
@@ -224,12 +246,9 @@ extern "C" gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_fyx, int64_t n,
     if (n < 0) return noalloc_fail(ctx, GT_ERR_INVALID_ARGUMENT, "negative row count");
     if (n == 0) return GT_OK;
     if (!d_fyx || !d_out) return noalloc_fail(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
-    if (n > kNoAllocMaxPoints)
-        return noalloc_fail(ctx, GT_ERR_CAPACITY_EXCEEDED, "gt_link_noalloc links at most 32768 detections");
-    if (memory > (uint32_t)kNoAllocMaxMemory)
-        return noalloc_fail(ctx, GT_ERR_CAPACITY_EXCEEDED, "gt_link_noalloc supports memory <= 3");
     const int dev = gt__ctx_device(ctx);
     cudaStream_t st = gt__ctx_stream(ctx);
+    DeviceGuard restore_device;
     NA_CK(cudaSetDevice(dev));
     for (const void* ptr : {(const void*)d_fyx, (const void*)d_out}) {
         cudaPointerAttributes at;
@@ -239,6 +258,17 @@ extern "C" gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_fyx, int64_t n,
             return noalloc_fail(ctx, GT_ERR_INVALID_ARGUMENT, "gt_link_noalloc takes device pointers of the context's device");
         }
     }
+    // the n rows read and the n ids written must lie inside their allocations
+    {
+        gt_status s = gt__device_span_check(ctx, d_fyx, (size_t)n * 12, "gt_link_noalloc rows (n x 3 float32)");
+        if (s != GT_OK) return s;
+        s = gt__device_span_check(ctx, d_out, (size_t)n * 8, "gt_link_noalloc ids (n int64)");
+        if (s != GT_OK) return s;
+    }
+    if (n > kNoAllocMaxPoints)
+        return noalloc_fail(ctx, GT_ERR_CAPACITY_EXCEEDED, "gt_link_noalloc links at most 32768 detections");
+    if (memory > (uint32_t)kNoAllocMaxMemory)
+        return noalloc_fail(ctx, GT_ERR_CAPACITY_EXCEEDED, "gt_link_noalloc supports memory <= 3");
     const NoAllocLayout L = noalloc_layout();
     if (L.total > kNoAllocBytes) return noalloc_fail(ctx, GT_ERR_INTERNAL, "static scratch layout too large");
     uint8_t* base;
@@ -313,6 +343,9 @@ extern "C" gt_status gt_link_noalloc(gt_ctx* ctx, const float* d_fyx, int64_t n,
     LL.b_pts = (int32_t*)(base + L.bpts);
     LL.b_dist = (float*)(base + L.bdist);
     LL.srt = srt;
+    // the list sizes select the linker variant with 32-bit list offsets when
+    // they fit, as gt_link does (a larger shared-memory working set per frame)
+    LL.f_entries = tots[0];
     NA_CK(link_fill_lists(in, LL, st));
     LinkScratch S;
     S.base = base + L.lay;

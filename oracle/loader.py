@@ -25,12 +25,21 @@ def _ptr(a, t):
     return a.ctypes.data_as(t)
 
 
+def reference_root():
+    """The reference checkout: $GT_REFERENCE_ROOT, else a ``reference``
+    directory beside this repository's root."""
+    env = os.environ.get("GT_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build():
     """Compile the oracle (and the reference translation when the checkout exists)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir(os.environ.get("GT_REFERENCE_ROOT", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref",
-                        "REF=" + os.environ.get("GT_REFERENCE_ROOT", "/root/reference")], check=True)
+    ref = reference_root()
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + ref], check=True)
 
 
 def lib():
