@@ -12,10 +12,19 @@
 // the reference's own WGSL source executed on the CPU: oracle/wgsl2cpp.py
 // translates the reference checkout's src/shaders/*.wgsl into C++ at build time
 // (output only under oracle/_ref/, never committed) and tests compare both.
-// The Rust post-processing (filter_close, doughnut, prune_blobs_log) and the
-// linker cannot be executed here (no Rust toolchain); they are pinned only by
-// hand-derived known-answer cases in tests/test_oracle_linking.py
-// ("parity partially pinned" for those rows).
+// The Rust post-processing (filter_close_trackpy, prune_blobs_log, the
+// doughnut block of post_process, the column layout and durations) and the
+// linker (Linker, link, linker_all, connect_all) are pinned the same way:
+// oracle/rust2py.py translates the reference's own Rust source into Python at
+// build time (oracle/_ref/rust_ref.py, run by oracle/ref_post.py with Rust's
+// binary32 and integer semantics), and tests/test_golden_post.py compares this
+// file with it on randomized inputs and against the committed fixture
+// tests/golden/postprocess_ref.npz.  The one piece not taken from the
+// reference is the neighbour order of the kd-tree crate (kd-tree 0.5.1,
+// not vendored): neighbour lists are in index order here and in the
+// translation's shim; the order decides only exact score ties in the
+// subnet search.  tests/test_oracle_linking.py keeps its hand-derived
+// known-answer cases.
 //
 // Floating-point conventions (shared with the CUDA kernels, which are
 // bit-exact against this file):

@@ -4,6 +4,14 @@ extract_max, walk + characterize; separable_log, logspace_max; the frame std
 reduction; correct_illumination; adaptive_filter; characterize at given points), translated to C++ by oracle/wgsl2cpp.py and built into
 oracle/_ref/ from the reference checkout, on small seeded synthetic frames.
 
+It also writes tests/golden/postprocess_ref.npz: whole tables (every column,
+particle ids and durations) of the reference's own path — its shaders, then
+its Rust post-processing (filter_close_trackpy, prune_blobs_log, the
+doughnut block, column layout) and its Linker — with the Rust translated to
+Python by oracle/rust2py.py (oracle/_ref/rust_ref.py) and driven by
+oracle/ref_post.py; and the particle ids of its link_rust / connect_rust
+paths (linker_all, connect_all) on seeded detection sets.
+
 The fixtures let the oracle and the GPU path be checked against the
 reference's shaders on machines that have no reference checkout.  Run from
 the repository root after building the oracle and its reference translation:
@@ -101,5 +109,80 @@ def main():
     print(path, os.path.getsize(path), "bytes")
 
 
+# whole-path cases: (style, keyword arguments, linker_reset_points)
+POST_CASES = [
+    ("trackpy", dict(diameter=9, minmass=300.0, search_range=5.0, memory=1), None),
+    ("trackpy", dict(diameter=7, minmass=100.0, separation=6, bg_radius=8.0, gap_radius=1.5, search_range=4.0,
+                     memory=2), [1]),
+    ("trackpy", dict(diameter=11, minmass=200.0, filter_close=False, doughnut_correction=False, search_range=6.0),
+     None),
+    ("trackpy", dict(diameter=9, minmass=250.0, characterize=False, search_range=5.0, memory=3), None),
+    ("log", dict(min_radius=2.0, max_radius=6.0, n_radii=4, minmass=50.0, search_range=5.0), None),
+    ("log", dict(min_radius=2.0, max_radius=6.0, n_radii=5, log_spacing=True, overlap_threshold=0.3, minmass=20.0,
+                 search_range=6.0, memory=1), None),
+]
+# link_rust / connect_rust cases: (seed, frames, points, search_range, memory, first frame)
+LINK_CASES = [(31, 12, 40, 5.0, 0, 0), (32, 15, 50, 5.0, 3, 0), (33, 10, 30, 4.0, 1, 4)]
+CONNECT_CASES = [(41, 6, 30, 2.0), (42, 5, 20, 3.0)]
+
+
+def detections(seed, T, n, R, size, first_frame=0):
+    """Seeded (frame, y, x) rows: n points doing Brownian steps of R/3,
+    5 % missing per frame, 10 % replaced by new points per frame."""
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0, size, (n, 2))
+    rows = []
+    for t in range(T):
+        keep = rng.random(n) > 0.05
+        for k in np.flatnonzero(keep):
+            rows.append((first_frame + t, pos[k, 0], pos[k, 1]))
+        pos = pos + rng.normal(0, R / 3, pos.shape)
+        dead = rng.random(n) < 0.1
+        pos[dead] = rng.uniform(0, size, (dead.sum(), 2))
+    return np.array(rows, np.float32)
+
+
+def post_main():
+    from oracle import ref_post
+    if not ref_post.available():
+        raise SystemExit("the reference's Rust translation (oracle/_ref/rust_ref.py) is not built")
+    out = {}
+    tp_frames, _ = video(6, 64, 80, 22, seed=21, D=0.8)
+    log_frames, _ = video(4, 48, 56, 10, seed=22, dtype=np.float32, read_noise=5.0, bg=50.0,
+                          sigma_range=(1.4, 4.0), D=0.5)
+    out["tp_frames"] = tp_frames.astype(np.uint16)
+    out["log_frames"] = log_frames
+    for c, (style, kw, reset) in enumerate(POST_CASES):
+        if style == "trackpy":
+            p = trackpy_params(**kw)
+            frames = tp_frames.astype(np.float32)
+        else:
+            kw2 = dict(kw)
+            p = log_params(kw2.pop("min_radius"), kw2.pop("max_radius"), **kw2)
+            frames = log_frames
+        table, cols = ref_post.batch(p, frames, linker_reset_points=reset)
+        out["post%d_table" % c] = table
+        out["post%d_columns" % c] = np.array(cols)
+    for c, (seed, T, n, R, mem, first) in enumerate(LINK_CASES):
+        rows = detections(seed, T, n, R, 100.0, first)
+        out["link%d_rows" % c] = rows
+        out["link%d_ids" % c] = ref_post.link(rows, R, mem)
+    for c, (seed, T, n, R) in enumerate(CONNECT_CASES):
+        a = detections(seed, T, n, R, 60.0)
+        b = a.copy()
+        rng = np.random.default_rng(seed)
+        b[:, 1:] += rng.normal(0, R / 2, (len(b), 2)).astype(np.float32)
+        b = b[rng.random(len(b)) > 0.2]
+        out["connect%d_a" % c] = a
+        out["connect%d_b" % c] = b
+        ia, ib = ref_post.connect(a, b, R)
+        out["connect%d_ia" % c] = ia
+        out["connect%d_ib" % c] = ib
+    path = os.path.join(HERE, "postprocess_ref.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     main()
+    post_main()
