@@ -532,7 +532,7 @@ def run_log(args):
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launch_count() - l0
     kernels = {}
-    for name in ("bandpass", "laplace", "logspace_max", "walk_characterize", "finalize", "scatter", "link_sort",
+    for name in ("bandpass", "log_scale_space", "laplace", "logspace_max", "walk_characterize", "finalize", "scatter", "link_sort",
                  "link_lists", "link_video", "link_rows"):
         n, kms = ctx.profile_read(name)
         if n:

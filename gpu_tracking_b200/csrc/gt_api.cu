@@ -477,6 +477,9 @@ struct LogTables {
     std::vector<float> radii, taps_g, taps_d, norm_g, norm_d;
     std::vector<int32_t> tap_off, rints;
     int max_rint = 0;
+    // the scale space runs as one fused kernel (gt_logss.cu) when its tiles
+    // fit; otherwise as a plane per radius plus a maxima pass
+    bool fused() const { return log_scale_space_supported(max_rint, (int)taps_g.size()); }
 };
 
 // separable_log.wgsl:27-76 tap values, computed per radius with sigma = r / sqrt(2)
@@ -992,7 +995,7 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     const int SC = F * per_super;
     const int nsuper = (int)((NT + SC - 1) / SC);
     CK(ctx->processed.ensure((size_t)F * npx * 4));
-    if (log_style) CK(ctx->planes.ensure((size_t)F * nslots * npx * 4));
+    if (log_style && !lt->fused()) CK(ctx->planes.ensure((size_t)F * nslots * npx * 4));
     CK(ctx->cand_count.ensure((size_t)F * nslots * 4));
     CK(ctx->cand_keys.ensure((size_t)F * nslots * cand_cap * 4));
     CK(ctx->feats_raw.ensure((size_t)SC * feat_cap * sizeof(Feature)));
@@ -1208,16 +1211,26 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                         CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
                                               ctx->st));
                     }
-                    {
-                        Prof pf(ctx, "laplace");
-                        CK(launch_laplace<TS>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
-                                             ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
-                                             lnd.as<float>(), lt->max_rint, nf, ctx->st));
-                    }
-                    {
-                        Prof pf(ctx, "logspace_max");
-                        CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf, ctx->cand_count.as<uint32_t>(),
-                                               ctx->cand_keys.as<uint32_t>(), cand_cap, flags, ctx->st));
+                    if (lt->fused()) {
+                        Prof pf(ctx, "log_scale_space");
+                        CK(launch_log_scale_space<TS>(src, (int64_t)npx, proc, lc, ltg.as<float>(), ltd.as<float>(),
+                                                     loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
+                                                     lnd.as<float>(), lt->max_rint, (int)lt->taps_g.size(), nf,
+                                                     ctx->cand_count.as<uint32_t>(), ctx->cand_keys.as<uint32_t>(),
+                                                     cand_cap, flags, ctx->st));
+                    } else {
+                        {
+                            Prof pf(ctx, "laplace");
+                            CK(launch_laplace<TS>(src, (int64_t)npx, ctx->planes.as<float>(), lc, ltg.as<float>(),
+                                                 ltd.as<float>(), loff.as<int32_t>(), lrint.as<int32_t>(),
+                                                 lng.as<float>(), lnd.as<float>(), lt->max_rint, nf, ctx->st));
+                        }
+                        {
+                            Prof pf(ctx, "logspace_max");
+                            CK(launch_logspace_max(ctx->planes.as<float>(), proc, lc, nf,
+                                                   ctx->cand_count.as<uint32_t>(), ctx->cand_keys.as<uint32_t>(),
+                                                   cand_cap, flags, ctx->st));
+                        }
                     }
                 }
                 sum_counts_kernel<<<1, 256, 0, ctx->st>>>(ctx->cand_count.as<uint32_t>(), nf * nslots, cand_cap,
@@ -1363,7 +1376,7 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         lt = log_tables(p);
         if (lt.radii.empty()) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "n_radii must be >= 1");
         if (lt.radii.size() > (size_t)kMaxRadii) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "n_radii > 256");
-        if (laplace_smem_bytes(lt.max_rint) > 227 * 1024)
+        if (!lt.fused() && laplace_smem_bytes(lt.max_rint) > 227 * 1024)
             return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "max_radius too large for the LoG tile kernel");
     } else {
         if (bandpass_smem_bytes(c.R, c.kd, true) > 227 * 1024)
@@ -1388,7 +1401,7 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
             return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
                            "adaptive_background >= 2 needs snr or minmass_snr (the image std between passes)");
     }
-    const int F = pick_chunk(NT, H, W, log_style ? (int)lt.radii.size() : 0);
+    const int F = pick_chunk(NT, H, W, (log_style && !lt.fused()) ? (int)lt.radii.size() : 0);
     ctx->total = NT;
     ctx->done = 0;
     std::vector<int64_t> fnum(NT);

@@ -172,6 +172,18 @@ cudaError_t launch_logspace_max(const float* planes, const float* processed, con
                                 uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags,
                                 cudaStream_t st);
 
+// fused scale space (gt_logss.cu): the LoG planes of every radius and their
+// 3x3x3 maxima in one pass over the frame, for rint <= kLogSSMaxR
+constexpr int kLogSSMaxR = 32;
+size_t log_scale_space_smem_bytes(int max_rint, int ntaps_total);
+bool log_scale_space_supported(int max_rint, int ntaps_total);
+template <typename T>
+cudaError_t launch_log_scale_space(const T* frames, int64_t frame_stride, const float* processed, const LogConsts& lc,
+                                   const float* taps_g, const float* taps_d, const int32_t* tap_off,
+                                   const int32_t* rints, const float* norm_g, const float* norm_d, int max_rint,
+                                   int ntaps_total, int nframes, uint32_t* cand_count, uint32_t* cand_keys,
+                                   uint32_t cand_cap, uint32_t* flags, cudaStream_t st);
+
 // mean frame (src/execute_gpu.rs:819-847)
 template <typename T>
 cudaError_t launch_mean_frame(const T* frames, int64_t T_, int64_t npix, float* out, cudaStream_t st);

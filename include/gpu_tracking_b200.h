@@ -323,7 +323,7 @@ GT_API const char* gt_version(void);
 /* Per-kernel timing with CUDA events on the engine's compute stream (no
  * counterpart in the reference): enable, run calls, then read the launch
  * count and summed milliseconds of a kernel class ("bandpass_localmax",
- * "walk_characterize", "finalize", "bandpass", "laplace", "logspace_max",
+ * "walk_characterize", "finalize", "bandpass", "log_scale_space", "laplace", "logspace_max",
  * "link_sort", "link_lists", "link_video"). */
 GT_API gt_status gt_profile_enable(gt_ctx* ctx, int32_t enable);
 GT_API gt_status gt_profile_read(gt_ctx* ctx, const char* name, int64_t* launches, double* total_ms);

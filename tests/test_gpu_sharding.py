@@ -1,7 +1,9 @@
 """batch_sharded with two ranks (gloo on 127.0.0.1) sharing one GPU: each
-rank locates its half of the frames, rank 0 gathers and links, and the table
-equals batch() on the whole video.  The ranks' kernels never wait on each
-other; they meet only through gloo on the host."""
+rank tracks its half of the frames (plus a prefix) with the engine, the
+chunk boundary is verified and the ids relabelled, and the table gathered on
+rank 0 equals batch() on the whole video in every column, particle ids and
+durations included.  The ranks' kernels never wait on each other; they meet
+only through gloo on the host."""
 import os
 import socket
 import sys
@@ -33,14 +35,13 @@ def worker(rank, world, port, q):
         import gpu_tracking_b200 as gt
         from gpu_tracking_b200 import sharding
         from synth import video
-        frames, _ = video(9, 96, 128, 30, seed=77, D=0.6)
-        kw = dict(minmass=300.0, search_range=5.0, memory=1, tqdm=False)
+        frames, _ = video(16, 96, 128, 30, seed=77, D=1.2, turnover=0.08)
+        kw = dict(minmass=300.0, search_range=6.0, memory=2, tqdm=False)
         df = sharding.batch_sharded(frames, 9, **kw)
         if rank == 0:
             whole = gt.batch(frames, 9, **kw)
-            cols = [c for c in whole.columns if c != "duration"]
-            same = len(df) == len(whole) and all(
-                np.array_equal(df[c].to_numpy(), whole[c].to_numpy()) for c in cols)
+            same = len(df) == len(whole) and list(df.columns) == list(whole.columns) and all(
+                np.array_equal(df[c].to_numpy(), whole[c].to_numpy()) for c in whole.columns)
             q.put((rank, same, len(df)))
         else:
             q.put((rank, df is None, 0))
