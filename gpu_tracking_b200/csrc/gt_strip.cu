@@ -5,9 +5,12 @@
 // instruction throughput.  A CTA owns a strip of 128 output columns and walks
 // down a segment of rows eight rows per step:
 //   A  the step's raw rows are staged in shared memory (4 pixels per load,
-//      converted exactly to float), the next step's are prefetched;
-//   B  row pass: each thread makes 4 adjacent columns from float4 loads;
-//   C  column pass: each thread makes the step's 8 rows of one column;
+//      converted exactly to float) as pairs of rows j and j + 4, the next
+//      step's are prefetched;
+//   B  row pass: each thread makes 4 adjacent columns of rows j and j + 4,
+//      the two rows as the lanes of packed f32x2 operations;
+//   C  column pass: each thread makes 2 adjacent columns of 2 rows, the two
+//      columns as the lanes of packed f32x2 operations;
 //   D  vertical dilation maximum, 8 rows of one column per thread;
 //   E  horizontal dilation maximum, the candidate test and the store of the
 //      segment's processed rows, 4 columns per thread, slots reserved once
@@ -16,6 +19,9 @@
 // every row twice (at r and r + ring), so any window of consecutive rows is
 // contiguous and every read in the tap loops is a constant offset from one
 // base address.  The tap loops are unrolled for the compile-time radius.
+// Packed f32x2 arithmetic (__ffma2_rn, __fadd2_rn, __fmul2_rn) rounds each
+// lane as its scalar operation does, so the packed stages compute the same
+// values as one scalar operation per pixel.
 // The floating-point operation sequence of every output is the oracle's:
 // sequential fused multiply-adds over the taps, sequential boxcar sums (for
 // integer inputs a pairwise window sum and sliding differences instead: every
@@ -59,8 +65,11 @@ struct StripGeom {
     static constexpr int RAWN = kStepRows * RWp;
     static constexpr int RAWPT = (RAWN + kStripThreads - 1) / kStripThreads;
     // the vertical maxima (stages D-E) reuse the staged raw rows (stages A-B)
-    static constexpr size_t smem_floats = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp +
-                                          (size_t)(2 * PR) * PWp;
+    // tap and divisor pairs for the packed stages follow the rings
+    static constexpr size_t off_pairs = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp + (size_t)(2 * PR) * PWp;
+    static constexpr size_t smem_floats = off_pairs + 2 * (2 * R + 1) + 8;
+    static constexpr int RAWV2 = (kStepRows / 2) * RW4;   // staging items: 4 pixels of rows j and j + 4
+    static constexpr int RAWV2PT = (RAWV2 + kStripThreads - 1) / kStripThreads;
     static constexpr int min_blocks = (smem_floats * 4 + 1024) * 3 <= 227 * 1024 ? 3 : 2;
     static_assert(RWp % 4 == 0 && RWp >= PWp + 2 * R, "staged raw row");
     static_assert(RWp >= PWp, "vertical maxima fit in the staging rows");
@@ -68,6 +77,7 @@ struct StripGeom {
     static_assert(4 * 31 + KD + 2 <= PW - 1 && SH4 + O + kStripTW <= PWp, "dilation windows inside the row");
     static_assert(KD >= kStepRows && kStepRows == 8, "vertical maxima: 8 rows share the window rows 7 .. KD-1");
     static_assert(PWp <= kStripThreads, "one thread per column in the column pass and vertical maxima");
+    static_assert(PWp % 2 == 0 && off_pairs % 2 == 0, "column pairs and tap pairs are 8-byte aligned");
 };
 
 template <typename T>
@@ -126,6 +136,31 @@ struct Tree<1> {
     __device__ __forceinline__ static float sum(const float* a) { return a[0]; }
 };
 
+template <int N>
+struct Tree2 {
+    __device__ __forceinline__ static float2 sum(const float2* a) {
+        return __fadd2_rn(Tree2<N / 2>::sum(a), Tree2<N - N / 2>::sum(a + N / 2));
+    }
+};
+template <>
+struct Tree2<1> {
+    __device__ __forceinline__ static float2 sum(const float2* a) { return a[0]; }
+};
+
+// a - b per lane (IEEE subtraction is addition of the negation)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+
+// x / gnorm and x / kk per lane; dz holds (zh_g, zl_g, zh_k, zl_k) as pairs
+template <bool FAST>
+__device__ __forceinline__ float2 div2_gnorm(float2 x, const float2* dz, const LocateConsts& c) {
+    return FAST ? __ffma2_rn(x, dz[0], __fmul2_rn(x, dz[1]))
+                : make_float2(__fdiv_rn(x.x, c.gnorm), __fdiv_rn(x.y, c.gnorm));
+}
+template <bool FAST>
+__device__ __forceinline__ float2 div2_kk(float2 x, const float2* dz, const LocateConsts& c) {
+    return FAST ? __ffma2_rn(x, dz[2], __fmul2_rn(x, dz[3])) : make_float2(__fdiv_rn(x.x, c.kk), __fdiv_rn(x.y, c.kk));
+}
+
 template <bool FAST>
 __device__ __forceinline__ float div_gnorm(float x, const LocateConsts& c) {
     return FAST ? __fmaf_rn(x, c.zh_g, __fmul_rn(x, c.zl_g)) : __fdiv_rn(x, c.gnorm);
@@ -150,6 +185,9 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     float* xb = xg + 2 * XR * PWp;              // [2XR][PWp]    row pass boxcar
     float* pr = xb + 2 * XR * PWp;              // [2PR][PWp]    processed rows, stored twice
     float* vb = stage;                          // [8][PWp]      vertical maxima (pc0-relative columns)
+    float2* stage2 = (float2*)stage;            // [4][RWp]      (row j, row j + 4) pixel pairs
+    float2* tp2 = (float2*)(sm + G::off_pairs); // [2R+1]        (tap, tap)
+    float2* dz = tp2 + (2 * R + 1);             // [4]           divisor pairs
 
     const int H = c.H, W = c.W;
     const int f = blockIdx.z;
@@ -171,18 +209,20 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
     // ---- A: staging of raw rows (registers hold the next step's pixels)
-    typename Quad<T>::V pv[G::RAWVPT];
+    typename Quad<T>::V pv[G::RAWV2PT][2];
     float ps_[G::RAWPT];
     auto load_raw = [&](int s) {
         const int rbase = x0 + kStepRows * s;
         if (vec) {
 #pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
+            for (int q = 0; q < G::RAWV2PT; q++) {
                 const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
+                if (v < G::RAWV2) {
                     const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    const int gr = min(max(rbase + j, 0), H - 1);
-                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
+                    const int gr0 = min(max(rbase + j, 0), H - 1);
+                    const int gr1 = min(max(rbase + j + 4, 0), H - 1);
+                    pv[q][0] = Quad<T>::load(img + (size_t)gr0 * W + xa + 4 * k4);
+                    pv[q][1] = Quad<T>::load(img + (size_t)gr1 * W + xa + 4 * k4);
                 }
             }
         } else {
@@ -208,6 +248,13 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     // start as zeros instead of whatever the previous kernel left.
     for (int i = tid; i < 2 * 2 * XR * PWp / 4; i += kStripThreads)
         ((float4*)xg)[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (tid <= 2 * R) tp2[tid] = make_float2(c.taps[tid], c.taps[tid]);
+    if (tid == 0) {
+        dz[0] = make_float2(c.zh_g, c.zh_g);
+        dz[1] = make_float2(c.zl_g, c.zl_g);
+        dz[2] = make_float2(c.zh_k, c.zh_k);
+        dz[3] = make_float2(c.zl_k, c.zl_k);
+    }
     const float trunc_thr = 1.0f / 255.0f;
     // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
     const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
@@ -216,128 +263,161 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     for (int s = 0; s < nsteps; s++) {
         if (vec) {
 #pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
+            for (int q = 0; q < G::RAWV2PT; q++) {
                 const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
+                if (v < G::RAWV2) {
                     const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    *(float4*)(stage + j * RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
+                    const float4 a = Quad<T>::cvt(pv[q][0]), b = Quad<T>::cvt(pv[q][1]);
+                    float4* dst = (float4*)(stage2 + j * RWp + 4 * k4);
+                    dst[0] = make_float4(a.x, b.x, a.y, b.y);
+                    dst[1] = make_float4(a.z, b.z, a.w, b.w);
                 }
             }
         } else {
 #pragma unroll
             for (int q = 0; q < G::RAWPT; q++) {
                 const int idx = tid + q * kStripThreads;
-                if (idx < G::RAWN) stage[idx] = ps_[q];
+                if (idx < G::RAWN) {
+                    const int j = idx / RWp, k = idx - j * RWp;
+                    stage[((j & 3) * RWp + k) * 2 + (j >> 2)] = ps_[q];
+                }
             }
         }
         __syncthreads();
         if (s + 1 < nsteps) load_raw(s + 1);
 
-        // ---- B: row pass (preprocess_rows.wgsl), 8 rows x PWp columns, 4 per thread
-        {
-            for (int t = tid; t < kStepRows * G::NG; t += kStripThreads) {
-                const int j = t / G::NG, gq = t - j * G::NG;
-                const int col = 4 * gq;
-                const float4* src = (const float4*)(stage + j * RWp + col);
-                float x[4 * G::NX4];
+        // ---- B: row pass (preprocess_rows.wgsl), rows j and j + 4 as the two
+        // lanes, 4 columns per thread
+        for (int t = tid; t < (kStepRows / 2) * G::NG; t += kStripThreads) {
+            const int jp = t / G::NG, gq = t - jp * G::NG;
+            const int col = 4 * gq;
+            const float4* src = (const float4*)(stage2 + jp * RWp + col);
+            float2 x[4 * G::NX4];
 #pragma unroll
-                for (int i = 0; i < G::NX4; i++) {
-                    const float4 v = src[i];
-                    x[4 * i] = v.x;
-                    x[4 * i + 1] = v.y;
-                    x[4 * i + 2] = v.z;
-                    x[4 * i + 3] = v.w;
-                }
-                float og[4], ob[4];
-                float cs = 0.0f;
+            for (int i = 0; i < 2 * G::NX4; i++) {
+                const float4 v = src[i];
+                x[2 * i] = make_float2(v.x, v.y);
+                x[2 * i + 1] = make_float2(v.z, v.w);
+            }
+            float2 og[4], ob[4];
+            float2 cs = make_float2(0.0f, 0.0f);
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    float gs = 0.0f;
-                    if (!edge_cols) {
+            for (int k = 0; k < 4; k++) {
+                float2 gs = make_float2(0.0f, 0.0f);
+                if (!edge_cols) {
 #pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
-                    } else {
-                        // Gaussian taps outside the frame are skipped
-                        const int gcol = ps + col + k;
+                    for (int i = 0; i <= 2 * R; i++) gs = __ffma2_rn(tp2[i], x[k + i], gs);
+                } else {
+                    // Gaussian taps outside the frame are skipped
+                    const int gcol = ps + col + k;
 #pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) {
-                            const int gc = gcol + i - R;
-                            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
+                    for (int i = 0; i <= 2 * R; i++) {
+                        const int gc = gcol + i - R;
+                        if (gc >= 0 && gc < W) {
+                            gs.x = __fmaf_rn(c.taps[i], x[k + i].x, gs.x);
+                            gs.y = __fmaf_rn(c.taps[i], x[k + i].y, gs.y);
                         }
                     }
-                    if (kInt) {
-                        // exact integers: the window sum, then sliding differences
-                        if (k == 0) cs = Tree<2 * R + 1>::sum(x);
-                        else cs = __fadd_rn(cs, __fsub_rn(x[k + 2 * R], x[k - 1]));
-                    } else {
-                        cs = 0.0f;
-#pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, x[k + i]);
-                    }
-                    og[k] = div_gnorm<FAST>(gs, c);
-                    ob[k] = cs;
                 }
-                const int xrow = (kStepRows * s + j) % XR;
-                const float4 g4 = make_float4(og[0], og[1], og[2], og[3]);
-                const float4 b4 = make_float4(ob[0], ob[1], ob[2], ob[3]);
-                *(float4*)(xg + xrow * PWp + col) = g4;
-                *(float4*)(xg + (xrow + XR) * PWp + col) = g4;
-                *(float4*)(xb + xrow * PWp + col) = b4;
-                *(float4*)(xb + (xrow + XR) * PWp + col) = b4;
+                if (kInt) {
+                    // exact integers: the window sum, then sliding differences
+                    if (k == 0) cs = Tree2<2 * R + 1>::sum(x);
+                    else cs = __fadd2_rn(cs, sub2(x[k + 2 * R], x[k - 1]));
+                } else {
+                    cs = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (int i = 0; i <= 2 * R; i++) cs = __fadd2_rn(cs, x[k + i]);
+                }
+                og[k] = div2_gnorm<FAST>(gs, dz, c);
+                ob[k] = cs;
             }
+            const int r0 = (kStepRows * s + jp) % XR, r1 = (kStepRows * s + jp + 4) % XR;
+            const float4 g0 = make_float4(og[0].x, og[1].x, og[2].x, og[3].x);
+            const float4 g1 = make_float4(og[0].y, og[1].y, og[2].y, og[3].y);
+            const float4 b0_ = make_float4(ob[0].x, ob[1].x, ob[2].x, ob[3].x);
+            const float4 b1_ = make_float4(ob[0].y, ob[1].y, ob[2].y, ob[3].y);
+            *(float4*)(xg + r0 * PWp + col) = g0;
+            *(float4*)(xg + (r0 + XR) * PWp + col) = g0;
+            *(float4*)(xg + r1 * PWp + col) = g1;
+            *(float4*)(xg + (r1 + XR) * PWp + col) = g1;
+            *(float4*)(xb + r0 * PWp + col) = b0_;
+            *(float4*)(xb + (r0 + XR) * PWp + col) = b0_;
+            *(float4*)(xb + r1 * PWp + col) = b1_;
+            *(float4*)(xb + (r1 + XR) * PWp + col) = b1_;
         }
         __syncthreads();
 
         // ---- C: column pass (preprocess_cols.wgsl) for the step's 8 processed
-        // rows q = x0 + 8s - R + k, one column per thread
-        if (tid < PWp) {
-            const int pc = tid;
-            const int q0 = x0 + kStepRows * s - R;
-            const int gcol = ps + pc;
-            // row-pass rows q0 - R .. q0 + 7 + R: relative index 8s - 2R + i
+        // rows q = x0 + 8s - R + k: each thread makes 2 adjacent columns (the
+        // two lanes) of 2 rows
+        {
+            constexpr int NP = PWp / 2;
+            // row-pass rows of processed row q: relative index 8s - 2R + k + i
             const int w0 = (kStepRows * s + (XR - 2 * R)) % XR;
-            const float* pg = xg + w0 * PWp + pc;
-            const float* pb = xb + w0 * PWp + pc;
-            float vg[kStepRows + 2 * R], vbx[kStepRows + 2 * R];
-#pragma unroll
-            for (int i = 0; i < kStepRows + 2 * R; i++) {
-                vg[i] = pg[i * PWp];
-                vbx[i] = pb[i * PWp];
-            }
-            const bool col_in = (gcol >= 0 && gcol < W);
-            const bool rows_in = (q0 >= R && q0 + kStepRows - 1 < H - R);
-            float cs = 0.0f;
-            // processed row q has relative index q - (x0 - R) = 8s + k
             const int p0 = (kStepRows * s) % PR;
+            for (int task = tid; task < (kStepRows / 2) * NP; task += kStripThreads) {
+                const int kq = task / NP, cp = task - kq * NP;
+                const int pc = 2 * cp, kr = 2 * kq;
+                const int q0 = x0 + kStepRows * s - R + kr;
+                const int gcol = ps + pc;
+                const float2* pg = (const float2*)(xg + (w0 + kr) * PWp + pc);
+                const float2* pb = (const float2*)(xb + (w0 + kr) * PWp + pc);
+                const bool cin0 = (gcol >= 0 && gcol < W), cin1 = (gcol + 1 >= 0 && gcol + 1 < W);
+                const bool rows_in = (q0 >= R && q0 + 1 < H - R);
+                // the Gaussian sums of both rows first, then the boxcar sums:
+                // one window of rows is live at a time
+                float2 gq[2];
+                {
+                    float2 vg[2 + 2 * R];
 #pragma unroll
-            for (int k = 0; k < kStepRows; k++) {
-                const int q = q0 + k;
-                float gs = 0.0f;
-                if (rows_in) {
+                    for (int i = 0; i < 2 + 2 * R; i++) vg[i] = pg[i * (PWp / 2)];
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
-                } else {
+                    for (int k = 0; k < 2; k++) {
+                        const int q = q0 + k;
+                        float2 gs = make_float2(0.0f, 0.0f);
+                        if (rows_in) {
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) {
-                        const int gr = q + i - R;
-                        if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
+                            for (int i = 0; i <= 2 * R; i++) gs = __ffma2_rn(tp2[i], vg[k + i], gs);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i <= 2 * R; i++) {
+                                const int gr = q + i - R;
+                                if (gr >= 0 && gr < H) {
+                                    gs.x = __fmaf_rn(c.taps[i], vg[k + i].x, gs.x);
+                                    gs.y = __fmaf_rn(c.taps[i], vg[k + i].y, gs.y);
+                                }
+                            }
+                        }
+                        gq[k] = div2_gnorm<FAST>(gs, dz, c);
                     }
                 }
-                if (kInt) {
-                    if (k == 0) cs = Tree<2 * R + 1>::sum(vbx);
-                    else cs = __fadd_rn(cs, __fsub_rn(vbx[k + 2 * R], vbx[k - 1]));
-                } else {
-                    cs = 0.0f;
+                float2 vbx[2 + 2 * R];
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[k + i]);
+                for (int i = 0; i < 2 + 2 * R; i++) vbx[i] = pb[i * (PWp / 2)];
+                float2 cs = make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int q = q0 + k;
+                    if (kInt) {
+                        if (k == 0) cs = Tree2<2 * R + 1>::sum(vbx);
+                        else cs = __fadd2_rn(cs, sub2(vbx[k + 2 * R], vbx[k - 1]));
+                    } else {
+                        cs = make_float2(0.0f, 0.0f);
+#pragma unroll
+                        for (int i = 0; i <= 2 * R; i++) cs = __fadd2_rn(cs, vbx[k + i]);
+                    }
+                    float2 r = sub2(gq[k], div2_kk<FAST>(cs, dz, c));
+                    if (c.truncate) {
+                        if (r.x < trunc_thr) r.x = 0.0f;
+                        if (r.y < trunc_thr) r.y = 0.0f;
+                    }
+                    const bool q_in = (q >= 0 && q < H);
+                    const float2 v = make_float2((cin0 && q_in) ? r.x : -INFINITY, (cin1 && q_in) ? r.y : -INFINITY);
+                    int pp = p0 + kr + k;
+                    if (pp >= PR) pp -= PR;
+                    *(float2*)(pr + pp * PWp + pc) = v;
+                    *(float2*)(pr + (pp + PR) * PWp + pc) = v;
                 }
-                float r = __fsub_rn(div_gnorm<FAST>(gs, c), div_kk<FAST>(cs, c));
-                if (c.truncate && r < trunc_thr) r = 0.0f;
-                const float v = (col_in && q >= 0 && q < H) ? r : -INFINITY;
-                int pp = p0 + k;
-                if (pp >= PR) pp -= PR;
-                pr[pp * PWp + pc] = v;
-                pr[(pp + PR) * PWp + pc] = v;
             }
         }
         __syncthreads();
