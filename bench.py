@@ -89,6 +89,16 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def load_issue():
+    """Thread-instructions per pixel of the dominant kernel from the committed
+    ncu summary (profiles/issue.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "issue.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
 def load_traffic():
     """Per-frame DRAM traffic of the dominant kernel from the committed ncu summary."""
     try:
@@ -722,6 +732,22 @@ def main():
                 "algorithmic_bytes_per_frame": bytes_per_frame,
                 "kernel_share": {k: round(v[1] / total_k, 4) for k, v in kernels.items()},
                 "whole_step_frac": frames_all * bytes_per_frame / (ms / 1000.0) / 1e9 / peak}
+    # the kernel is bound by instruction issue, not HBM: its thread-instructions
+    # per pixel (ncu) against the per-pixel operation floor, and the issue rate
+    # it reaches against the SMs' peak (148 SMs x 4 schedulers x 32 lanes per clock)
+    issue = load_issue().get(dom[0])
+    issue_roofline = None
+    if issue and dom[1][1] > 0:
+        sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+        avg_launch_s = dom[1][1] / 1000.0 / dom[1][0]
+        tipx = float(issue["thread_instr_per_px"])
+        achieved_i = tipx * S * S * frames_per_launch / avg_launch_s / 1e12
+        peak_i = 148 * 4 * 32 * sm_mhz * 1e6 / 1e12
+        issue_roofline = {"unit": "T thread-instr/s", "thread_instr_per_px": tipx,
+                          "floor_instr_per_px": issue.get("floor_instr_per_px"),
+                          "floor": issue.get("floor"), "achieved": achieved_i, "peak": peak_i,
+                          "frac": achieved_i / peak_i, "fp32_lane_ops_per_px": issue.get("fp32_lane_ops_per_px"),
+                          "us_per_frame": avg_launch_s / frames_per_launch * 1e6, "source": issue.get("source")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -739,8 +765,8 @@ def main():
                 "config": dict(CONFIG, frames=T, height=S, width=S,
                                parallelism="dp%d (one video per rank)" % world),
                 "features_per_s": feats_per_s, "features_per_frame": feats_per_frame,
-                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clk}
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "issue_roofline": issue_roofline,
+                "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
