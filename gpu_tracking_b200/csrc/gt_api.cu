@@ -1,4 +1,7 @@
-// gt_api.cu — the C ABI (include/gpu_tracking_b200.h) and its host runtime.
+// gt_api.cu — the C ABI (include/gpu_tracking_b200.h): context, the locate
+// runtime and the batch calls.  The linking calls are in gt_linkdrv.cu, the
+// result tables in gt_table.cu; the internals they share (context, buffers,
+// error handling, profiling) in gt_runtime.cuh.
 //
 // The runtime replaces execute_gpu / submit_work / get_work / post_process
 // (src/execute_gpu.rs:95-467, 671-1184) and setup_state (src/gpu_setup.rs:611-1292):
@@ -7,9 +10,7 @@
 //     copy of chunk c+1 overlaps the kernels of chunk c;
 //   * every per-frame result stays in HBM until the whole video is done
 //     (filter, doughnut and linking included), then one table is assembled
-//     on the device; gt_table_export copies any set of its columns out in one
-//     call (pinned staging lanes, widened to the DataFrame's dtypes on host
-//     threads), gt_table_column_* one column at a time;
+//     on the device;
 //   * capacities (candidates / detections per frame) grow and the call is
 //     replayed when a kernel reports an overflow, so nothing is truncated.
 #include <cuda.h>
@@ -32,250 +33,12 @@
 
 #include "gt_kernels.h"
 #include "gt_proposal.h"
+#include "gt_runtime.cuh"
 
 using namespace gt;
+using namespace gt::rt;
 
 namespace {
-
-struct DBuf {
-    void* p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf&) = delete;
-    DBuf& operator=(const DBuf&) = delete;
-    ~DBuf() {
-        if (p) cudaFree(p);
-    }
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= n && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        size_t want = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) n = want;
-        return e;
-    }
-    template <class T>
-    T* as() const {
-        return (T*)p;
-    }
-};
-
-// Result tables come and go with every call: their columns are stream-ordered
-// allocations from one pool per device that keeps its memory, so a call
-// neither maps fresh device memory nor synchronises the device to free it.
-cudaMemPool_t table_pool(int device) {
-    static std::mutex mu;
-    static std::map<int, cudaMemPool_t> pools;
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = pools.find(device);
-    if (it != pools.end()) return it->second;
-    cudaMemPoolProps props;
-    std::memset(&props, 0, sizeof(props));
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = device;
-    cudaMemPool_t pool = nullptr;
-    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    pools[device] = pool;
-    return pool;
-}
-
-struct TBuf {
-    void* p = nullptr;
-    size_t n = 0;
-    int device = 0;
-    cudaStream_t stream = nullptr;   // the call's compute stream
-    TBuf() = default;
-    TBuf(const TBuf&) = delete;
-    TBuf& operator=(const TBuf&) = delete;
-    // a table is freed only when no work on it is pending
-    ~TBuf() {
-        if (p) cudaFreeAsync(p, cudaStreamPerThread);
-    }
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= n && p) return cudaSuccess;
-        if (p) cudaFreeAsync(p, stream);
-        p = nullptr;
-        n = 0;
-        const size_t want = std::max<size_t>(bytes, 256);
-        cudaMemPool_t pool = table_pool(device);
-        if (!pool) return cudaErrorMemoryAllocation;
-        cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, stream);
-        if (e == cudaSuccess) n = want;
-        return e;
-    }
-    template <class T>
-    T* as() const {
-        return (T*)p;
-    }
-};
-
-struct KernelStat {
-    int64_t launches = 0;
-    double ms = 0.0;
-};
-
-}  // namespace
-
-struct gt_ctx {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t st = nullptr;   // compute
-    cudaStream_t cp = nullptr;   // host -> device copies
-    cudaStream_t lk = nullptr;   // linking of located frames, overlapped with locating
-    cudaEvent_t located = nullptr, linked = nullptr;
-    cudaEvent_t used[2] = {nullptr, nullptr};    // compute finished with staging buffer b
-    cudaEvent_t filled[2] = {nullptr, nullptr};  // staging buffer b holds its chunk
-    std::string err;
-    const volatile int32_t* interrupt = nullptr;
-    std::atomic<int64_t> done{0}, total{0};
-    // profiling of the main kernels (CUDA events on the compute stream)
-    bool profile = false;
-    std::map<std::string, KernelStat> stats;
-    std::map<std::string, int64_t> launch_count;
-    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
-    std::vector<cudaEvent_t> event_pool;
-    // device buffers, grown on demand and kept for the next call
-    DBuf stage[2], processed, planes, cand_count, cand_keys, feats_raw, feat_count, feats_out, kept_count,
-        fin_scratch, flags, ident, tabs_f, tabs_i, tabs_s, tabs_m, row_off, frame_num;
-    DBuf l_srt, l_sortscr, l_fcnt, l_bcnt, l_foff, l_boff, l_fpts, l_bpts, l_bdist, l_scan, l_scratch, l_ids, l_cnt,
-        l_dur, l_flags, l_goff, l_pgroup, l_vgrp, l_reset, l_vpoff, l_px, l_py, l_ge, l_rowdur, l_part;
-    // windowed linking inside gt_batch (slot mode)
-    DBuf fstd, std_scratch, amask, astatus, acount;   // snr / minmass_snr / adaptive_background
-    DBuf illum_taps, illum_shared, illum_prof, illum_corr;  // illumination correction
-    DBuf cnn_x, cnn_p, cnn_q, cnn_head;   // learned proposals: network input, activations, outputs
-    DBuf walk_starts;                     // walk starts of the current call (u64)
-    int64_t last_walk_starts = 0;
-    int32_t illum_rint = 0;
-    DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
-        w_cnt, w_flags, w_vgrp, w_reset;
-    int64_t w_list_cap = 0;   // entries of each window neighbour-list buffer (0 = not sized yet)
-    int64_t w_edge_cap = 0;   // backward edges per frame the window scratch holds
-    uint32_t cand_cap = 16384;
-    uint32_t feat_cap = 4096;
-};
-
-struct gt_table {
-    int device = 0;
-    int64_t n = 0;
-    TBuf frame, particle, duration;
-    TBuf col[GT_NUM_COLUMNS];
-    bool has[GT_NUM_COLUMNS] = {};
-    gt_table(int dev, cudaStream_t st) : device(dev) {
-        for (TBuf* b : {&frame, &particle, &duration}) {
-            b->device = dev;
-            b->stream = st;
-        }
-        for (auto& b : col) {
-            b.device = dev;
-            b.stream = st;
-        }
-    }
-};
-
-namespace {
-
-gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
-    va_end(ap);
-    if (ctx) ctx->err = buf;
-    return st;
-}
-
-#define CK(expr)                                                                                             \
-    do {                                                                                                     \
-        cudaError_t e_ = (expr);                                                                             \
-        if (e_ != cudaSuccess)                                                                               \
-            return set_err(ctx, GT_ERR_CUDA, "CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_), __FILE__, \
-                           __LINE__, #expr);                                                                 \
-    } while (0)
-
-#define CKS(expr)                        \
-    do {                                 \
-        gt_status s_ = (expr);           \
-        if (s_ != GT_OK) return s_;      \
-    } while (0)
-
-// --------------------------------------------------------------- profiling
-// Counts every kernel launch of the engine; with profiling enabled also
-// brackets it with CUDA events on the compute stream.
-struct Prof {
-    gt_ctx* ctx;
-    const char* name;
-    cudaStream_t stream;
-    cudaEvent_t a = nullptr, b = nullptr;
-    Prof(gt_ctx* c, const char* n, cudaStream_t s = nullptr) : ctx(c), name(n), stream(s ? s : c->st) {
-        ctx->launch_count[name]++;
-        if (!ctx->profile) return;
-        a = take();
-        b = take();
-        cudaEventRecord(a, stream);
-    }
-    cudaEvent_t take() {
-        if (!ctx->event_pool.empty()) {
-            cudaEvent_t e = ctx->event_pool.back();
-            ctx->event_pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        return e;
-    }
-    ~Prof() {
-        if (!ctx->profile) return;
-        cudaEventRecord(b, stream);
-        ctx->pending.push_back({name, {a, b}});
-    }
-};
-
-// Host wall-clock of one phase of a call, accumulated under `name` next to
-// the kernels' device times when profiling is on (gaps between kernels are
-// host work: allocation, uploads, read-backs).
-struct HostSpan {
-    gt_ctx* ctx;
-    const char* name;
-    std::chrono::steady_clock::time_point t0;
-    HostSpan(gt_ctx* c, const char* n) : ctx(c), name(n), t0(std::chrono::steady_clock::now()) {}
-    ~HostSpan() {
-        if (!ctx->profile) return;
-        auto& s = ctx->stats[name];
-        s.launches++;
-        s.ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
-};
-
-// Folds finished launches into the statistics; with block, waits for all.
-void drain_profile(gt_ctx* ctx, bool block = true) {
-    size_t keep = 0;
-    for (size_t i = 0; i < ctx->pending.size(); i++) {
-        auto& p = ctx->pending[i];
-        if (block) {
-            cudaEventSynchronize(p.second.second);
-        } else if (cudaEventQuery(p.second.second) != cudaSuccess) {
-            cudaGetLastError();
-            ctx->pending[keep++] = p;
-            continue;
-        }
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
-        auto& s = ctx->stats[p.first];
-        s.launches++;
-        s.ms += ms;
-        ctx->event_pool.push_back(p.second.first);
-        ctx->event_pool.push_back(p.second.second);
-    }
-    ctx->pending.resize(keep);
-}
 
 // ------------------------------------------------------- derived parameters
 struct Derived {
@@ -507,226 +270,7 @@ LogTables log_tables(const gt_params& p) {
     return t;
 }
 
-size_t dtype_bytes(int32_t dtype) { return dtype == GT_DTYPE_F32 ? 4 : (dtype == GT_DTYPE_U16 ? 2 : 1); }
-
-// cuMemGetAddressRange through the runtime's driver entry point (no link
-// against libcuda); null when the driver does not offer it.
-typedef CUresult (*AddressRangeFn)(CUdeviceptr*, size_t*, CUdeviceptr);
-AddressRangeFn address_range_fn() {
-    static AddressRangeFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* q = nullptr;
-        cudaDriverEntryPointQueryResult r;
-        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &q, cudaEnableDefault, &r) == cudaSuccess &&
-            r == cudaDriverEntryPointSuccess)
-            fn = (AddressRangeFn)q;
-        else
-            cudaGetLastError();
-    });
-    return fn;
-}
-
-// Host or device frames; device frames must live on the context's device and
-// the `bytes` the call reads must lie inside the allocation that holds them
-// (a wrong dtype or shape for a device tensor is an error, not a read past
-// the end of its memory).
-gt_status check_frames_ptr(gt_ctx* ctx, const void* frames, size_t bytes, bool* on_device) {
-    cudaPointerAttributes at;
-    cudaError_t e = cudaPointerGetAttributes(&at, frames);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        *on_device = false;
-        return GT_OK;
-    }
-    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
-        if (at.device != ctx->device)
-            return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "frames live on device %d, context is on device %d",
-                           at.device, ctx->device);
-        *on_device = true;
-        CUdeviceptr base = 0;
-        size_t size = 0;
-        AddressRangeFn fn = address_range_fn();
-        if (at.type == cudaMemoryTypeDevice && fn && fn(&base, &size, (CUdeviceptr)frames) == CUDA_SUCCESS) {
-            const uint64_t off = (uint64_t)(uintptr_t)frames - (uint64_t)base;
-            if (off > size || bytes > size - off)
-                return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
-                               "the device frames (%zu bytes from their pointer) run past the end of their "
-                               "allocation (%zu bytes left): check the dtype and shape",
-                               bytes, (size_t)(size - std::min<uint64_t>(off, size)));
-        }
-    } else {
-        *on_device = false;
-    }
-    return GT_OK;
-}
-
-bool interrupted(gt_ctx* ctx) { return ctx->interrupt && *ctx->interrupt != 0; }
-
-template <class T>
-gt_status upload(gt_ctx* ctx, DBuf& b, const std::vector<T>& v) {
-    CK(b.ensure(std::max<size_t>(1, v.size()) * sizeof(T)));
-    if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
-    return GT_OK;
-}
-
 // ---------------------------------------------------------------- linking
-struct LinkJob {
-    // host description of the groups (frames) and videos to link
-    std::vector<int64_t> goff;   // ngroups + 1, row offsets into px/py
-    std::vector<int32_t> vgrp;   // nvideos + 1
-    std::vector<uint8_t> reset;  // per group
-    float radius = 0;
-    int32_t memory = 0;
-};
-
-// Runs the linker over px/py (device, npoints) and writes ids (device) and,
-// when row_dur is given, per-row durations and f32-rounded particle ids.
-gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float* py, int64_t* ids_out,
-                   int64_t* row_dur, int64_t* row_particle, std::vector<int64_t>* counters) {
-    const int ngroups = (int)job.goff.size() - 1;
-    const int nvideos = (int)job.vgrp.size() - 1;
-    const int64_t N = job.goff.back();
-    const int K = job.memory + 1;
-    std::unique_ptr<HostSpan> hs(new HostSpan(ctx, "host_link_prep"));
-    int max_group = 0;
-    for (int g = 0; g < ngroups; g++) max_group = std::max<int64_t>(max_group, job.goff[g + 1] - job.goff[g]);
-    std::vector<int32_t> pgroup(N);
-    for (int g = 0; g < ngroups; g++)
-        for (int64_t i = job.goff[g]; i < job.goff[g + 1]; i++) pgroup[i] = g;
-    CKS(upload(ctx, ctx->l_goff, job.goff));
-    CKS(upload(ctx, ctx->l_pgroup, pgroup));
-    CKS(upload(ctx, ctx->l_vgrp, job.vgrp));
-    CKS(upload(ctx, ctx->l_reset, job.reset));
-    LinkInput in;
-    in.px = px;
-    in.py = py;
-    in.goff = ctx->l_goff.as<int64_t>();
-    in.pgroup = ctx->l_pgroup.as<int32_t>();
-    in.vgrp = ctx->l_vgrp.as<int32_t>();
-    in.reset = ctx->l_reset.as<uint8_t>();
-    in.ngroups = ngroups;
-    in.nvideos = nvideos;
-    in.npoints = N;
-    in.radius = job.radius;
-    in.memory = job.memory;
-
-    int np2 = 1;
-    while (np2 < max_group) np2 <<= 1;
-    size_t per_group = (np2 > 4096) ? (size_t)np2 * 8 : 0;
-    CK(ctx->l_srt.ensure(std::max<int64_t>(N, 1) * 4));
-    CK(ctx->l_sortscr.ensure(std::max<size_t>(per_group * ngroups, 8)));
-    {
-        Prof pf(ctx, "link_sort");
-        CK(link_sort_groups(in, ctx->l_srt.as<uint32_t>(), ctx->l_sortscr.as<uint8_t>(), per_group, max_group,
-                            ctx->st));
-    }
-    const size_t NK = (size_t)N * K;
-    CK(ctx->l_fcnt.ensure((NK + 1) * 8));
-    CK(ctx->l_bcnt.ensure((NK + 1) * 8));
-    CK(ctx->l_foff.ensure((NK + 1) * 8));
-    CK(ctx->l_boff.ensure((NK + 1) * 8));
-    CK(cudaMemsetAsync(ctx->l_fcnt.p, 0, (NK + 1) * 8, ctx->st));
-    CK(cudaMemsetAsync(ctx->l_bcnt.p, 0, (NK + 1) * 8, ctx->st));
-    {
-        Prof pf(ctx, "link_lists");
-        CK(link_count_lists(in, ctx->l_srt.as<uint32_t>(), ctx->l_fcnt.as<int64_t>(), ctx->l_bcnt.as<int64_t>(),
-                            ctx->st));
-    }
-    size_t tmp_bytes = 0;
-    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, ctx->l_fcnt.as<int64_t>(), ctx->l_foff.as<int64_t>(),
-                                     (int64_t)NK + 1, ctx->st));
-    CK(ctx->l_scan.ensure(tmp_bytes));
-    CK(cub::DeviceScan::ExclusiveSum(ctx->l_scan.p, tmp_bytes, ctx->l_fcnt.as<int64_t>(), ctx->l_foff.as<int64_t>(),
-                                     (int64_t)NK + 1, ctx->st));
-    CK(cub::DeviceScan::ExclusiveSum(ctx->l_scan.p, tmp_bytes, ctx->l_bcnt.as<int64_t>(), ctx->l_boff.as<int64_t>(),
-                                     (int64_t)NK + 1, ctx->st));
-    hs.reset(new HostSpan(ctx, "host_link_counts"));
-    int64_t ftot = 0, btot = 0;
-    CK(cudaMemcpyAsync(&ftot, ctx->l_foff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(&btot, ctx->l_boff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
-    // per-group backward-edge totals bound the per-frame edge list
-    std::vector<int64_t> gb(ngroups + 1);
-    std::vector<int64_t> boff_at(ngroups + 1);
-    for (int g = 0; g <= ngroups; g++)
-        CK(cudaMemcpyAsync(&boff_at[g], ctx->l_boff.as<int64_t>() + job.goff[g] * K, 8, cudaMemcpyDeviceToHost,
-                           ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    hs.reset(new HostSpan(ctx, "host_link_run"));
-    int64_t max_edges = 1;
-    for (int g = 0; g < ngroups; g++) max_edges = std::max(max_edges, boff_at[g + 1] - boff_at[g]);
-    CK(ctx->l_fpts.ensure(std::max<int64_t>(ftot, 1) * 4));
-    CK(ctx->l_bpts.ensure(std::max<int64_t>(btot, 1) * 4));
-    CK(ctx->l_bdist.ensure(std::max<int64_t>(btot, 1) * 4));
-    LinkLists L;
-    L.f_off = ctx->l_foff.as<int64_t>();
-    L.b_off = ctx->l_boff.as<int64_t>();
-    L.f_pts = ctx->l_fpts.as<int32_t>();
-    L.b_pts = ctx->l_bpts.as<int32_t>();
-    L.b_dist = ctx->l_bdist.as<float>();
-    L.srt = ctx->l_srt.as<uint32_t>();
-    L.f_entries = ftot;
-    {
-        Prof pf(ctx, "link_lists");
-        CK(link_fill_lists(in, L, ctx->st));
-    }
-    // scratch per video
-    int64_t max_np = 1;
-    for (int v = 0; v < nvideos; v++) max_np = std::max(max_np, job.goff[job.vgrp[v + 1]] - job.goff[job.vgrp[v]]);
-    LinkScratch S;
-    S.max_group = std::max(max_group, 1);
-    S.max_edges = max_edges;
-    S.bytes_per_video = link_scratch_bytes(S.max_group, S.max_edges, max_np, job.memory);
-    S.max_points = max_np;
-    CK(ctx->l_scratch.ensure(S.bytes_per_video * nvideos));
-    S.base = ctx->l_scratch.as<uint8_t>();
-    LinkOutput out;
-    CK(ctx->l_cnt.ensure(nvideos * 8));
-    CK(ctx->l_dur.ensure(std::max<int64_t>(N, 1) * 8));
-    CK(ctx->l_flags.ensure(nvideos * 4));
-    CK(cudaMemsetAsync(ctx->l_flags.p, 0, nvideos * 4, ctx->st));
-    out.ids = ids_out;
-    out.counter = ctx->l_cnt.as<int64_t>();
-    out.dur = ctx->l_dur.as<int64_t>();
-    out.vpoff = nullptr;
-    out.flags = ctx->l_flags.as<uint32_t>();
-    {
-        Prof pf(ctx, "link_video");
-        CK(link_run(in, L, S, out, ctx->st));
-    }
-    std::vector<uint32_t> flags(nvideos);
-    CK(cudaMemcpyAsync(flags.data(), out.flags, nvideos * 4, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    uint32_t all = 0;
-    for (auto f : flags) all |= f;
-    if (all & kFlagTooDense)
-        return set_err(ctx, GT_ERR_TOO_DENSE_TO_LINK,
-                       "computational load during linking is abnormally high. try setting a smaller search range "
-                       "or track with settings that give fewer detections.");
-    if (all & kFlagSubnetBudget)
-        return set_err(ctx, GT_ERR_SUBNET_TOO_EXPENSIVE, "a linking subnet exceeded the device search budget");
-    if (all & kFlagScratch) return set_err(ctx, GT_ERR_INTERNAL, "linker scratch overflow");
-    if (counters) {
-        counters->resize(nvideos);
-        CK(cudaMemcpy(counters->data(), out.counter, nvideos * 8, cudaMemcpyDeviceToHost));
-    }
-    hs.reset(new HostSpan(ctx, "host_link_durations"));
-    if (row_dur) {
-        {
-            Prof pf(ctx, "link_durations");
-            CK(link_durations(in, out, row_dur, ctx->st));
-        }
-        CK(cudaMemcpyAsync(flags.data(), out.flags, nvideos * 4, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
-        for (auto f : flags)
-            if (f & kFlagScratch)
-                return set_err(ctx, GT_ERR_INTERNAL,
-                               "a particle id has no duration entry after a linker reset (the reference panics here)");
-    }
-    (void)row_particle;
-    return GT_OK;
-}
-
 // acc += sum of min(count[i], cap) over the chunk's frames (walk starts)
 __global__ void sum_counts_kernel(const uint32_t* __restrict__ count, int n, uint32_t cap,
                                   unsigned long long* __restrict__ acc) {
@@ -734,11 +278,6 @@ __global__ void sum_counts_kernel(const uint32_t* __restrict__ count, int n, uin
     for (int i = threadIdx.x; i < n; i += blockDim.x) s += min(count[i], cap);
     for (int d = 16; d; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
-}
-
-__global__ void f32_round_ids_kernel(const int64_t* ids, int64_t* out, int64_t n) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (int64_t)(float)ids[i];
 }
 
 // Windowed linking inside gt_batch.  Every super-chunk of located frames is
@@ -1503,8 +1042,7 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
                          ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
             if (tab->n > 0) {
                 Prof pf(ctx, "round_ids");
-                f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
-                    ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+                CK(launch_round_ids(ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n, ctx->st));
             }
             CK(cudaGetLastError());
         }
@@ -1545,35 +1083,6 @@ gt_status validate(gt_ctx* ctx, const gt_params* p, const void* frames, int32_t 
 // (src/linking.rs:97-196): a group is emitted whenever the frame number
 // increases (so a positive first frame yields a leading empty group 0); a
 // decreasing frame number is NonSortedCharacterization.
-gt_status subset_groups(gt_ctx* ctx, const float* rows, int64_t n, int ncols, std::vector<int64_t>& goff,
-                        std::vector<int64_t>& gframe) {
-    goff.assign(1, 0);
-    gframe.clear();
-    float cur = 0.0f;
-    int64_t idx = 0;
-    while (true) {
-        if (idx < n) {
-            float f = rows[idx * ncols];
-            if (f > cur) {
-                goff.push_back(idx);
-                gframe.push_back((int64_t)cur);
-                cur = f;
-                continue;
-            }
-            if (f < cur)
-                return set_err(ctx, GT_ERR_NON_SORTED_CHARACTERIZATION,
-                               "the points provided for characterization aren't sorted in ascending frame number.");
-            idx++;
-        } else {
-            if (idx > goff.back()) {
-                goff.push_back(idx);
-                gframe.push_back((int64_t)cur);
-            }
-            break;
-        }
-    }
-    return GT_OK;
-}
 
 template <typename T>
 gt_status mean_impl(gt_ctx* ctx, const T* frames, bool on_device, int64_t NT, int32_t H, int32_t W, float* out) {
@@ -1733,8 +1242,7 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
                      ctx->l_ids.as<int64_t>(), tab->duration.as<int64_t>(), nullptr, nullptr));
         if (tab->n > 0) {
             Prof pf(ctx, "round_ids");
-            f32_round_ids_kernel<<<(unsigned)((tab->n + 255) / 256), 256, 0, ctx->st>>>(
-                ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n);
+            CK(launch_round_ids(ctx->l_ids.as<int64_t>(), tab->particle.as<int64_t>(), tab->n, ctx->st));
         }
         CK(cudaGetLastError());
         tab->has[GT_COL_PARTICLE] = true;
@@ -1812,8 +1320,7 @@ gt_status batch_videos_impl(gt_ctx* ctx, const gt_params& p, int32_t n_videos, c
         CK(tab->particle.ensure(m * 8));
         CK(tab->duration.ensure(m * 8));
         if (n > 0) {
-            f32_round_ids_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->st>>>(ctx->l_ids.as<int64_t>() + base,
-                                                                                 tab->particle.as<int64_t>(), n);
+            CK(launch_round_ids(ctx->l_ids.as<int64_t>() + base, tab->particle.as<int64_t>(), n, ctx->st));
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(tab->duration.p, ctx->l_rowdur.as<int64_t>() + base, (size_t)n * 8,
                                cudaMemcpyDeviceToDevice, ctx->st));
@@ -2004,204 +1511,6 @@ gt_status gt_progress(const gt_ctx* ctx, int64_t* done, int64_t* total) {
     return GT_OK;
 }
 
-int64_t gt_table_nrows(const gt_table* t) { return t ? t->n : 0; }
-
-int32_t gt_table_has_column(const gt_table* t, int32_t column) {
-    if (!t || column < 0 || column >= GT_NUM_COLUMNS) return 0;
-    return t->has[column] ? 1 : 0;
-}
-
-gt_status gt_table_column_f32(const gt_table* t, int32_t column, float* dst) {
-    if (!t || !dst || column < 0 || column >= GT_NUM_COLUMNS) return GT_ERR_INVALID_ARGUMENT;
-    if (!t->has[column]) return GT_ERR_INVALID_ARGUMENT;
-    if (t->n == 0) return GT_OK;
-    cudaSetDevice(t->device);
-    if (column == GT_COL_FRAME || column == GT_COL_PARTICLE || column == GT_COL_DURATION) {
-        std::vector<int64_t> v(t->n);
-        const TBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
-        if (cudaMemcpy(v.data(), b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
-        for (int64_t i = 0; i < t->n; i++) dst[i] = (float)v[i];
-        return GT_OK;
-    }
-    if (cudaMemcpy(dst, t->col[column].p, t->n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
-    return GT_OK;
-}
-
-gt_status gt_table_column_i64(const gt_table* t, int32_t column, int64_t* dst) {
-    if (!t || !dst) return GT_ERR_INVALID_ARGUMENT;
-    if (column != GT_COL_FRAME && column != GT_COL_PARTICLE && column != GT_COL_DURATION)
-        return GT_ERR_INVALID_ARGUMENT;
-    if (!t->has[column]) return GT_ERR_INVALID_ARGUMENT;
-    if (t->n == 0) return GT_OK;
-    cudaSetDevice(t->device);
-    const TBuf& b = column == GT_COL_FRAME ? t->frame : (column == GT_COL_PARTICLE ? t->particle : t->duration);
-    if (cudaMemcpy(dst, b.p, t->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return GT_ERR_CUDA;
-    return GT_OK;
-}
-
-namespace {
-
-// Table export: each lane (one host thread) owns two pinned slots and a
-// stream; it copies its share of the rows chunk by chunk into one slot while
-// it widens the previous chunk from the other into the destination.
-constexpr int kExportLanes = 8;
-constexpr size_t kExportSlot = (size_t)1 << 20;
-constexpr int kExportMaxDevices = 64;
-
-struct ExportLane {
-    char* slot[2] = {nullptr, nullptr};
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-};
-
-struct ExportPool {
-    std::mutex mu;
-    bool ready = false;
-    ExportLane lane[kExportLanes];
-};
-
-// One pool per device for the life of the process (never destroyed: no CUDA
-// call runs from a static destructor after the runtime has shut down).
-ExportPool* export_pool(int device) {
-    static ExportPool* pools = new ExportPool[kExportMaxDevices];
-    return device >= 0 && device < kExportMaxDevices ? &pools[device] : nullptr;
-}
-
-// All or nothing: on a failure everything created so far is released and the
-// next call tries again.
-cudaError_t export_pool_init(ExportPool& p) {
-    if (p.ready) return cudaSuccess;
-    char* block = nullptr;
-    cudaError_t e = cudaHostAlloc((void**)&block, 2 * kExportLanes * kExportSlot, cudaHostAllocDefault);
-    if (e != cudaSuccess) return e;
-    for (int l = 0; l < kExportLanes && e == cudaSuccess; l++) {
-        ExportLane& L = p.lane[l];
-        L.slot[0] = block + (2 * l) * kExportSlot;
-        L.slot[1] = block + (2 * l + 1) * kExportSlot;
-        e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
-        for (int s = 0; s < 2 && e == cudaSuccess; s++) e = cudaEventCreateWithFlags(&L.ev[s], cudaEventDisableTiming);
-    }
-    if (e != cudaSuccess) {
-        for (ExportLane& L : p.lane) {
-            for (cudaEvent_t& ev : L.ev)
-                if (ev) cudaEventDestroy(ev), ev = nullptr;
-            if (L.st) cudaStreamDestroy(L.st), L.st = nullptr;
-            L.slot[0] = L.slot[1] = nullptr;
-        }
-        cudaFreeHost(block);
-        return e;
-    }
-    p.ready = true;
-    return cudaSuccess;
-}
-
-struct ExportItem {
-    const char* src;   // device rows
-    char* dst;         // host rows
-    int64_t rows;
-    bool widen;        // float32 -> double; otherwise int64 copied as is
-};
-
-cudaError_t export_lane(int device, ExportLane& L, const std::vector<ExportItem>& items) {
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) return e;
-    auto issue = [&](size_t i) {
-        const ExportItem& it = items[i];
-        const size_t bytes = (size_t)it.rows * (it.widen ? 4 : 8);
-        cudaError_t r = cudaMemcpyAsync(L.slot[i & 1], it.src, bytes, cudaMemcpyDeviceToHost, L.st);
-        return r != cudaSuccess ? r : cudaEventRecord(L.ev[i & 1], L.st);
-    };
-    if (items.empty()) return cudaSuccess;
-    if ((e = issue(0)) != cudaSuccess) return e;
-    for (size_t i = 0; i < items.size(); i++) {
-        // slot (i + 1) & 1 held item i - 1, already widened by this thread
-        if (i + 1 < items.size() && (e = issue(i + 1)) != cudaSuccess) break;
-        if ((e = cudaEventSynchronize(L.ev[i & 1])) != cudaSuccess) break;
-        const ExportItem& it = items[i];
-        if (it.widen) {
-            const float* s = (const float*)L.slot[i & 1];
-            double* d = (double*)it.dst;
-            for (int64_t j = 0; j < it.rows; j++) d[j] = (double)s[j];
-        } else {
-            memcpy(it.dst, L.slot[i & 1], (size_t)it.rows * 8);
-        }
-    }
-    // nothing may still land in the slots once the pool is handed on
-    cudaError_t e2 = cudaStreamSynchronize(L.st);
-    return e != cudaSuccess ? e : e2;
-}
-
-}  // namespace
-
-namespace {
-
-gt_status table_export_impl(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
-    if (!t || ncolumns < 0 || (ncolumns > 0 && (!columns || !dst))) return GT_ERR_INVALID_ARGUMENT;
-    for (int32_t k = 0; k < ncolumns; k++) {
-        const int32_t c = columns[k];
-        if (c < 0 || c >= GT_NUM_COLUMNS || !t->has[c] || !dst[k]) return GT_ERR_INVALID_ARGUMENT;
-    }
-    const int64_t N = t->n;
-    if (N == 0 || ncolumns == 0) return GT_OK;
-    ExportPool* pool = export_pool(t->device);
-    if (!pool) return GT_ERR_INVALID_ARGUMENT;
-    std::lock_guard<std::mutex> lock(pool->mu);
-    if (cudaSetDevice(t->device) != cudaSuccess || export_pool_init(*pool) != cudaSuccess) return GT_ERR_CUDA;
-    // lanes: one per 256k rows, at most kExportLanes and half the host threads
-    const int hw = std::max(1, (int)std::thread::hardware_concurrency() / 2);
-    const int lanes = (int)std::max<int64_t>(1, std::min<int64_t>({kExportLanes, hw, (N + (1 << 18) - 1) >> 18}));
-    std::vector<std::vector<ExportItem>> work(lanes);
-    for (int l = 0; l < lanes; l++) {
-        const int64_t r0 = N * l / lanes, r1 = N * (l + 1) / lanes;
-        for (int32_t k = 0; k < ncolumns; k++) {
-            const int32_t c = columns[k];
-            const bool integer = c == GT_COL_FRAME || c == GT_COL_PARTICLE || c == GT_COL_DURATION;
-            const TBuf& b = c == GT_COL_FRAME ? t->frame
-                                              : (c == GT_COL_PARTICLE ? t->particle
-                                                                      : (c == GT_COL_DURATION ? t->duration : t->col[c]));
-            const int64_t chunk = (int64_t)(kExportSlot / (integer ? 8 : 4));
-            for (int64_t r = r0; r < r1; r += chunk) {
-                ExportItem it;
-                it.rows = std::min(chunk, r1 - r);
-                it.src = (const char*)b.p + (size_t)r * (integer ? 8 : 4);
-                it.dst = (char*)dst[k] + (size_t)r * 8;
-                it.widen = !integer;
-                work[l].push_back(it);
-            }
-        }
-    }
-    std::vector<cudaError_t> err(lanes, cudaSuccess);
-    std::vector<std::thread> th;
-    // lanes whose thread cannot be started run on the calling thread
-    for (int l = 1; l < lanes; l++) {
-        try {
-            th.emplace_back([&, l] { err[l] = export_lane(t->device, pool->lane[l], work[l]); });
-        } catch (...) {
-            err[l] = export_lane(t->device, pool->lane[l], work[l]);
-        }
-    }
-    err[0] = export_lane(t->device, pool->lane[0], work[0]);
-    for (auto& x : th) x.join();
-    for (cudaError_t e : err)
-        if (e != cudaSuccess) return GT_ERR_CUDA;
-    return GT_OK;
-}
-
-}  // namespace
-
-gt_status gt_table_export(const gt_table* t, const int32_t* columns, int32_t ncolumns, void* const* dst) {
-    try {
-        return table_export_impl(t, columns, ncolumns, dst);
-    } catch (...) {
-        return GT_ERR_INTERNAL;   // no C++ exception crosses the C ABI
-    }
-}
-
-void gt_table_free(gt_table* t) {
-    if (!t) return;
-    cudaSetDevice(t->device);
-    delete t;
-}
 
 gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int32_t dtype, int64_t T, int32_t H,
                    int32_t W, const int64_t* frame_numbers, const int64_t* linker_reset_points, int64_t n_reset,
@@ -2326,155 +1635,6 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const voi
         return st;
     }
     *out = tab.release();
-    return GT_OK;
-}
-
-gt_status gt_link(gt_ctx* ctx, const float* frame_y_x, int64_t n, float search_range, uint32_t memory,
-                  int64_t* particle_out) {
-    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
-    if (n == 0) return GT_OK;
-    if (!frame_y_x || !particle_out) return set_err(ctx, GT_ERR_INVALID_ARGUMENT, "null argument");
-    CK(cudaSetDevice(ctx->device));
-    LinkJob job;
-    std::vector<int64_t> gframe;
-    CKS(subset_groups(ctx, frame_y_x, n, 3, job.goff, gframe));
-    const int64_t N = job.goff.back();
-    job.vgrp = {0, (int32_t)gframe.size()};
-    job.reset.assign(gframe.size(), 0);
-    job.radius = search_range;
-    job.memory = (int32_t)memory;
-    std::vector<float> px(N), py(N);
-    for (int64_t i = 0; i < N; i++) {
-        px[i] = frame_y_x[3 * i + 1];
-        py[i] = frame_y_x[3 * i + 2];
-    }
-    CKS(upload(ctx, ctx->l_px, px));
-    CKS(upload(ctx, ctx->l_py, py));
-    CK(ctx->l_ids.ensure(std::max<int64_t>(N, 1) * 8));
-    CKS(run_link(ctx, job, ctx->l_px.as<float>(), ctx->l_py.as<float>(), ctx->l_ids.as<int64_t>(), nullptr, nullptr,
-                 nullptr));
-    CK(cudaMemcpyAsync(particle_out, ctx->l_ids.p, N * 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    return GT_OK;
-}
-
-// connect_all (src/linking.rs:960-1020): the frame bookkeeping runs on the
-// host exactly as the reference's iterators do; every connected frame pair is
-// an independent two-frame linking job, all of them solved in one launch.
-gt_status gt_connect(gt_ctx* ctx, const float* a1, int64_t n1, const float* a2, int64_t n2, float search_range,
-                     int64_t* out1, int64_t* out2) {
-    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
-    CK(cudaSetDevice(ctx->device));
-    std::vector<int64_t> g1, f1, g2, f2;
-    CKS(subset_groups(ctx, a1, n1, 3, g1, f1));
-    CKS(subset_groups(ctx, a2, n2, 3, g2, f2));
-    // operations in the reference's order
-    struct Op {
-        int kind;  // 0 fill side 1, 1 fill side 2, 2 connect
-        int64_t i1, i2;
-    };
-    std::vector<Op> ops;
-    size_t p1 = 0, p2 = 0;
-    auto next1 = [&](int64_t* g) { if (p1 < f1.size()) { *g = (int64_t)p1++; return true; } return false; };
-    auto next2 = [&](int64_t* g) { if (p2 < f2.size()) { *g = (int64_t)p2++; return true; } return false; };
-    while (true) {
-        int64_t a, b;
-        bool h1 = next1(&a), h2 = next2(&b);
-        if (h1 && h2) {
-            if (f1[a] == f2[b]) {
-                ops.push_back({2, a, b});
-                continue;
-            }
-            // sync_iterators (src/linking.rs:914-958)
-            bool left = f1[a] > f2[b];
-            int64_t hit = left ? a : b;
-            if (left) ops.push_back({1, -1, b}); else ops.push_back({0, a, -1});
-            while (true) {
-                int64_t nx;
-                bool got = left ? next2(&nx) : next1(&nx);
-                if (!got) {
-                    if (left) ops.push_back({0, hit, -1}); else ops.push_back({1, -1, hit});
-                    break;
-                }
-                int64_t fh = left ? f1[hit] : f2[hit];
-                int64_t fn = left ? f2[nx] : f1[nx];
-                if (fh > fn) {
-                    if (left) ops.push_back({1, -1, nx}); else ops.push_back({0, nx, -1});
-                } else if (fh == fn) {
-                    if (left) ops.push_back({2, hit, nx}); else ops.push_back({2, nx, hit});
-                    break;
-                } else {
-                    if (left) ops.push_back({1, -1, nx}); else ops.push_back({0, nx, -1});
-                    if (left) ops.push_back({0, hit, -1}); else ops.push_back({1, -1, hit});
-                    hit = nx;
-                    left = !left;
-                }
-            }
-        } else if (h1) {
-            ops.push_back({0, a, -1});
-        } else if (h2) {
-            ops.push_back({1, -1, b});
-        } else {
-            break;
-        }
-    }
-    // linking jobs for the connect operations
-    LinkJob job;
-    job.goff.assign(1, 0);
-    job.vgrp.assign(1, 0);
-    job.radius = search_range;
-    job.memory = 0;
-    std::vector<float> px, py;
-    std::vector<int64_t> op_video(ops.size(), -1);
-    for (size_t k = 0; k < ops.size(); k++) {
-        if (ops[k].kind != 2) continue;
-        op_video[k] = (int64_t)job.vgrp.size() - 1;
-        for (int side = 0; side < 2; side++) {
-            const float* arr = side ? a2 : a1;
-            const std::vector<int64_t>& go = side ? g2 : g1;
-            int64_t gi = side ? ops[k].i2 : ops[k].i1;
-            for (int64_t i = go[gi]; i < go[gi + 1]; i++) {
-                px.push_back(arr[3 * i + 1]);
-                py.push_back(arr[3 * i + 2]);
-            }
-            job.goff.push_back((int64_t)px.size());
-            job.reset.push_back(0);
-        }
-        job.vgrp.push_back((int32_t)job.goff.size() - 1);
-    }
-    std::vector<int64_t> local((size_t)px.size());
-    std::vector<int64_t> counters;
-    if (!px.empty()) {
-        CKS(upload(ctx, ctx->l_px, px));
-        CKS(upload(ctx, ctx->l_py, py));
-        CK(ctx->l_ids.ensure(px.size() * 8));
-        CKS(run_link(ctx, job, ctx->l_px.as<float>(), ctx->l_py.as<float>(), ctx->l_ids.as<int64_t>(), nullptr,
-                     nullptr, &counters));
-        CK(cudaMemcpy(local.data(), ctx->l_ids.p, px.size() * 8, cudaMemcpyDeviceToHost));
-    }
-    std::vector<int64_t> r1, r2;
-    int64_t part = 0;
-    for (size_t k = 0; k < ops.size(); k++) {
-        const Op& o = ops[k];
-        if (o.kind == 0) {
-            for (int64_t i = g1[o.i1]; i < g1[o.i1 + 1]; i++) r1.push_back(part++);
-        } else if (o.kind == 1) {
-            for (int64_t i = g2[o.i2]; i < g2[o.i2 + 1]; i++) r2.push_back(part++);
-        } else {
-            int64_t v = op_video[k];
-            int64_t b0 = job.goff[job.vgrp[v]], b1 = job.goff[job.vgrp[v] + 1], b2 = job.goff[job.vgrp[v] + 2];
-            for (int64_t i = b0; i < b1; i++) r1.push_back(part + local[i]);
-            for (int64_t i = b1; i < b2; i++) r2.push_back(part + local[i]);
-            part += counters[v];
-        }
-    }
-    if ((int64_t)r1.size() != n1 || (int64_t)r2.size() != n2)
-        return set_err(ctx, GT_ERR_INVALID_ARGUMENT,
-                       "connect produced %lld/%lld ids for %lld/%lld rows (frame interleaving the reference "
-                       "double-counts)",
-                       (long long)r1.size(), (long long)r2.size(), (long long)n1, (long long)n2);
-    if (n1) std::memcpy(out1, r1.data(), n1 * 8);
-    if (n2) std::memcpy(out2, r2.data(), n2 * 8);
     return GT_OK;
 }
 
