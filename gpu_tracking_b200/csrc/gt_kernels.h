@@ -25,6 +25,21 @@ struct FinalizeConsts {
     uint8_t radius_rank_desc[kMaxRadii];
 };
 
+// One frame of a ragged batch (frames of many videos and sizes in one launch
+// per stage): its pixels, where its processed image starts in the batch's
+// buffer, its size, and whether 4-pixel loads of its rows are aligned.
+struct RaggedFrame {
+    const void* raw;
+    int64_t proc_off;
+    int32_t H, W;
+    int32_t vec_ok;
+    int32_t pad;
+};
+// One bandpass tile of a ragged batch: frame slot, first output column, rows [r0, r1).
+struct StripTask {
+    int32_t slot, c0, r0, r1;
+};
+
 struct TableCols {
     int64_t* frame;
     float* col[GT_NUM_COLUMNS];
@@ -128,6 +143,16 @@ cudaError_t launch_bandpass(const T* frames, int64_t frame_stride, float* proces
 
 // Streaming strip kernel for the specialised (radius, dilation) pairs; returns
 // false when the pair has no specialisation (the tile kernel is used then).
+// The strip kernel over a ragged batch: persistent CTAs (grid of them) take
+// the tiles of `tasks` (*ntasks of them, in device memory) in turn; candidate
+// lists per frame slot.  False when no specialisation exists (as launch_strip).
+template <typename T>
+bool launch_strip_ragged(const RaggedFrame* frames, const StripTask* tasks, const int32_t* ntasks, int grid,
+                         float* processed, const LocateConsts& c, uint32_t* cand_count, uint32_t* cand_keys,
+                         uint32_t cand_cap, uint32_t* flags, cudaStream_t st, cudaError_t* err);
+// CTAs of the strip kernel resident per SM for these parameters (0: no specialisation)
+template <typename T>
+int strip_blocks_per_sm(const LocateConsts& c);
 template <typename T>
 bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                   uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,
@@ -142,7 +167,7 @@ cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_s
                         int nframes, int n_slots, const uint32_t* cand_count, const uint32_t* cand_keys,
                         uint32_t cand_cap, uint32_t max_cands, const float* radii, const int32_t* angle_off,
                         const float2* angles, Feature* feats, uint32_t* feat_count, uint32_t feat_cap,
-                        uint32_t* flags, cudaStream_t st);
+                        uint32_t* flags, cudaStream_t st, const RaggedFrame* rf = nullptr);
 
 template <typename T>
 cudaError_t launch_characterize_points(const float* processed, const T* frames, int64_t frame_stride,
@@ -152,11 +177,14 @@ cudaError_t launch_characterize_points(const float* processed, const T* frames, 
                                        int32_t has_r, Feature* feats, uint32_t* feat_count, uint32_t feat_cap,
                                        cudaStream_t st);
 
+// rf (optional): per-slot frames of a ragged batch (pixels and size replace
+// frames / frame_index / fc.H, fc.W)
 template <typename T>
 cudaError_t launch_finalize(const Feature* feats, const uint32_t* feat_count, uint32_t feat_cap, Feature* out,
                             uint32_t* kept_count, uint8_t* gscratch, const FinalizeConsts& fc, const T* frames,
                             int64_t frame_stride, const int32_t* frame_index, const short2* dn_inds,
-                            const int4* dn_meta, uint32_t* flags, int ngroups, cudaStream_t st);
+                            const int4* dn_meta, uint32_t* flags, int ngroups, cudaStream_t st,
+                            const RaggedFrame* rf = nullptr);
 
 cudaError_t launch_scatter(const Feature* feats, uint32_t feat_cap, const uint32_t* kept_count, uint32_t max_kept,
                            const int64_t* row_off, const int64_t* frame_number, const TableCols& tab, int32_t g0,

@@ -386,10 +386,10 @@ __device__ __forceinline__ WalkRes get_center_fixed(const float* __restrict__ p,
 }
 
 template <int RI>
-__device__ __forceinline__ WalkRes walk_fixed(const float* __restrict__ p, const LocateConsts& c, int u0, int v0) {
+__device__ __forceinline__ WalkRes walk_fixed(const float* __restrict__ p, const LocateConsts& c, const int H,
+                                              const int W, int u0, int v0) {
     int pu = u0, pv = v0;
     WalkRes res = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    const int H = c.H, W = c.W;
     const float thr = c.shift_thr;
     for (uint32_t it = 0; it < c.max_iter; it++) {
         if (pu >= RI && pu + RI < H && pv >= RI && pv + RI < W)
@@ -450,16 +450,17 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
                   const LocateConsts c, const uint32_t* __restrict__ cand_count,
                   const uint32_t* __restrict__ cand_keys, uint32_t cand_cap, const int32_t* __restrict__ angle_off,
                   const float2* __restrict__ angles, Feature* __restrict__ feats, uint32_t* __restrict__ feat_count,
-                  uint32_t feat_cap, uint32_t* __restrict__ flags) {
+                  uint32_t feat_cap, uint32_t* __restrict__ flags, const RaggedFrame* __restrict__ rf) {
     const int f = blockIdx.y;
     const uint32_t n = min(cand_count[f], cand_cap);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    // a ragged batch gives every frame slot its own size, pixels and processed image
+    const int H = rf ? rf[f].H : c.H, W = rf ? rf[f].W : c.W;
     const uint32_t key = cand_keys[(size_t)f * cand_cap + i];
-    const int u = (int)(key / (uint32_t)c.W), v = (int)(key % (uint32_t)c.W);
-    const int H = c.H, W = c.W;
-    const float* p = processed + (size_t)f * H * W;
-    const WalkRes res = walk_fixed<RI>(p, c, u, v);
+    const int u = (int)(key / (uint32_t)W), v = (int)(key % (uint32_t)W);
+    const float* p = rf ? processed + rf[f].proc_off : processed + (size_t)f * H * W;
+    const WalkRes res = walk_fixed<RI>(p, c, H, W, u, v);
     float minmass;
     if (c.minmass > 0.0f) minmass = c.minmass;
     else minmass = __fmul_rn(__fmul_rn(__fmul_rn(c.minmass_snr, res.count), c.frame_std ? c.frame_std[f] : c.image_std),
@@ -479,7 +480,7 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
     ft.ridx = 0;
     if (c.characterize) {
         // characterize.wgsl:61-143 at the rounded position, radius RI
-        const T* raw = frames + (size_t)f * frame_stride;
+        const T* raw = rf ? (const T*)rf[f].raw : frames + (size_t)f * frame_stride;
         const int cu = sat_f2i(rintf(ft.x)), cv = sat_f2i(rintf(ft.y));
         const float2* ang = angles + angle_off[RI];
         float middle = 0.0f;
@@ -1139,10 +1140,11 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
                 Feature* __restrict__ out, uint32_t* __restrict__ kept_count, uint8_t* __restrict__ gscratch,
                 const FinalizeConsts fc, const T* __restrict__ frames, int64_t frame_stride,
                 const int32_t* __restrict__ frame_index, const short2* __restrict__ dn_inds,
-                const int4* __restrict__ dn_meta, uint32_t* __restrict__ flags) {
+                const int4* __restrict__ dn_meta, uint32_t* __restrict__ flags, const RaggedFrame* __restrict__ rf) {
     extern __shared__ uint64_t fsm[];
     __shared__ int wsum[33];
     const int g = blockIdx.x;
+    const int fW = rf ? rf[g].W : fc.W;
     const int n = (int)min(feat_count[g], feat_cap);
     const Feature* F = feats + (size_t)g * feat_cap;
     int np2 = 1;
@@ -1200,10 +1202,10 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
                 int lo = 0, hi = n;
                 if (fc.band >= 0) {
                     // rows of candidates that can hold a neighbour (|x - u| <= reach)
-                    int64_t u = (int64_t)q.key_lo / fc.W;
+                    int64_t u = (int64_t)q.key_lo / fW;
                     int64_t ulo = u - fc.band, uhi = u + fc.band + 1;
-                    uint64_t klo = ulo <= 0 ? 0ull : ((uint64_t)(ulo * fc.W) << 24);
-                    uint64_t khi = ((uint64_t)(uhi * fc.W) << 24);
+                    uint64_t klo = ulo <= 0 ? 0ull : ((uint64_t)(ulo * fW) << 24);
+                    uint64_t khi = ((uint64_t)(uhi * fW) << 24);
                     int a = 0, b = n;
                     while (a < b) { int m = (a + b) >> 1; if (keys[m] < klo) a = m + 1; else b = m; }
                     lo = a;
@@ -1259,7 +1261,6 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
 
     // 3. doughnut correction of the kept rows, one warp per row
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const T* raw = frames + (size_t)frame_index[g] * frame_stride;
     // 4. compaction in output order
     int total = 0;
     for (int base = 0; base < n; base += blockDim.x) {
@@ -1287,18 +1288,19 @@ __global__ void __launch_bounds__(32 * kDoughnutWarps)
 doughnut_kernel(Feature* __restrict__ out, const uint32_t* __restrict__ kept_count, uint32_t feat_cap,
                 const FinalizeConsts fc, const T* __restrict__ frames, int64_t frame_stride,
                 const int32_t* __restrict__ frame_index, const short2* __restrict__ dn_inds,
-                const int4* __restrict__ dn_meta) {
+                const int4* __restrict__ dn_meta, const RaggedFrame* __restrict__ rf) {
     __shared__ uint32_t hist[kDoughnutWarps * 256];
     const int g = blockIdx.y;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int total = (int)kept_count[g];
-    const T* raw = frames + (size_t)frame_index[g] * frame_stride;
+    const T* raw = rf ? (const T*)rf[g].raw : frames + (size_t)frame_index[g] * frame_stride;
+    const int H = rf ? rf[g].H : fc.H, W = rf ? rf[g].W : fc.W;
     uint32_t* myhist = hist + wid * 256;
     for (int q = blockIdx.x * kDoughnutWarps + wid; q < total; q += gridDim.x * kDoughnutWarps) {
         Feature* o = out + (size_t)g * feat_cap + q;
         Feature ft = *o;
         const int4 m = dn_meta[fc.log_style ? ft.ridx : 0];
-        doughnut_warp<T>(raw, fc.H, fc.W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);
+        doughnut_warp<T>(raw, H, W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);
         if (lane == 0) {
             o->d_raw = ft.d_raw;
             o->d_bg = ft.d_bg;
@@ -1373,16 +1375,17 @@ cudaError_t launch_walk(const float* processed, const T* frames, int64_t frame_s
                         int nframes, int n_slots, const uint32_t* cand_count, const uint32_t* cand_keys,
                         uint32_t cand_cap, uint32_t max_cands, const float* radii, const int32_t* angle_off,
                         const float2* angles, Feature* feats, uint32_t* feat_count, uint32_t feat_cap,
-                        uint32_t* flags, cudaStream_t st) {
+                        uint32_t* flags, cudaStream_t st, const RaggedFrame* rf) {
     if (max_cands == 0) return cudaSuccess;
     dim3 grid((max_cands + 127) / 128, nframes, n_slots);
+    if (rf && (radii || n_slots != 1)) return cudaErrorInvalidValue;   // ragged batches: trackpy style only
     if (!radii && n_slots == 1) {
         const int ri = (c.circle - 1) / 2;
 #define GT_WALK_FIXED(RI)                                                                                          \
     if (ri == RI) {                                                                                                \
         walk_kernel_fixed<T, RI><<<grid, 128, 0, st>>>(processed, frames, frame_stride, c, cand_count, cand_keys,  \
                                                        cand_cap, angle_off, angles, feats, feat_count, feat_cap,   \
-                                                       flags);                                                     \
+                                                       flags, rf);                                                 \
         return cudaGetLastError();                                                                                 \
     }
         GT_WALK_FIXED(2) GT_WALK_FIXED(3) GT_WALK_FIXED(4) GT_WALK_FIXED(5) GT_WALK_FIXED(6) GT_WALK_FIXED(7)
@@ -1448,16 +1451,17 @@ template <typename T>
 cudaError_t launch_finalize(const Feature* feats, const uint32_t* feat_count, uint32_t feat_cap, Feature* out,
                             uint32_t* kept_count, uint8_t* gscratch, const FinalizeConsts& fc, const T* frames,
                             int64_t frame_stride, const int32_t* frame_index, const short2* dn_inds,
-                            const int4* dn_meta, uint32_t* flags, int ngroups, cudaStream_t st) {
+                            const int4* dn_meta, uint32_t* flags, int ngroups, cudaStream_t st,
+                            const RaggedFrame* rf) {
     size_t smem = finalize_smem_bytes();
     cudaFuncSetAttribute(finalize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     finalize_kernel<T><<<ngroups, kFinalizeThreads, smem, st>>>(feats, feat_count, feat_cap, out, kept_count,
                                                                 gscratch, fc, frames, frame_stride, frame_index,
-                                                                dn_inds, dn_meta, flags);
+                                                                dn_inds, dn_meta, flags, rf);
     if (fc.doughnut && ngroups > 0) {
         dim3 grid(kDoughnutBlocks, ngroups);
         doughnut_kernel<T><<<grid, 32 * kDoughnutWarps, 0, st>>>(out, kept_count, feat_cap, fc, frames,
-                                                                  frame_stride, frame_index, dn_inds, dn_meta);
+                                                                  frame_stride, frame_index, dn_inds, dn_meta, rf);
     }
     return cudaGetLastError();
 }
@@ -1477,7 +1481,7 @@ cudaError_t launch_scatter(const Feature* feats, uint32_t feat_cap, const uint32
     template cudaError_t launch_walk<T>(const float*, const T*, int64_t, const LocateConsts&, int, int,          \
                                         const uint32_t*, const uint32_t*, uint32_t, uint32_t, const float*,      \
                                         const int32_t*, const float2*, Feature*, uint32_t*, uint32_t, uint32_t*, \
-                                        cudaStream_t);                                                           \
+                                        cudaStream_t, const RaggedFrame*);                                       \
     template cudaError_t launch_walk_local<T>(const T*, int64_t, const LocateConsts&, int, const uint32_t*,     \
                                               const uint32_t*, uint32_t, const int32_t*, const float2*, Feature*, \
                                               uint32_t*, uint32_t, uint32_t*, cudaStream_t);                     \
@@ -1487,7 +1491,8 @@ cudaError_t launch_scatter(const Feature* feats, uint32_t feat_cap, const uint32
                                                        int32_t, Feature*, uint32_t*, uint32_t, cudaStream_t);     \
     template cudaError_t launch_finalize<T>(const Feature*, const uint32_t*, uint32_t, Feature*, uint32_t*,      \
                                             uint8_t*, const FinalizeConsts&, const T*, int64_t, const int32_t*,  \
-                                            const short2*, const int4*, uint32_t*, int, cudaStream_t);
+                                            const short2*, const int4*, uint32_t*, int, cudaStream_t,            \
+                                            const RaggedFrame*);
 
 GT_INSTANTIATE(uint16_t)
 GT_INSTANTIATE(float)

@@ -5,12 +5,9 @@
 // instruction throughput.  A CTA owns a strip of 128 output columns and walks
 // down a segment of rows eight rows per step:
 //   A  the step's raw rows are staged in shared memory (4 pixels per load,
-//      converted exactly to float) as pairs of rows j and j + 4, the next
-//      step's are prefetched;
-//   B  row pass: each thread makes 4 adjacent columns of rows j and j + 4,
-//      the two rows as the lanes of packed f32x2 operations;
-//   C  column pass: each thread makes 2 adjacent columns of 2 rows, the two
-//      columns as the lanes of packed f32x2 operations;
+//      converted exactly to float), the next step's are prefetched;
+//   B  row pass: each thread makes 4 adjacent columns from float4 loads;
+//   C  column pass: each thread makes the step's 8 rows of one column;
 //   D  vertical dilation maximum, 8 rows of one column per thread;
 //   E  horizontal dilation maximum, the candidate test and the store of the
 //      segment's processed rows, 4 columns per thread, slots reserved once
@@ -19,9 +16,6 @@
 // every row twice (at r and r + ring), so any window of consecutive rows is
 // contiguous and every read in the tap loops is a constant offset from one
 // base address.  The tap loops are unrolled for the compile-time radius.
-// Packed f32x2 arithmetic (__ffma2_rn, __fadd2_rn, __fmul2_rn) rounds each
-// lane as its scalar operation does, so the packed stages compute the same
-// values as one scalar operation per pixel.
 // The floating-point operation sequence of every output is the oracle's:
 // sequential fused multiply-adds over the taps, sequential boxcar sums (for
 // integer inputs a pairwise window sum and sliding differences instead: every
@@ -65,11 +59,8 @@ struct StripGeom {
     static constexpr int RAWN = kStepRows * RWp;
     static constexpr int RAWPT = (RAWN + kStripThreads - 1) / kStripThreads;
     // the vertical maxima (stages D-E) reuse the staged raw rows (stages A-B)
-    // tap and divisor pairs for the packed stages follow the rings
-    static constexpr size_t off_pairs = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp + (size_t)(2 * PR) * PWp;
-    static constexpr size_t smem_floats = off_pairs + 2 * (2 * R + 1) + 8;
-    static constexpr int RAWV2 = (kStepRows / 2) * RW4;   // staging items: 4 pixels of rows j and j + 4
-    static constexpr int RAWV2PT = (RAWV2 + kStripThreads - 1) / kStripThreads;
+    static constexpr size_t smem_floats = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp +
+                                          (size_t)(2 * PR) * PWp;
     static constexpr int min_blocks = (smem_floats * 4 + 1024) * 3 <= 227 * 1024 ? 3 : 2;
     static_assert(RWp % 4 == 0 && RWp >= PWp + 2 * R, "staged raw row");
     static_assert(RWp >= PWp, "vertical maxima fit in the staging rows");
@@ -77,7 +68,6 @@ struct StripGeom {
     static_assert(4 * 31 + KD + 2 <= PW - 1 && SH4 + O + kStripTW <= PWp, "dilation windows inside the row");
     static_assert(KD >= kStepRows && kStepRows == 8, "vertical maxima: 8 rows share the window rows 7 .. KD-1");
     static_assert(PWp <= kStripThreads, "one thread per column in the column pass and vertical maxima");
-    static_assert(PWp % 2 == 0 && off_pairs % 2 == 0, "column pairs and tap pairs are 8-byte aligned");
 };
 
 template <typename T>
@@ -136,31 +126,6 @@ struct Tree<1> {
     __device__ __forceinline__ static float sum(const float* a) { return a[0]; }
 };
 
-template <int N>
-struct Tree2 {
-    __device__ __forceinline__ static float2 sum(const float2* a) {
-        return __fadd2_rn(Tree2<N / 2>::sum(a), Tree2<N - N / 2>::sum(a + N / 2));
-    }
-};
-template <>
-struct Tree2<1> {
-    __device__ __forceinline__ static float2 sum(const float2* a) { return a[0]; }
-};
-
-// a - b per lane (IEEE subtraction is addition of the negation)
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-
-// x / gnorm and x / kk per lane; dz holds (zh_g, zl_g, zh_k, zl_k) as pairs
-template <bool FAST>
-__device__ __forceinline__ float2 div2_gnorm(float2 x, const float2* dz, const LocateConsts& c) {
-    return FAST ? __ffma2_rn(x, dz[0], __fmul2_rn(x, dz[1]))
-                : make_float2(__fdiv_rn(x.x, c.gnorm), __fdiv_rn(x.y, c.gnorm));
-}
-template <bool FAST>
-__device__ __forceinline__ float2 div2_kk(float2 x, const float2* dz, const LocateConsts& c) {
-    return FAST ? __ffma2_rn(x, dz[2], __fmul2_rn(x, dz[3])) : make_float2(__fdiv_rn(x.x, c.kk), __fdiv_rn(x.y, c.kk));
-}
-
 template <bool FAST>
 __device__ __forceinline__ float div_gnorm(float x, const LocateConsts& c) {
     return FAST ? __fmaf_rn(x, c.zh_g, __fmul_rn(x, c.zl_g)) : __fdiv_rn(x, c.gnorm);
@@ -170,11 +135,15 @@ __device__ __forceinline__ float div_kk(float x, const LocateConsts& c) {
     return FAST ? __fmaf_rn(x, c.zh_k, __fmul_rn(x, c.zl_k)) : __fdiv_rn(x, c.kk);
 }
 
+// One tile: the strip of output columns [c0, c0 + 128) and rows [R0, R1) of
+// an H x W frame (img: its pixels, proc: its processed image), candidates
+// appended to the list counted by *cand_slot (keys at cout).
 template <typename T, int R, int KD, bool FAST>
-__global__ void __launch_bounds__(kStripThreads, StripGeom<R, KD>::min_blocks)
-strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restrict__ processed, const LocateConsts c,
-             int SH, int vec_ok, uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys,
-             uint32_t cand_cap, uint32_t* __restrict__ flags) {
+__device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __restrict__ proc, const LocateConsts& c,
+                                           const int H, const int W, const int c0, const int R0, const int R1,
+                                           const int vec_ok, const float thr, uint32_t* __restrict__ cand_slot,
+                                           uint32_t* __restrict__ cout, const uint32_t cand_cap,
+                                           uint32_t* __restrict__ flags) {
     using G = StripGeom<R, KD>;
     constexpr int O = G::O, E = G::E, PWp = G::PWp, RWp = G::RWp, XR = G::XR, PR = G::PR, SH4 = G::SH4;
     constexpr bool kInt = IsIntPix<T>::value;
@@ -185,21 +154,11 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     float* xb = xg + 2 * XR * PWp;              // [2XR][PWp]    row pass boxcar
     float* pr = xb + 2 * XR * PWp;              // [2PR][PWp]    processed rows, stored twice
     float* vb = stage;                          // [8][PWp]      vertical maxima (pc0-relative columns)
-    float2* stage2 = (float2*)stage;            // [4][RWp]      (row j, row j + 4) pixel pairs
-    float2* tp2 = (float2*)(sm + G::off_pairs); // [2R+1]        (tap, tap)
-    float2* dz = tp2 + (2 * R + 1);             // [4]           divisor pairs
 
-    const int H = c.H, W = c.W;
-    const int f = blockIdx.z;
-    const int c0 = blockIdx.x * kStripTW;
-    const int R0 = blockIdx.y * SH;
-    const int R1 = min(R0 + SH, H);
     const int x0 = R0 - O - R;          // first raw / row-pass row
     const int pc0 = c0 - O;             // first processed column of the strip's dilation windows
     const int xa = pc0 - R - SH4;       // first staged raw column (a multiple of 4)
     const int ps = xa + R;              // processed column of row-pass index 0 (= pc0 - SH4)
-    const T* img = frames + (size_t)f * frame_stride;
-    float* proc = processed + (size_t)f * H * W;
     const int tid = threadIdx.x;
     const bool edge_cols = (xa < 0) || (xa + RWp > W);
     const bool vec = vec_ok && !edge_cols;
@@ -209,20 +168,18 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
     // ---- A: staging of raw rows (registers hold the next step's pixels)
-    typename Quad<T>::V pv[G::RAWV2PT][2];
+    typename Quad<T>::V pv[G::RAWVPT];
     float ps_[G::RAWPT];
     auto load_raw = [&](int s) {
         const int rbase = x0 + kStepRows * s;
         if (vec) {
 #pragma unroll
-            for (int q = 0; q < G::RAWV2PT; q++) {
+            for (int q = 0; q < G::RAWVPT; q++) {
                 const int v = tid + q * kStripThreads;
-                if (v < G::RAWV2) {
+                if (v < G::RAWV) {
                     const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    const int gr0 = min(max(rbase + j, 0), H - 1);
-                    const int gr1 = min(max(rbase + j + 4, 0), H - 1);
-                    pv[q][0] = Quad<T>::load(img + (size_t)gr0 * W + xa + 4 * k4);
-                    pv[q][1] = Quad<T>::load(img + (size_t)gr1 * W + xa + 4 * k4);
+                    const int gr = min(max(rbase + j, 0), H - 1);
+                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
                 }
             }
         } else {
@@ -248,176 +205,133 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
     // start as zeros instead of whatever the previous kernel left.
     for (int i = tid; i < 2 * 2 * XR * PWp / 4; i += kStripThreads)
         ((float4*)xg)[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (tid <= 2 * R) tp2[tid] = make_float2(c.taps[tid], c.taps[tid]);
-    if (tid == 0) {
-        dz[0] = make_float2(c.zh_g, c.zh_g);
-        dz[1] = make_float2(c.zl_g, c.zl_g);
-        dz[2] = make_float2(c.zh_k, c.zh_k);
-        dz[3] = make_float2(c.zl_k, c.zl_k);
-    }
     const float trunc_thr = 1.0f / 255.0f;
-    // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
-    const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
-    uint32_t* cout = cand_keys + (size_t)f * cand_cap;
 
     for (int s = 0; s < nsteps; s++) {
         if (vec) {
 #pragma unroll
-            for (int q = 0; q < G::RAWV2PT; q++) {
+            for (int q = 0; q < G::RAWVPT; q++) {
                 const int v = tid + q * kStripThreads;
-                if (v < G::RAWV2) {
+                if (v < G::RAWV) {
                     const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    const float4 a = Quad<T>::cvt(pv[q][0]), b = Quad<T>::cvt(pv[q][1]);
-                    float4* dst = (float4*)(stage2 + j * RWp + 4 * k4);
-                    dst[0] = make_float4(a.x, b.x, a.y, b.y);
-                    dst[1] = make_float4(a.z, b.z, a.w, b.w);
+                    *(float4*)(stage + j * RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
                 }
             }
         } else {
 #pragma unroll
             for (int q = 0; q < G::RAWPT; q++) {
                 const int idx = tid + q * kStripThreads;
-                if (idx < G::RAWN) {
-                    const int j = idx / RWp, k = idx - j * RWp;
-                    stage[((j & 3) * RWp + k) * 2 + (j >> 2)] = ps_[q];
-                }
+                if (idx < G::RAWN) stage[idx] = ps_[q];
             }
         }
         __syncthreads();
         if (s + 1 < nsteps) load_raw(s + 1);
 
-        // ---- B: row pass (preprocess_rows.wgsl), rows j and j + 4 as the two
-        // lanes, 4 columns per thread
-        for (int t = tid; t < (kStepRows / 2) * G::NG; t += kStripThreads) {
-            const int jp = t / G::NG, gq = t - jp * G::NG;
-            const int col = 4 * gq;
-            const float4* src = (const float4*)(stage2 + jp * RWp + col);
-            float2 x[4 * G::NX4];
+        // ---- B: row pass (preprocess_rows.wgsl), 8 rows x PWp columns, 4 per thread
+        {
+            for (int t = tid; t < kStepRows * G::NG; t += kStripThreads) {
+                const int j = t / G::NG, gq = t - j * G::NG;
+                const int col = 4 * gq;
+                const float4* src = (const float4*)(stage + j * RWp + col);
+                float x[4 * G::NX4];
 #pragma unroll
-            for (int i = 0; i < 2 * G::NX4; i++) {
-                const float4 v = src[i];
-                x[2 * i] = make_float2(v.x, v.y);
-                x[2 * i + 1] = make_float2(v.z, v.w);
-            }
-            float2 og[4], ob[4];
-            float2 cs = make_float2(0.0f, 0.0f);
+                for (int i = 0; i < G::NX4; i++) {
+                    const float4 v = src[i];
+                    x[4 * i] = v.x;
+                    x[4 * i + 1] = v.y;
+                    x[4 * i + 2] = v.z;
+                    x[4 * i + 3] = v.w;
+                }
+                float og[4], ob[4];
+                float cs = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                float2 gs = make_float2(0.0f, 0.0f);
-                if (!edge_cols) {
+                for (int k = 0; k < 4; k++) {
+                    float gs = 0.0f;
+                    if (!edge_cols) {
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) gs = __ffma2_rn(tp2[i], x[k + i], gs);
-                } else {
-                    // Gaussian taps outside the frame are skipped
-                    const int gcol = ps + col + k;
+                        for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
+                    } else {
+                        // Gaussian taps outside the frame are skipped
+                        const int gcol = ps + col + k;
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) {
-                        const int gc = gcol + i - R;
-                        if (gc >= 0 && gc < W) {
-                            gs.x = __fmaf_rn(c.taps[i], x[k + i].x, gs.x);
-                            gs.y = __fmaf_rn(c.taps[i], x[k + i].y, gs.y);
+                        for (int i = 0; i <= 2 * R; i++) {
+                            const int gc = gcol + i - R;
+                            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x[k + i], gs);
                         }
                     }
-                }
-                if (kInt) {
-                    // exact integers: the window sum, then sliding differences
-                    if (k == 0) cs = Tree2<2 * R + 1>::sum(x);
-                    else cs = __fadd2_rn(cs, sub2(x[k + 2 * R], x[k - 1]));
-                } else {
-                    cs = make_float2(0.0f, 0.0f);
+                    if (kInt) {
+                        // exact integers: the window sum, then sliding differences
+                        if (k == 0) cs = Tree<2 * R + 1>::sum(x);
+                        else cs = __fadd_rn(cs, __fsub_rn(x[k + 2 * R], x[k - 1]));
+                    } else {
+                        cs = 0.0f;
 #pragma unroll
-                    for (int i = 0; i <= 2 * R; i++) cs = __fadd2_rn(cs, x[k + i]);
+                        for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, x[k + i]);
+                    }
+                    og[k] = div_gnorm<FAST>(gs, c);
+                    ob[k] = cs;
                 }
-                og[k] = div2_gnorm<FAST>(gs, dz, c);
-                ob[k] = cs;
+                const int xrow = (kStepRows * s + j) % XR;
+                const float4 g4 = make_float4(og[0], og[1], og[2], og[3]);
+                const float4 b4 = make_float4(ob[0], ob[1], ob[2], ob[3]);
+                *(float4*)(xg + xrow * PWp + col) = g4;
+                *(float4*)(xg + (xrow + XR) * PWp + col) = g4;
+                *(float4*)(xb + xrow * PWp + col) = b4;
+                *(float4*)(xb + (xrow + XR) * PWp + col) = b4;
             }
-            const int r0 = (kStepRows * s + jp) % XR, r1 = (kStepRows * s + jp + 4) % XR;
-            const float4 g0 = make_float4(og[0].x, og[1].x, og[2].x, og[3].x);
-            const float4 g1 = make_float4(og[0].y, og[1].y, og[2].y, og[3].y);
-            const float4 b0_ = make_float4(ob[0].x, ob[1].x, ob[2].x, ob[3].x);
-            const float4 b1_ = make_float4(ob[0].y, ob[1].y, ob[2].y, ob[3].y);
-            *(float4*)(xg + r0 * PWp + col) = g0;
-            *(float4*)(xg + (r0 + XR) * PWp + col) = g0;
-            *(float4*)(xg + r1 * PWp + col) = g1;
-            *(float4*)(xg + (r1 + XR) * PWp + col) = g1;
-            *(float4*)(xb + r0 * PWp + col) = b0_;
-            *(float4*)(xb + (r0 + XR) * PWp + col) = b0_;
-            *(float4*)(xb + r1 * PWp + col) = b1_;
-            *(float4*)(xb + (r1 + XR) * PWp + col) = b1_;
         }
         __syncthreads();
 
         // ---- C: column pass (preprocess_cols.wgsl) for the step's 8 processed
-        // rows q = x0 + 8s - R + k: each thread makes 2 adjacent columns (the
-        // two lanes) of 2 rows
-        {
-            constexpr int NP = PWp / 2;
-            // row-pass rows of processed row q: relative index 8s - 2R + k + i
+        // rows q = x0 + 8s - R + k, one column per thread
+        if (tid < PWp) {
+            const int pc = tid;
+            const int q0 = x0 + kStepRows * s - R;
+            const int gcol = ps + pc;
+            // row-pass rows q0 - R .. q0 + 7 + R: relative index 8s - 2R + i
             const int w0 = (kStepRows * s + (XR - 2 * R)) % XR;
+            const float* pg = xg + w0 * PWp + pc;
+            const float* pb = xb + w0 * PWp + pc;
+            float vg[kStepRows + 2 * R], vbx[kStepRows + 2 * R];
+#pragma unroll
+            for (int i = 0; i < kStepRows + 2 * R; i++) {
+                vg[i] = pg[i * PWp];
+                vbx[i] = pb[i * PWp];
+            }
+            const bool col_in = (gcol >= 0 && gcol < W);
+            const bool rows_in = (q0 >= R && q0 + kStepRows - 1 < H - R);
+            float cs = 0.0f;
+            // processed row q has relative index q - (x0 - R) = 8s + k
             const int p0 = (kStepRows * s) % PR;
-            for (int task = tid; task < (kStepRows / 2) * NP; task += kStripThreads) {
-                const int kq = task / NP, cp = task - kq * NP;
-                const int pc = 2 * cp, kr = 2 * kq;
-                const int q0 = x0 + kStepRows * s - R + kr;
-                const int gcol = ps + pc;
-                const float2* pg = (const float2*)(xg + (w0 + kr) * PWp + pc);
-                const float2* pb = (const float2*)(xb + (w0 + kr) * PWp + pc);
-                const bool cin0 = (gcol >= 0 && gcol < W), cin1 = (gcol + 1 >= 0 && gcol + 1 < W);
-                const bool rows_in = (q0 >= R && q0 + 1 < H - R);
-                // the Gaussian sums of both rows first, then the boxcar sums:
-                // one window of rows is live at a time
-                float2 gq[2];
-                {
-                    float2 vg[2 + 2 * R];
 #pragma unroll
-                    for (int i = 0; i < 2 + 2 * R; i++) vg[i] = pg[i * (PWp / 2)];
+            for (int k = 0; k < kStepRows; k++) {
+                const int q = q0 + k;
+                float gs = 0.0f;
+                if (rows_in) {
 #pragma unroll
-                    for (int k = 0; k < 2; k++) {
-                        const int q = q0 + k;
-                        float2 gs = make_float2(0.0f, 0.0f);
-                        if (rows_in) {
+                    for (int i = 0; i <= 2 * R; i++) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
+                } else {
 #pragma unroll
-                            for (int i = 0; i <= 2 * R; i++) gs = __ffma2_rn(tp2[i], vg[k + i], gs);
-                        } else {
-#pragma unroll
-                            for (int i = 0; i <= 2 * R; i++) {
-                                const int gr = q + i - R;
-                                if (gr >= 0 && gr < H) {
-                                    gs.x = __fmaf_rn(c.taps[i], vg[k + i].x, gs.x);
-                                    gs.y = __fmaf_rn(c.taps[i], vg[k + i].y, gs.y);
-                                }
-                            }
-                        }
-                        gq[k] = div2_gnorm<FAST>(gs, dz, c);
+                    for (int i = 0; i <= 2 * R; i++) {
+                        const int gr = q + i - R;
+                        if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], vg[k + i], gs);
                     }
                 }
-                float2 vbx[2 + 2 * R];
+                if (kInt) {
+                    if (k == 0) cs = Tree<2 * R + 1>::sum(vbx);
+                    else cs = __fadd_rn(cs, __fsub_rn(vbx[k + 2 * R], vbx[k - 1]));
+                } else {
+                    cs = 0.0f;
 #pragma unroll
-                for (int i = 0; i < 2 + 2 * R; i++) vbx[i] = pb[i * (PWp / 2)];
-                float2 cs = make_float2(0.0f, 0.0f);
-#pragma unroll
-                for (int k = 0; k < 2; k++) {
-                    const int q = q0 + k;
-                    if (kInt) {
-                        if (k == 0) cs = Tree2<2 * R + 1>::sum(vbx);
-                        else cs = __fadd2_rn(cs, sub2(vbx[k + 2 * R], vbx[k - 1]));
-                    } else {
-                        cs = make_float2(0.0f, 0.0f);
-#pragma unroll
-                        for (int i = 0; i <= 2 * R; i++) cs = __fadd2_rn(cs, vbx[k + i]);
-                    }
-                    float2 r = sub2(gq[k], div2_kk<FAST>(cs, dz, c));
-                    if (c.truncate) {
-                        if (r.x < trunc_thr) r.x = 0.0f;
-                        if (r.y < trunc_thr) r.y = 0.0f;
-                    }
-                    const bool q_in = (q >= 0 && q < H);
-                    const float2 v = make_float2((cin0 && q_in) ? r.x : -INFINITY, (cin1 && q_in) ? r.y : -INFINITY);
-                    int pp = p0 + kr + k;
-                    if (pp >= PR) pp -= PR;
-                    *(float2*)(pr + pp * PWp + pc) = v;
-                    *(float2*)(pr + (pp + PR) * PWp + pc) = v;
+                    for (int i = 0; i <= 2 * R; i++) cs = __fadd_rn(cs, vbx[k + i]);
                 }
+                float r = __fsub_rn(div_gnorm<FAST>(gs, c), div_kk<FAST>(cs, c));
+                if (c.truncate && r < trunc_thr) r = 0.0f;
+                const float v = (col_in && q >= 0 && q < H) ? r : -INFINITY;
+                int pp = p0 + k;
+                if (pp >= PR) pp -= PR;
+                pr[pp * PWp + pc] = v;
+                pr[(pp + PR) * PWp + pc] = v;
             }
         }
         __syncthreads();
@@ -527,7 +441,7 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
             const int wtot = __shfl_sync(0xffffffffu, incl, 31);
             uint32_t base = 0;
             if (wtot > 0) {
-                if (lane == 31) base = atomicAdd(cand_count + f, (uint32_t)wtot);
+                if (lane == 31) base = atomicAdd(cand_slot, (uint32_t)wtot);
                 base = __shfl_sync(0xffffffffu, base, 31);
             }
             uint32_t pos = base + (uint32_t)(incl - cnt);
@@ -541,6 +455,41 @@ strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restri
             }
         }
         __syncthreads();
+    }
+}
+
+template <typename T, int R, int KD, bool FAST>
+__global__ void __launch_bounds__(kStripThreads, StripGeom<R, KD>::min_blocks)
+strip_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __restrict__ processed, const LocateConsts c,
+             int SH, int vec_ok, uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys,
+             uint32_t cand_cap, uint32_t* __restrict__ flags) {
+    const int H = c.H, W = c.W;
+    const int f = blockIdx.z;
+    const int R0 = blockIdx.y * SH;
+    // extract_max.wgsl:37: pic_std * snr * rough_snr_factor
+    const float thr = c.frame_std ? __fmul_rn(__fmul_rn(c.frame_std[f], c.snr), c.rough) : c.thr;
+    strip_tile<T, R, KD, FAST>(frames + (size_t)f * frame_stride, processed + (size_t)f * H * W, c, H, W,
+                               blockIdx.x * kStripTW, R0, min(R0 + SH, H), vec_ok, thr, cand_count + f,
+                               cand_keys + (size_t)f * cand_cap, cand_cap, flags);
+}
+
+// Many frames of different sizes (frames of many videos) in one persistent
+// launch: CTAs take tiles from a task list with a fixed stride.  The task and
+// frame tables live in device memory, so a captured launch replays for any
+// batch whose tables were rewritten.
+template <typename T, int R, int KD, bool FAST>
+__global__ void __launch_bounds__(kStripThreads, StripGeom<R, KD>::min_blocks)
+strip_ragged_kernel(const RaggedFrame* __restrict__ frames, const StripTask* __restrict__ tasks,
+                    const int32_t* __restrict__ ntasks, float* __restrict__ processed, const LocateConsts c,
+                    uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys, uint32_t cand_cap,
+                    uint32_t* __restrict__ flags) {
+    const int n = *ntasks;
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const StripTask tk = tasks[t];
+        const RaggedFrame d = frames[tk.slot];
+        strip_tile<T, R, KD, FAST>((const T*)d.raw, processed + d.proc_off, c, d.H, d.W, tk.c0, tk.r0, tk.r1,
+                                   d.vec_ok, c.thr, cand_count + tk.slot, cand_keys + (size_t)tk.slot * cand_cap,
+                                   cand_cap, flags);
     }
 }
 
@@ -591,6 +540,54 @@ bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const
 #undef GT_STRIP_TRY
     return false;
 }
+
+template <typename T, int R, int KD, bool FAST>
+cudaError_t strip_ragged_launch(const RaggedFrame* frames, const StripTask* tasks, const int32_t* ntasks, int grid,
+                                float* processed, const LocateConsts& c, uint32_t* cand_count, uint32_t* cand_keys,
+                                uint32_t cand_cap, uint32_t* flags, cudaStream_t st) {
+    const size_t smem = strip_smem<R, KD>();
+    cudaFuncSetAttribute(strip_ragged_kernel<T, R, KD, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(strip_ragged_kernel<T, R, KD, FAST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    strip_ragged_kernel<T, R, KD, FAST><<<grid, kStripThreads, smem, st>>>(frames, tasks, ntasks, processed, c,
+                                                                            cand_count, cand_keys, cand_cap, flags);
+    return cudaGetLastError();
+}
+
+template <typename T>
+bool launch_strip_ragged(const RaggedFrame* frames, const StripTask* tasks, const int32_t* ntasks, int grid,
+                         float* processed, const LocateConsts& c, uint32_t* cand_count, uint32_t* cand_keys,
+                         uint32_t cand_cap, uint32_t* flags, cudaStream_t st, cudaError_t* err) {
+    constexpr bool kInt = IsIntPix<T>::value;
+    if (kInt && !c.fast_div) return false;
+#define GT_STRIP_TRY(RR, KK)                                                                                  \
+    if (c.R == RR && c.kd == KK) {                                                                           \
+        *err = strip_ragged_launch<T, RR, KK, kInt>(frames, tasks, ntasks, grid, processed, c, cand_count,   \
+                                                    cand_keys, cand_cap, flags, st);                         \
+        return true;                                                                                         \
+    }
+    GT_STRIP_CASES(GT_STRIP_TRY)
+#undef GT_STRIP_TRY
+    return false;
+}
+
+template <typename T>
+int strip_blocks_per_sm(const LocateConsts& c) {
+#define GT_STRIP_TRY(RR, KK)                                                                                  \
+    if (c.R == RR && c.kd == KK) return StripGeom<RR, KK>::min_blocks;
+    GT_STRIP_CASES(GT_STRIP_TRY)
+#undef GT_STRIP_TRY
+    return 0;
+}
+
+#define GT_STRIP_RAGGED_INST(T)                                                                                  \
+    template bool launch_strip_ragged<T>(const RaggedFrame*, const StripTask*, const int32_t*, int, float*,      \
+                                         const LocateConsts&, uint32_t*, uint32_t*, uint32_t, uint32_t*,         \
+                                         cudaStream_t, cudaError_t*);                                            \
+    template int strip_blocks_per_sm<T>(const LocateConsts&);
+GT_STRIP_RAGGED_INST(uint16_t)
+GT_STRIP_RAGGED_INST(float)
+GT_STRIP_RAGGED_INST(uint8_t)
 
 template bool launch_strip<uint16_t>(const uint16_t*, int64_t, float*, const LocateConsts&, int, uint32_t*,
                                      uint32_t*, uint32_t, uint32_t*, cudaStream_t, cudaError_t*);

@@ -226,8 +226,9 @@ def batch_sharded(video, diameter, prefix=None, tracker=None, **kwargs):
         if tracker is not None:
             return tracker(video[f0:f1], range(f0, f1), search_range if linked else None, memory, **kwargs)
         extra = dict(search_range=search_range, memory=memory) if linked else {}
-        # frames= keeps the global frame numbers in the table
-        return api.batch(video[f0:f1], diameter, frames=range(f0, f1), **kwargs, **extra)
+        # frames= selects frames f0 .. f1-1 of the video and keeps their
+        # global numbers in the table
+        return api.batch(video, diameter, frames=range(f0, f1), **kwargs, **extra)
 
     if search_range is None:
         part = track(a, b, False)
