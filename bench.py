@@ -295,6 +295,16 @@ def run_ragged(args):
     ms_loop, rows_loop = timed(loop)
     if rows != rows_loop:
         raise SystemExit("gt_batch_videos found %d rows, the gt_batch loop %d" % (rows, rows_loop))
+    # where one call's time goes: device time of the stages, host time of the phases
+    ctx.profile(True)
+    together()
+    parts = {}
+    for name in ("ragged_wave", "scatter", "link_sort", "link_lists", "link_video", "link_durations", "round_ids",
+                 "host_locate", "host_assemble", "host_link"):
+        k, kms = ctx.profile_read(name)
+        if k:
+            parts[name] = {"count": k, "ms": kms}
+    ctx.profile(False)
     line = {"metric": "frames/s, 64 ragged videos (one gt_batch_videos call)", "value": frames / (ms / 1000.0),
             "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -302,6 +312,7 @@ def run_ragged(args):
                            l2="inputs (%.1f GB) larger than L2; no flush" % (pixels * 2 / 1e9)),
             "features_per_s": rows / (ms / 1000.0), "features": rows,
             "loop_of_gt_batch": {"value": frames / (ms_loop / 1000.0), "ms_per_step": ms_loop},
+            "profile_one_call": parts,
             "gpu_launches": launches, "clocks": clk}
     print(json.dumps(line))
     return 0

@@ -201,11 +201,15 @@ def batch_videos(videos, diameter, **kwargs):
     """``batch`` over many videos (any frame sizes and lengths) in one call.
 
     Returns one DataFrame per video, each equal to ``batch(video, diameter,
-    **kwargs)``.  The videos are located one after another and then linked
-    together in one GPU launch (one linker per video running side by side),
-    which is where a loop of ``batch`` calls spends most of its time on many
-    short videos.  ``frames`` and ``linker_reset_points`` are not supported
-    here.  Not part of the reference's API (it processes one video per call).
+    **kwargs)``.  The frames of all videos are located together in waves:
+    one launch per stage covers every frame of a wave whatever its size (a
+    persistent tile kernel, replayed as a CUDA graph, with the tile height
+    and wave size picked by an autotuner); parameter sets the waves do not
+    cover (snr, adaptive background, illumination correction) locate video
+    by video.  The videos are then linked together in one GPU launch (one
+    linker per video running side by side).  ``frames`` and
+    ``linker_reset_points`` are not supported here.  Not part of the
+    reference's API (it processes one video per call).
     """
     for k in ("frames", "linker_reset_points"):
         if kwargs.get(k) is not None:

@@ -849,11 +849,12 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     return GT_OK;
 }
 
-// Assemble the output table from per-frame results (kept_count, feats_out).
+// Assemble the output table from per-frame results (kept_count, feats_out)
+// of the NT frame slots starting at slot0.
 gt_status assemble_table(gt_ctx* ctx, int64_t NT, const std::vector<int64_t>& frame_numbers, bool log_style,
-                         gt_table* tab, std::vector<int64_t>& row_off) {
+                         gt_table* tab, std::vector<int64_t>& row_off, int64_t slot0 = 0) {
     std::vector<uint32_t> kept(NT);
-    CK(cudaMemcpyAsync(kept.data(), ctx->kept_count.p, NT * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(kept.data(), ctx->kept_count.as<uint32_t>() + slot0, NT * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     row_off.assign(NT + 1, 0);
     uint32_t maxk = 0;
@@ -882,8 +883,8 @@ gt_status assemble_table(gt_ctx* ctx, int64_t NT, const std::vector<int64_t>& fr
     for (int64_t g0 = 0; g0 < NT; g0 += 65535) {
         int ng = (int)std::min<int64_t>(65535, NT - g0);
         Prof pf(ctx, "scatter");
-        CK(launch_scatter(ctx->feats_out.as<Feature>() + (size_t)g0 * ctx->feat_cap, ctx->feat_cap,
-                          ctx->kept_count.as<uint32_t>() + g0, maxk, ctx->row_off.as<int64_t>(),
+        CK(launch_scatter(ctx->feats_out.as<Feature>() + (size_t)(slot0 + g0) * ctx->feat_cap, ctx->feat_cap,
+                          ctx->kept_count.as<uint32_t>() + slot0 + g0, maxk, ctx->row_off.as<int64_t>(),
                           ctx->frame_num.as<int64_t>(), tc, (int32_t)g0, ng, ctx->st));
     }
     return GT_OK;
@@ -1252,19 +1253,406 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
     return GT_OK;
 }
 
-// Many videos in one call: each video is located into its own table (as
-// gt_batch would, without linking), then every video is linked in ONE launch
-// of the whole-video linker (one CTA per video), so the videos' sequential
-// frame scans run side by side.  Results equal separate gt_batch calls.
+// ------------------------------------------------------------ ragged batches
+// Many videos of uneven frame size located together: the frames of all
+// videos, in order, are cut into waves of at most kRaggedSlots frames whose
+// processed images fit a byte budget.  A wave runs ONE launch per stage over
+// all its frames — the persistent strip kernel over the wave's tile list,
+// the walk over every frame's candidates, finalize and the doughnut over the
+// frame slots — each launch reading the wave's frame and tile tables from
+// device memory.  The launch sequence is therefore captured once as a CUDA
+// graph and replayed for every wave after the tables are rewritten.  Tile
+// height and wave budget come from the autotuner below.  Results equal one
+// gt_batch call per video (same kernels per tile and per frame).
+constexpr int kRaggedSlots = 256;
+
+struct RaggedShape {
+    int32_t seg;       // rows per strip tile
+    int64_t budget;    // processed-image bytes per wave
+};
+
+// Candidate shapes: tall tiles waste the fewest halo rows, short ones balance
+// the persistent CTAs better on small frames; a small wave keeps its
+// processed images in L2 for the walk, a large one fills the GPU with tiles.
+const RaggedShape kRaggedShapes[] = {{512, 1LL << 30}, {256, 1LL << 30}, {128, 1LL << 30},
+                                     {512, 192LL << 20}, {256, 192LL << 20}, {128, 192LL << 20}};
+constexpr int kRaggedNShapes = (int)(sizeof(kRaggedShapes) / sizeof(kRaggedShapes[0]));
+
+template <typename T>
+bool ragged_eligible(const gt_params& p, const LocateConsts& c) {
+    if (p.style != GT_STYLE_TRACKPY || p.has_snr || p.has_minmass_snr || p.has_adaptive_background ||
+        p.has_illumination_sigma)
+        return false;
+    if (!std::is_same<T, float>::value && !c.fast_div) return false;
+    const int ri = (c.circle - 1) / 2;
+    return strip_tile_width<T>(c) > 0 && ri >= 2 && ri <= 7;
+}
+
+struct RaggedSlot {
+    int32_t video;
+    int64_t t;
+};
+
+template <typename T>
+gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConsts& c, int32_t nv,
+                              const void* const* frames, const bool* on_device, const int64_t* T_, const int32_t* H_,
+                              const int32_t* W_, gt_table** tabs, std::vector<std::vector<int64_t>>& row_off) {
+    const int TW = strip_tile_width<T>(c);
+    // slots of the call: video v's frame t is slot vslot[v] + t
+    std::vector<int64_t> vslot((size_t)nv + 1, 0);
+    for (int32_t v = 0; v < nv; v++) vslot[(size_t)v + 1] = vslot[(size_t)v] + T_[v];
+    const int64_t NT = vslot[(size_t)nv];
+    int64_t max_px = 0;
+    for (int32_t v = 0; v < nv; v++) max_px = std::max<int64_t>(max_px, (int64_t)H_[v] * W_[v]);
+    int64_t max_budget = 0;
+    for (const auto& s : kRaggedShapes) max_budget = std::max(max_budget, s.budget);
+    max_budget = std::max<int64_t>(max_budget, max_px * 4);
+    ctx->total = NT;
+    ctx->done = 0;
+    // tuned shape for this workload
+    char keybuf[160];
+    snprintf(keybuf, sizeof(keybuf), "%d:%d:%d:%d:%d:%lld", (int)sizeof(T), c.R, c.kd, c.circle, p.doughnut_correction,
+             (long long)max_px);
+    const std::string tkey = keybuf;
+    auto tuned = ctx->rg_best.find(tkey);
+    // the tables
+    int64_t max_tasks = 0;
+    for (const auto& s : kRaggedShapes) {
+        // a wave's tiles: per frame ceil(W/TW) strips x ceil(H/seg) segments, at most
+        int64_t m = 0;
+        for (int32_t v = 0; v < nv; v++)
+            m = std::max<int64_t>(m, (int64_t)((W_[v] + TW - 1) / TW) * ((H_[v] + s.seg - 1) / s.seg));
+        max_tasks = std::max<int64_t>(max_tasks, m * kRaggedSlots);
+    }
+    const int grid = ctx->num_sms * strip_blocks_per_sm<T>(c);
+    // angle and doughnut tables, finalize constants (as locate_pass)
+    std::vector<float2> atab;
+    std::vector<int32_t> aoff;
+    angle_tables(std::max(0, (c.circle - 1) / 2), atab, aoff);
+    std::vector<short2> dn;
+    std::vector<int4> dmeta;
+    doughnut_tables(p, std::vector<float>{(float)p.diameter / 2.0f}, dn, dmeta);
+    FinalizeConsts fc;
+    std::memset(&fc, 0, sizeof(fc));
+    fc.H = (int32_t)0;
+    fc.W = (int32_t)0;
+    fc.filter_close = p.filter_close ? 1 : 0;
+    fc.separation = (float)p.separation;
+    {
+        int rint = std::max(0, (c.circle - 1) / 2);
+        long long band = (long long)std::ceil(fc.separation) + 2LL * ((long long)c.max_iter + rint) + 2;
+        fc.band = (c.truncate && band < (1LL << 30)) ? (int32_t)band : -1;
+    }
+    fc.doughnut = p.doughnut_correction ? 1 : 0;
+    for (int attempt = 0;; attempt++) {
+        const uint32_t cand_cap = ctx->cand_cap, feat_cap = ctx->feat_cap;
+        size_t fin_per_frame = 0;
+        if (feat_cap > (uint32_t)kFinalizeSmemSort) {
+            size_t np2 = 1;
+            while (np2 < feat_cap) np2 <<= 1;
+            fin_per_frame = (np2 * 17 + 255) & ~(size_t)255;
+        }
+        fc.scratch_per_frame = fin_per_frame;
+        CK(ctx->processed.ensure((size_t)max_budget));
+        CK(ctx->cand_count.ensure((size_t)kRaggedSlots * 4));
+        CK(ctx->cand_keys.ensure((size_t)kRaggedSlots * cand_cap * 4));
+        CK(ctx->feats_raw.ensure((size_t)kRaggedSlots * feat_cap * sizeof(Feature)));
+        CK(ctx->feat_count.ensure((size_t)kRaggedSlots * 4));
+        // one more result slot: the padding frames of a short wave write there
+        CK(ctx->feats_out.ensure((size_t)(NT + 1) * feat_cap * sizeof(Feature)));
+        CK(ctx->kept_count.ensure((size_t)(NT + 1) * 4));
+        CK(ctx->flags.ensure(16));
+        CK(ctx->walk_starts.ensure(8));
+        CK(ctx->fin_scratch.ensure(std::max<size_t>(fin_per_frame * kRaggedSlots, 256)));
+        CK(ctx->rg_frames.ensure((size_t)kRaggedSlots * sizeof(RaggedFrame)));
+        CK(ctx->rg_tasks.ensure((size_t)std::max<int64_t>(max_tasks, 1) * sizeof(StripTask)));
+        CK(ctx->rg_ntasks.ensure(4));
+        {
+            std::vector<int32_t> ident(kRaggedSlots);
+            for (int i = 0; i < kRaggedSlots; i++) ident[i] = i;
+            CKS(upload(ctx, ctx->ident, ident));
+        }
+        CKS(upload(ctx, ctx->tabs_f, atab));
+        CKS(upload(ctx, ctx->tabs_i, aoff));
+        CKS(upload(ctx, ctx->tabs_s, dn));
+        CKS(upload(ctx, ctx->tabs_m, dmeta));
+        CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
+        CK(cudaMemsetAsync(ctx->walk_starts.p, 0, 8, ctx->st));
+        bool any_host = false;
+        for (int32_t v = 0; v < nv; v++) any_host |= !on_device[v];
+        if (any_host) {
+            CK(ctx->stage[0].ensure((size_t)max_budget / 4 * sizeof(T)));
+            CK(ctx->stage[1].ensure((size_t)max_budget / 4 * sizeof(T)));
+        }
+        RaggedFrame* d_frames = ctx->rg_frames.as<RaggedFrame>();
+        StripTask* d_tasks = ctx->rg_tasks.as<StripTask>();
+        int32_t* d_ntasks = ctx->rg_ntasks.as<int32_t>();
+        float* proc = ctx->processed.as<float>();
+        uint32_t* flags = ctx->flags.as<uint32_t>();
+
+        // ---- the stage sequence of one wave (captured once, then replayed)
+        auto stages = [&](cudaStream_t st) -> gt_status {
+            CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)kRaggedSlots * 4, st));
+            CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)kRaggedSlots * 4, st));
+            cudaError_t e = cudaSuccess;
+            if (!launch_strip_ragged<T>(d_frames, d_tasks, d_ntasks, grid, proc, c, ctx->cand_count.as<uint32_t>(),
+                                        ctx->cand_keys.as<uint32_t>(), cand_cap, flags, st, &e))
+                return set_err(ctx, GT_ERR_INTERNAL, "no strip kernel for this parameter set");
+            CK(e);
+            sum_counts_kernel<<<1, 256, 0, st>>>(ctx->cand_count.as<uint32_t>(), kRaggedSlots, cand_cap,
+                                                 ctx->walk_starts.as<unsigned long long>());
+            CK(cudaGetLastError());
+            CK(launch_walk<T>(proc, (const T*)nullptr, 0, c, kRaggedSlots, 1, ctx->cand_count.as<uint32_t>(),
+                              ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap, nullptr, ctx->tabs_i.as<int32_t>(),
+                              ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
+                              feat_cap, flags, st, d_frames));
+            CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
+                                  ctx->feats_out.as<Feature>(), ctx->kept_count.as<uint32_t>(),
+                                  ctx->fin_scratch.as<uint8_t>(), fc, (const T*)nullptr, 0, ctx->ident.as<int32_t>(),
+                                  ctx->tabs_s.as<short2>(), ctx->tabs_m.as<int4>(), flags, kRaggedSlots, st,
+                                  d_frames));
+            return GT_OK;
+        };
+        // the graph names these buffers and sizes; a call that moved any of
+        // them captures a new one
+        char gk[512];
+        snprintf(gk, sizeof(gk), "%p %p %p %p %p %p %p %p %p %p %p %p %p %p %p %u %u %d %d %d %d %d", (void*)d_frames,
+                 (void*)d_tasks, (void*)d_ntasks, (void*)proc, ctx->cand_count.p, ctx->cand_keys.p, ctx->feats_raw.p,
+                 ctx->feat_count.p, ctx->feats_out.p, ctx->kept_count.p, ctx->fin_scratch.p, ctx->tabs_f.p,
+                 ctx->tabs_s.p, ctx->walk_starts.p, (void*)flags, cand_cap, feat_cap, (int)sizeof(T), c.R, c.kd,
+                 c.circle, grid);
+        std::string gkey = std::string(gk) + ":" + std::string((const char*)&c, sizeof(c)) +
+                           std::string((const char*)&fc, sizeof(fc));
+        if (ctx->rg_graph && ctx->rg_graph_key != gkey) {
+            cudaGraphExecDestroy(ctx->rg_graph);
+            ctx->rg_graph = nullptr;
+        }
+        if (!ctx->rg_graph) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+            gt_status sst = stages(ctx->st);
+            cudaError_t ee = cudaStreamEndCapture(ctx->st, &g);
+            if (sst != GT_OK) {
+                if (g) cudaGraphDestroy(g);
+                return sst;
+            }
+            CK(ee);
+            cudaError_t ei = cudaGraphInstantiate(&ctx->rg_graph, g, 0);
+            cudaGraphDestroy(g);
+            CK(ei);
+            ctx->rg_graph_key = gkey;
+        }
+
+        // ---- waves
+        int64_t cur = 0;     // next slot of the call
+        int shape_i = -1;    // tuning: index of the shape being timed
+        std::vector<double> shape_ms(kRaggedNShapes, 0.0), shape_px(kRaggedNShapes, 0.0);
+        RaggedShape shape = kRaggedShapes[0];
+        if (tuned != ctx->rg_best.end()) shape = RaggedShape{tuned->second.first, tuned->second.second};
+        // tune when the call has waves to spare and no shape is known yet
+        int64_t tot_px = 0;
+        for (int32_t v = 0; v < nv; v++) tot_px += T_[v] * (int64_t)H_[v] * W_[v];
+        const bool tune = tuned == ctx->rg_best.end() &&
+                          (ctx->rg_force_tune || tot_px * 4 >= 8 * kRaggedNShapes * (1LL << 30));
+        if (tune) shape_i = 0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (tune) {
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+        }
+        std::vector<RaggedSlot> wave;
+        std::vector<RaggedFrame> hf(kRaggedSlots);
+        std::vector<StripTask> htask;
+        int wave_no = 0;
+        auto video_of = [&](int64_t slot) -> int32_t {
+            return (int32_t)(std::upper_bound(vslot.begin(), vslot.end(), slot) - vslot.begin() - 1);
+        };
+        while (cur < NT) {
+            if (interrupted(ctx)) {
+                cudaStreamSynchronize(ctx->st);
+                cudaStreamSynchronize(ctx->cp);
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+                return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
+            }
+            if (shape_i >= 0) shape = kRaggedShapes[shape_i % kRaggedNShapes];
+            // the wave: frames in order while the budget and the slots last
+            // (the tuning test hook shrinks the budgets, so that small calls
+            // run many waves)
+            const int64_t budget = ctx->rg_force_tune ? std::max<int64_t>(shape.budget >> 12, 1) : shape.budget;
+            wave.clear();
+            int64_t used = 0;
+            while (cur < NT && (int)wave.size() < kRaggedSlots) {
+                const int32_t v = video_of(cur);
+                const int64_t px = (int64_t)H_[v] * W_[v];
+                if (!wave.empty() && used + px * 4 > budget) break;
+                wave.push_back(RaggedSlot{v, cur - vslot[(size_t)v]});
+                used += px * 4;
+                cur++;
+            }
+            // host frames of the wave go to a staging buffer
+            const int b = wave_no & 1;
+            bool staged = false;
+            int64_t soff = 0;
+            std::vector<const void*> raw(wave.size());
+            for (size_t i = 0; i < wave.size(); i++) {
+                const int32_t v = wave[i].video;
+                const size_t fb = (size_t)H_[v] * W_[v] * sizeof(T);
+                const T* src = (const T*)frames[v] + (size_t)wave[i].t * H_[v] * W_[v];
+                if (on_device[v]) {
+                    raw[i] = src;
+                } else {
+                    if (!staged) {
+                        CK(cudaStreamWaitEvent(ctx->cp, ctx->used[b], 0));
+                        staged = true;
+                    }
+                    // 16-byte aligned frame starts in the staging buffer
+                    soff = (soff + 15) & ~(int64_t)15;
+                    uint8_t* dst = ctx->stage[b].as<uint8_t>() + soff;
+                    CK(cudaMemcpyAsync(dst, src, fb, cudaMemcpyHostToDevice, ctx->cp));
+                    raw[i] = dst;
+                    soff += (int64_t)fb;
+                }
+            }
+            if (staged) {
+                CK(cudaEventRecord(ctx->filled[b], ctx->cp));
+                CK(cudaStreamWaitEvent(ctx->st, ctx->filled[b], 0));
+            }
+            // frame and tile tables (largest tiles first: the persistent
+            // CTAs finish together)
+            htask.clear();
+            int64_t poff = 0;
+            for (int i = 0; i < kRaggedSlots; i++) {
+                RaggedFrame& f = hf[(size_t)i];
+                if (i < (int)wave.size()) {
+                    const int32_t v = wave[(size_t)i].video;
+                    f.raw = raw[(size_t)i];
+                    f.proc_off = poff;
+                    f.H = H_[v];
+                    f.W = W_[v];
+                    f.vec_ok = (W_[v] % 4 == 0 && ((uintptr_t)raw[(size_t)i] % (4 * sizeof(T))) == 0) ? 1 : 0;
+                    f.out_slot = (int32_t)(vslot[(size_t)v] + wave[(size_t)i].t);
+                    poff += (int64_t)H_[v] * W_[v];
+                    for (int32_t r0 = 0; r0 < H_[v]; r0 += shape.seg)
+                        for (int32_t c0 = 0; c0 < W_[v]; c0 += TW)
+                            htask.push_back(StripTask{i, c0, r0, std::min(r0 + shape.seg, H_[v])});
+                } else {
+                    f.raw = nullptr;
+                    f.proc_off = 0;
+                    f.H = f.W = 0;
+                    f.vec_ok = 0;
+                    f.out_slot = (int32_t)NT;   // the spare result slot
+                }
+            }
+            std::stable_sort(htask.begin(), htask.end(), [](const StripTask& a, const StripTask& b2) {
+                return (a.r1 - a.r0) > (b2.r1 - b2.r0);
+            });
+            const int32_t ntask = (int32_t)htask.size();
+            CK(cudaMemcpyAsync(d_frames, hf.data(), hf.size() * sizeof(RaggedFrame), cudaMemcpyHostToDevice, ctx->st));
+            if (ntask > 0)
+                CK(cudaMemcpyAsync(d_tasks, htask.data(), htask.size() * sizeof(StripTask), cudaMemcpyHostToDevice,
+                                   ctx->st));
+            CK(cudaMemcpyAsync(d_ntasks, &ntask, 4, cudaMemcpyHostToDevice, ctx->st));
+            if (shape_i >= 0) CK(cudaEventRecord(e0, ctx->st));
+            {
+                Prof pf(ctx, "ragged_wave");
+                CK(cudaGraphLaunch(ctx->rg_graph, ctx->st));
+            }
+            if (staged) CK(cudaEventRecord(ctx->used[b], ctx->st));
+            if (shape_i >= 0) {
+                CK(cudaEventRecord(e1, ctx->st));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                // the first round of shapes warms up; the second one counts
+                if (shape_i >= kRaggedNShapes) {
+                    shape_ms[(size_t)(shape_i % kRaggedNShapes)] += ms;
+                    shape_px[(size_t)(shape_i % kRaggedNShapes)] += (double)used / 4.0;
+                }
+                shape_i++;
+                if (shape_i == 2 * kRaggedNShapes) {
+                    int best = 0;
+                    for (int k = 1; k < kRaggedNShapes; k++)
+                        if (shape_ms[(size_t)k] / shape_px[(size_t)k] < shape_ms[(size_t)best] / shape_px[(size_t)best])
+                            best = k;
+                    ctx->rg_best[tkey] = {kRaggedShapes[best].seg, kRaggedShapes[best].budget};
+                    shape = kRaggedShapes[best];
+                    shape_i = -1;
+                }
+            }
+            ctx->done = cur;
+            wave_no++;
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        uint32_t fl = 0;
+        CK(cudaMemcpyAsync(&fl, flags, 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (!(fl & (kFlagCandOverflow | kFlagFeatOverflow))) break;
+        if (attempt > 8) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame capacity exceeded");
+        const uint64_t npx = (uint64_t)max_px;
+        if (fl & kFlagCandOverflow) {
+            uint64_t ncap = std::min<uint64_t>((uint64_t)ctx->cand_cap * 4, npx + 1);
+            if (ncap <= ctx->cand_cap) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "candidate capacity exceeded");
+            ctx->cand_cap = (uint32_t)ncap;
+        }
+        if (fl & kFlagFeatOverflow) {
+            uint64_t nf = std::min<uint64_t>((uint64_t)ctx->feat_cap * 4, std::min<uint64_t>(npx + 1, 1u << 24));
+            if (nf <= ctx->feat_cap)
+                return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame detection capacity exceeded");
+            ctx->feat_cap = (uint32_t)nf;
+        }
+    }
+    // ---- per-video tables
+    for (int32_t v = 0; v < nv; v++) {
+        std::vector<int64_t> fnum((size_t)T_[v]);
+        for (int64_t t = 0; t < T_[v]; t++) fnum[(size_t)t] = t;
+        HostSpan hs(ctx, "host_assemble");
+        CKS(assemble_table(ctx, T_[v], fnum, false, tabs[v], row_off[(size_t)v], vslot[(size_t)v]));
+        if (!p.doughnut_correction)
+            tabs[v]->has[GT_COL_RAW_MASS] = tabs[v]->has[GT_COL_RAW_BG_MEDIAN] =
+                tabs[v]->has[GT_COL_RAW_MASS_CORRECTED] = false;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    drain_profile(ctx, false);
+    return GT_OK;
+}
+
+// Many videos in one call: the videos are located together in ragged waves
+// (batch_videos_ragged) where the parameter set allows it, otherwise each
+// into its own table as gt_batch would; then every video is linked in ONE
+// launch of the whole-video linker (one CTA per video), so the videos'
+// sequential frame scans run side by side.  Results equal separate gt_batch
+// calls.
 template <typename T>
 gt_status batch_videos_impl(gt_ctx* ctx, const gt_params& p, int32_t n_videos, const void* const* frames,
                             const int64_t* T_, const int32_t* H_, const int32_t* W_, gt_table** tabs) {
     gt_params pl = p;
     pl.has_search_range = 0;
     std::vector<std::vector<int64_t>> row_off((size_t)n_videos);
+    std::unique_ptr<bool[]> on_dev(new bool[(size_t)std::max(n_videos, 1)]);
     for (int32_t v = 0; v < n_videos; v++) {
-        bool on_device = false;
-        CKS(check_frames_ptr(ctx, frames[v], (size_t)T_[v] * H_[v] * W_[v] * sizeof(T), &on_device));
+        on_dev[(size_t)v] = false;
+        CKS(check_frames_ptr(ctx, frames[v], (size_t)T_[v] * H_[v] * W_[v] * sizeof(T), &on_dev[(size_t)v]));
+    }
+    bool ragged = n_videos > 0 && !ctx->no_ragged;
+    LocateConsts c;
+    if (ragged) {
+        int32_t Hm = 0, Wm = 0;
+        for (int32_t v = 0; v < n_videos; v++) {
+            Hm = std::max(Hm, H_[v]);
+            Wm = std::max(Wm, W_[v]);
+        }
+        CKS(make_locate_consts(ctx, p, Hm, Wm, c));
+        set_fast_div<T>(ctx, c);
+        ragged = ragged_eligible<T>(p, c);
+    }
+    if (ragged) {
+        HostSpan hs(ctx, "host_locate");
+        CKS(batch_videos_ragged<T>(ctx, p, c, n_videos, frames, on_dev.get(), T_, H_, W_, tabs, row_off));
+    }
+    for (int32_t v = 0; v < n_videos && !ragged; v++) {
+        const bool on_device = on_dev[(size_t)v];
         const int64_t NT = T_[v];
         gt_status st = batch_impl<T>(ctx, pl, (const T*)frames[v], on_device, NT, H_[v], W_[v], nullptr, nullptr, 0,
                                      tabs[v]);
@@ -1393,6 +1781,31 @@ GT_API gt_status gt__set_capacities(gt_ctx* ctx, int64_t cand_cap, int64_t feat_
     return GT_OK;
 }
 
+// Test hook: gt_batch_videos locates video by video (ragged = 0) or in
+// ragged waves where the parameters allow (ragged = 1, the default; 2: the
+// autotuner runs on every call, however small).  The tuned wave shapes are
+// forgotten, so the next call tunes again.
+GT_API gt_status gt__set_ragged(gt_ctx* ctx, int32_t ragged) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    ctx->no_ragged = ragged == 0;
+    ctx->rg_force_tune = ragged == 2;
+    ctx->rg_best.clear();
+    return GT_OK;
+}
+
+// Test hook: the wave shape the autotuner chose for the last ragged call
+// (0, 0 when none was tuned).
+GT_API gt_status gt__ragged_shape(const gt_ctx* ctx, int32_t* seg, int64_t* budget) {
+    if (!ctx) return GT_ERR_INVALID_ARGUMENT;
+    *seg = 0;
+    *budget = 0;
+    for (const auto& kv : ctx->rg_best) {
+        *seg = kv.second.first;
+        *budget = kv.second.second;
+    }
+    return GT_OK;
+}
+
 // Test hook: the capacities the last call ended with.
 GT_API gt_status gt__get_capacities(const gt_ctx* ctx, int64_t* cand_cap, int64_t* feat_cap) {
     if (!ctx) return GT_ERR_INVALID_ARGUMENT;
@@ -1488,6 +1901,7 @@ void gt_destroy(gt_ctx* ctx) {
         cudaEventDestroy(ctx->used[i]);
         cudaEventDestroy(ctx->filled[i]);
     }
+    if (ctx->rg_graph) cudaGraphExecDestroy(ctx->rg_graph);
     cudaEventDestroy(ctx->located);
     cudaEventDestroy(ctx->linked);
     cudaStreamDestroy(ctx->st);

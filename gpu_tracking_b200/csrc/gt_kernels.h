@@ -27,13 +27,14 @@ struct FinalizeConsts {
 
 // One frame of a ragged batch (frames of many videos and sizes in one launch
 // per stage): its pixels, where its processed image starts in the batch's
-// buffer, its size, and whether 4-pixel loads of its rows are aligned.
+// buffer, its size, whether 4-pixel loads of its rows are aligned, and the
+// slot of the call's per-frame results (detections, kept count) it fills.
 struct RaggedFrame {
     const void* raw;
     int64_t proc_off;
     int32_t H, W;
     int32_t vec_ok;
-    int32_t pad;
+    int32_t out_slot;
 };
 // One bandpass tile of a ragged batch: frame slot, first output column, rows [r0, r1).
 struct StripTask {
@@ -153,6 +154,9 @@ bool launch_strip_ragged(const RaggedFrame* frames, const StripTask* tasks, cons
 // CTAs of the strip kernel resident per SM for these parameters (0: no specialisation)
 template <typename T>
 int strip_blocks_per_sm(const LocateConsts& c);
+// Output columns of one strip tile for these parameters (0: no specialisation)
+template <typename T>
+int strip_tile_width(const LocateConsts& c);
 template <typename T>
 bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                   uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,

@@ -1145,6 +1145,7 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
     __shared__ int wsum[33];
     const int g = blockIdx.x;
     const int fW = rf ? rf[g].W : fc.W;
+    const int og = rf ? rf[g].out_slot : g;   // result slot (ragged batches: the frame's slot of the call)
     const int n = (int)min(feat_count[g], feat_cap);
     const Feature* F = feats + (size_t)g * feat_cap;
     int np2 = 1;
@@ -1164,7 +1165,7 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
     } else {
         if (need > fc.scratch_per_frame) {
             if (threadIdx.x == 0) atomicOr(flags, kFlagFeatOverflow);
-            if (threadIdx.x == 0) kept_count[g] = 0;
+            if (threadIdx.x == 0) kept_count[og] = 0;
             return;
         }
         uint8_t* base = gscratch + (size_t)g * fc.scratch_per_frame;
@@ -1270,12 +1271,12 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
         int pos = block_excl_scan(k, &tot, wsum);
         if (k) {
             Feature ft = F[perm[order[i]]];
-            out[(size_t)g * feat_cap + total + pos] = ft;
+            out[(size_t)og * feat_cap + total + pos] = ft;
         }
         total += tot;
         __syncthreads();
     }
-    if (threadIdx.x == 0) kept_count[g] = (uint32_t)total;
+    if (threadIdx.x == 0) kept_count[og] = (uint32_t)total;
 }
 
 // Doughnut correction of the kept rows (src/execute_gpu.rs:717-790): one warp
@@ -1291,13 +1292,14 @@ doughnut_kernel(Feature* __restrict__ out, const uint32_t* __restrict__ kept_cou
                 const int4* __restrict__ dn_meta, const RaggedFrame* __restrict__ rf) {
     __shared__ uint32_t hist[kDoughnutWarps * 256];
     const int g = blockIdx.y;
+    const int og = rf ? rf[g].out_slot : g;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int total = (int)kept_count[g];
+    const int total = (int)kept_count[og];
     const T* raw = rf ? (const T*)rf[g].raw : frames + (size_t)frame_index[g] * frame_stride;
     const int H = rf ? rf[g].H : fc.H, W = rf ? rf[g].W : fc.W;
     uint32_t* myhist = hist + wid * 256;
     for (int q = blockIdx.x * kDoughnutWarps + wid; q < total; q += gridDim.x * kDoughnutWarps) {
-        Feature* o = out + (size_t)g * feat_cap + q;
+        Feature* o = out + (size_t)og * feat_cap + q;
         Feature ft = *o;
         const int4 m = dn_meta[fc.log_style ? ft.ridx : 0];
         doughnut_warp<T>(raw, H, W, ft, dn_inds + m.x, m.y, dn_inds + m.z, m.w, myhist);

@@ -147,6 +147,15 @@ struct gt_ctx {
     int32_t illum_rint = 0;
     DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
         w_cnt, w_flags, w_vgrp, w_reset;
+    // ragged batches (gt_batch_videos): frame / task tables of the current
+    // wave, the captured stage graph (valid while the buffers it names stay
+    // where they are: rg_graph_key) and the tuned wave shape per workload
+    DBuf rg_frames, rg_tasks, rg_ntasks;
+    cudaGraphExec_t rg_graph = nullptr;
+    std::string rg_graph_key;
+    std::map<std::string, std::pair<int32_t, int64_t>> rg_best;
+    bool no_ragged = false;   // test hook: gt_batch_videos locates video by video
+    bool rg_force_tune = false;   // test hook: tune on every ragged call
     int64_t w_list_cap = 0;   // entries of each window neighbour-list buffer (0 = not sized yet)
     int64_t w_edge_cap = 0;   // backward edges per frame the window scratch holds
     uint32_t cand_cap = 16384;

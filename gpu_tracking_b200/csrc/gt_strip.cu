@@ -580,11 +580,23 @@ int strip_blocks_per_sm(const LocateConsts& c) {
     return 0;
 }
 
+template <typename T>
+int strip_tile_width(const LocateConsts& c) {
+    constexpr bool kInt = IsIntPix<T>::value;
+    if (kInt && !c.fast_div) return 0;
+#define GT_STRIP_TRY(RR, KK)                                                                                  \
+    if (c.R == RR && c.kd == KK) return kStripTW;
+    GT_STRIP_CASES(GT_STRIP_TRY)
+#undef GT_STRIP_TRY
+    return 0;
+}
+
 #define GT_STRIP_RAGGED_INST(T)                                                                                  \
     template bool launch_strip_ragged<T>(const RaggedFrame*, const StripTask*, const int32_t*, int, float*,      \
                                          const LocateConsts&, uint32_t*, uint32_t*, uint32_t, uint32_t*,         \
                                          cudaStream_t, cudaError_t*);                                            \
-    template int strip_blocks_per_sm<T>(const LocateConsts&);
+    template int strip_blocks_per_sm<T>(const LocateConsts&);                                                    \
+    template int strip_tile_width<T>(const LocateConsts&);
 GT_STRIP_RAGGED_INST(uint16_t)
 GT_STRIP_RAGGED_INST(float)
 GT_STRIP_RAGGED_INST(uint8_t)
