@@ -299,8 +299,8 @@ def run_ragged(args):
     ctx.profile(True)
     together()
     parts = {}
-    for name in ("ragged_wave", "scatter", "link_sort", "link_lists", "link_video", "link_durations", "round_ids",
-                 "host_locate", "host_assemble", "host_link"):
+    for name in ("bandpass_localmax", "walk_characterize", "finalize", "scatter", "link_sort", "link_lists",
+                 "link_video", "link_durations", "round_ids", "host_locate", "host_assemble", "host_link"):
         k, kms = ctx.profile_read(name)
         if k:
             parts[name] = {"count": k, "ms": kms}
@@ -567,14 +567,18 @@ def run_log(args):
     # one at the sampled SM clock: 148 SMs x 128 FP32 lanes x 2 flops
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    lap = kernels.get("laplace") or kernels.get("log_scale_space")
+    fused = "log_scale_space" in kernels
+    lap = kernels.get("log_scale_space") or kernels.get("laplace")
     roofline = None
     if lap:
         achieved = flops_per_frame * frames / (lap[1] / 1000.0) / 1e12
+        tr = load_traffic().get("log_scale_space", {}) if fused else {}
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "kernel": "laplace (+ logspace_max)",
+                    "frac": achieved / fp32_peak,
+                    "kernel": "log_scale_space (all radii and the 3-D maximum)" if fused else "laplace",
                     "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x 2 flops at the sampled SM clock",
-                    "flops_per_frame": flops_per_frame, "taps_per_pixel": taps, "traffic": None}
+                    "flops_per_frame": flops_per_frame, "taps_per_pixel": taps,
+                    "traffic": tr.get("dram_bytes_per_frame"), "traffic_source": tr.get("source")}
     hbm_peak, hbm_kind = load_peaks()
     total_k = sum(v[1] for v in kernels.values()) or 1.0
     line = {"metric": "frames/s, multi-scale LoG 1024x1024 float32 (10 radii), detect+characterize+link",
@@ -663,6 +667,8 @@ def main():
     barrier()
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launch_count() - l0
+    # local-maximum candidates the walk started from in the last call (noise maxima included)
+    cands_per_frame = L.gt_last_walk_starts(ctx.handle) / float(T)
     kernels = {}
     for name in ("bandpass_localmax", "walk_characterize", "finalize", "scatter", "link_sort", "link_lists",
                  "link_video", "link_rows", "link_durations", "round_ids"):
@@ -776,6 +782,7 @@ def main():
                 "config": dict(CONFIG, frames=T, height=S, width=S,
                                parallelism="dp%d (one video per rank)" % world),
                 "features_per_s": feats_per_s, "features_per_frame": feats_per_frame,
+                "candidates_per_frame": cands_per_frame,
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "issue_roofline": issue_roofline,
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))

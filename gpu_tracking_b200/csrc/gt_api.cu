@@ -1390,15 +1390,23 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
         float* proc = ctx->processed.as<float>();
         uint32_t* flags = ctx->flags.as<uint32_t>();
 
-        // ---- the stage sequence of one wave (captured once, then replayed)
-        auto stages = [&](cudaStream_t st) -> gt_status {
+        // ---- the stage sequence of one wave (captured once, then replayed;
+        // a profiled call launches it directly, timing every stage)
+        auto stages = [&](cudaStream_t st, bool timed) -> gt_status {
+            std::unique_ptr<Prof> pf;
+            auto stage = [&](const char* name) {
+                pf.reset();
+                if (timed) pf.reset(new Prof(ctx, name, st));
+            };
             CK(cudaMemsetAsync(ctx->cand_count.p, 0, (size_t)kRaggedSlots * 4, st));
             CK(cudaMemsetAsync(ctx->feat_count.p, 0, (size_t)kRaggedSlots * 4, st));
             cudaError_t e = cudaSuccess;
+            stage("bandpass_localmax");
             if (!launch_strip_ragged<T>(d_frames, d_tasks, d_ntasks, grid, proc, c, ctx->cand_count.as<uint32_t>(),
                                         ctx->cand_keys.as<uint32_t>(), cand_cap, flags, st, &e))
                 return set_err(ctx, GT_ERR_INTERNAL, "no strip kernel for this parameter set");
             CK(e);
+            stage("walk_characterize");
             sum_counts_kernel<<<1, 256, 0, st>>>(ctx->cand_count.as<uint32_t>(), kRaggedSlots, cand_cap,
                                                  ctx->walk_starts.as<unsigned long long>());
             CK(cudaGetLastError());
@@ -1406,6 +1414,7 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
                               ctx->cand_keys.as<uint32_t>(), cand_cap, cand_cap, nullptr, ctx->tabs_i.as<int32_t>(),
                               ctx->tabs_f.as<float2>(), ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(),
                               feat_cap, flags, st, d_frames));
+            stage("finalize");
             CK(launch_finalize<T>(ctx->feats_raw.as<Feature>(), ctx->feat_count.as<uint32_t>(), feat_cap,
                                   ctx->feats_out.as<Feature>(), ctx->kept_count.as<uint32_t>(),
                                   ctx->fin_scratch.as<uint8_t>(), fc, (const T*)nullptr, 0, ctx->ident.as<int32_t>(),
@@ -1430,7 +1439,7 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
         if (!ctx->rg_graph) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
-            gt_status sst = stages(ctx->st);
+            gt_status sst = stages(ctx->st, false);
             cudaError_t ee = cudaStreamEndCapture(ctx->st, &g);
             if (sst != GT_OK) {
                 if (g) cudaGraphDestroy(g);
@@ -1453,7 +1462,7 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
         int64_t tot_px = 0;
         for (int32_t v = 0; v < nv; v++) tot_px += T_[v] * (int64_t)H_[v] * W_[v];
         const bool tune = tuned == ctx->rg_best.end() &&
-                          (ctx->rg_force_tune || tot_px * 4 >= 8 * kRaggedNShapes * (1LL << 30));
+                          (ctx->rg_force_tune || tot_px * 4 >= 2 * kRaggedNShapes * (1LL << 30));
         if (tune) shape_i = 0;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (tune) {
@@ -1554,8 +1563,11 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
                                    ctx->st));
             CK(cudaMemcpyAsync(d_ntasks, &ntask, 4, cudaMemcpyHostToDevice, ctx->st));
             if (shape_i >= 0) CK(cudaEventRecord(e0, ctx->st));
-            {
-                Prof pf(ctx, "ragged_wave");
+            if (ctx->profile) {
+                CKS(stages(ctx->st, true));
+            } else {
+                // the graph's kernels: strip, candidate totals, walk, finalize (+ doughnut)
+                ctx->launch_count["ragged_wave"] += fc.doughnut ? 5 : 4;
                 CK(cudaGraphLaunch(ctx->rg_graph, ctx->st));
             }
             if (staged) CK(cudaEventRecord(ctx->used[b], ctx->st));

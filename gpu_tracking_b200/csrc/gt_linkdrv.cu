@@ -16,6 +16,19 @@ using namespace gt::rt;
 namespace gt {
 namespace rt {
 
+// pgroup[i] = g for the points i of group g (goff: group offsets)
+__global__ void fill_pgroup_kernel(const int64_t* __restrict__ goff, int ngroups, int32_t* __restrict__ pgroup) {
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x)
+        for (int64_t i = goff[g] + threadIdx.x; i < goff[g + 1]; i += blockDim.x) pgroup[i] = g;
+}
+
+// out[g] = boff[goff[g] * K], g = 0..ngroups: where each group's backward lists start
+__global__ void group_list_starts_kernel(const int64_t* __restrict__ boff, const int64_t* __restrict__ goff, int K,
+                                         int ngroups, int64_t* __restrict__ out) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g <= ngroups) out[g] = boff[goff[g] * K];
+}
+
 // Runs the linker over px/py (device, npoints) and writes ids (device) and,
 // when row_dur is given, per-row durations and f32-rounded particle ids.
 gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float* py, int64_t* ids_out,
@@ -27,11 +40,13 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     std::unique_ptr<HostSpan> hs(new HostSpan(ctx, "host_link_prep"));
     int max_group = 0;
     for (int g = 0; g < ngroups; g++) max_group = std::max<int64_t>(max_group, job.goff[g + 1] - job.goff[g]);
-    std::vector<int32_t> pgroup(N);
-    for (int g = 0; g < ngroups; g++)
-        for (int64_t i = job.goff[g]; i < job.goff[g + 1]; i++) pgroup[i] = g;
     CKS(upload(ctx, ctx->l_goff, job.goff));
-    CKS(upload(ctx, ctx->l_pgroup, pgroup));
+    CK(ctx->l_pgroup.ensure((size_t)std::max<int64_t>(N, 1) * 4));
+    if (N > 0 && ngroups > 0) {
+        fill_pgroup_kernel<<<std::min(ngroups, 4 * ctx->num_sms), 256, 0, ctx->st>>>(
+            ctx->l_goff.as<int64_t>(), ngroups, ctx->l_pgroup.as<int32_t>());
+        CK(cudaGetLastError());
+    }
     CKS(upload(ctx, ctx->l_vgrp, job.vgrp));
     CKS(upload(ctx, ctx->l_reset, job.reset));
     LinkInput in;
@@ -82,11 +97,12 @@ gt_status run_link(gt_ctx* ctx, const LinkJob& job, const float* px, const float
     CK(cudaMemcpyAsync(&ftot, ctx->l_foff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&btot, ctx->l_boff.as<int64_t>() + NK, 8, cudaMemcpyDeviceToHost, ctx->st));
     // per-group backward-edge totals bound the per-frame edge list
-    std::vector<int64_t> gb(ngroups + 1);
     std::vector<int64_t> boff_at(ngroups + 1);
-    for (int g = 0; g <= ngroups; g++)
-        CK(cudaMemcpyAsync(&boff_at[g], ctx->l_boff.as<int64_t>() + job.goff[g] * K, 8, cudaMemcpyDeviceToHost,
-                           ctx->st));
+    CK(ctx->l_ge.ensure((size_t)(ngroups + 1) * 8));
+    group_list_starts_kernel<<<(ngroups + 256) / 256, 256, 0, ctx->st>>>(
+        ctx->l_boff.as<int64_t>(), ctx->l_goff.as<int64_t>(), K, ngroups, ctx->l_ge.as<int64_t>());
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(boff_at.data(), ctx->l_ge.p, (size_t)(ngroups + 1) * 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     hs.reset(new HostSpan(ctx, "host_link_run"));
     int64_t max_edges = 1;

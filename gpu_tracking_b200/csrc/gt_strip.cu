@@ -10,8 +10,9 @@
 //   C  column pass: each thread makes the step's 8 rows of one column;
 //   D  vertical dilation maximum, 8 rows of one column per thread;
 //   E  horizontal dilation maximum, the candidate test and the store of the
-//      segment's processed rows, 4 columns per thread, slots reserved once
-//      per warp.
+//      segment's processed rows, 4 columns per thread; candidates gather in a
+//      shared-memory buffer of the tile (one shared atomic per warp) and go
+//      to the frame's list with one global reservation per tile.
 // The row-pass rows and the processed rows live in ring buffers that hold
 // every row twice (at r and r + ring), so any window of consecutive rows is
 // contiguous and every read in the tap loops is a constant offset from one
@@ -37,6 +38,7 @@ namespace gt {
 constexpr int kStripTW = 128;
 constexpr int kStripThreads = 288;
 constexpr int kStepRows = 8;
+constexpr int kCandBuf = 768;   // candidate keys a tile buffers in shared memory
 
 template <int R, int KD>
 struct StripGeom {
@@ -60,7 +62,7 @@ struct StripGeom {
     static constexpr int RAWPT = (RAWN + kStripThreads - 1) / kStripThreads;
     // the vertical maxima (stages D-E) reuse the staged raw rows (stages A-B)
     static constexpr size_t smem_floats = (size_t)kStepRows * RWp + 2 * (size_t)(2 * XR) * PWp +
-                                          (size_t)(2 * PR) * PWp;
+                                          (size_t)(2 * PR) * PWp + 4 + kCandBuf;
     static constexpr int min_blocks = (smem_floats * 4 + 1024) * 3 <= 227 * 1024 ? 3 : 2;
     static_assert(RWp % 4 == 0 && RWp >= PWp + 2 * R, "staged raw row");
     static_assert(RWp >= PWp, "vertical maxima fit in the staging rows");
@@ -154,6 +156,8 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
     float* xb = xg + 2 * XR * PWp;              // [2XR][PWp]    row pass boxcar
     float* pr = xb + 2 * XR * PWp;              // [2PR][PWp]    processed rows, stored twice
     float* vb = stage;                          // [8][PWp]      vertical maxima (pc0-relative columns)
+    uint32_t* cbuf_n = (uint32_t*)(pr + 2 * PR * PWp);   // [4]   buffered candidates, flush base
+    uint32_t* cbuf = cbuf_n + 4;                // [kCandBuf]    candidate keys of the tile
 
     const int x0 = R0 - O - R;          // first raw / row-pass row
     const int pc0 = c0 - O;             // first processed column of the strip's dilation windows
@@ -197,6 +201,7 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
             }
         }
     };
+    if (tid == 0) *cbuf_n = 0;
     load_raw(0);
     // The first column-pass groups read row-pass rows above x0 that no step
     // writes.  The outputs that need them are never used, but the sliding
@@ -439,20 +444,46 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
                 if (lane >= dd) incl += v;
             }
             const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+            // slots in the tile's shared candidate buffer (one shared
+            // atomic per warp); a full buffer sends the warp's candidates
+            // straight to the frame's list
             uint32_t base = 0;
-            if (wtot > 0) {
-                if (lane == 31) base = atomicAdd(cand_slot, (uint32_t)wtot);
-                base = __shfl_sync(0xffffffffu, base, 31);
-            }
+            if (lane == 31) base = atomicAdd(cbuf_n, (uint32_t)wtot);
+            base = __shfl_sync(0xffffffffu, base, 31);
             uint32_t pos = base + (uint32_t)(incl - cnt);
+            if (base + (uint32_t)wtot <= (uint32_t)kCandBuf) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                if (!(cmask & (1u << k))) continue;
-                if (pos < cand_cap) cout[pos] = (uint32_t)cd * (uint32_t)W + (uint32_t)(ccol + k);
-                else atomicOr(flags, kFlagCandOverflow);
-                pos++;
+                for (int k = 0; k < 4; k++) {
+                    if (!(cmask & (1u << k))) continue;
+                    cbuf[pos++] = (uint32_t)cd * (uint32_t)W + (uint32_t)(ccol + k);
+                }
+            } else {
+                uint32_t gb = 0;
+                if (lane == 31) gb = atomicAdd(cand_slot, (uint32_t)wtot);
+                gb = __shfl_sync(0xffffffffu, gb, 31);
+                pos = gb + (uint32_t)(incl - cnt);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (!(cmask & (1u << k))) continue;
+                    if (pos < cand_cap) cout[pos] = (uint32_t)cd * (uint32_t)W + (uint32_t)(ccol + k);
+                    else atomicOr(flags, kFlagCandOverflow);
+                    pos++;
+                }
             }
             }
+        }
+        __syncthreads();
+    }
+    // the tile's buffered candidates go to the frame's list in one reservation
+    __syncthreads();
+    {
+        const uint32_t n = min(*cbuf_n, (uint32_t)kCandBuf);
+        if (tid == 0) cbuf_n[1] = n ? atomicAdd(cand_slot, n) : 0u;
+        __syncthreads();
+        const uint32_t gb = cbuf_n[1];
+        for (uint32_t i = tid; i < n; i += kStripThreads) {
+            if (gb + i < cand_cap) cout[gb + i] = cbuf[i];
+            else atomicOr(flags, kFlagCandOverflow);
         }
         __syncthreads();
     }
