@@ -1046,6 +1046,25 @@ __device__ float warp_upper_median(const T* __restrict__ raw, int H, int W, int 
 // bit from the top, counting keys below each trial value with one warp
 // reduction; bits that every valid key shares are taken as they are.
 constexpr int kMedianRegs = 13;
+// Median keys: the orderable bits of a float pixel, or an integer pixel's
+// own value (the same order, in the fewest bits: the bit-by-bit search only
+// visits the bits in which the annulus' values differ).
+template <typename T>
+struct MedKey {
+    __device__ static uint32_t key(const T* raw, size_t i) { return float_order_key(load_px<T>(raw, i)); }
+    __device__ static float value(uint32_t k) { return float_from_order_key(k); }
+};
+template <>
+struct MedKey<uint16_t> {
+    __device__ static uint32_t key(const uint16_t* raw, size_t i) { return (uint32_t)__ldg(raw + i); }
+    __device__ static float value(uint32_t k) { return (float)k; }
+};
+template <>
+struct MedKey<uint8_t> {
+    __device__ static uint32_t key(const uint8_t* raw, size_t i) { return (uint32_t)__ldg(raw + i); }
+    __device__ static float value(uint32_t k) { return (float)k; }
+};
+
 template <typename T>
 __device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ raw, int H, int W, int mu, int mv,
                                         const short2* __restrict__ inds, int n_inds, int* n_out) {
@@ -1061,7 +1080,7 @@ __device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ ra
             const short2 d = inds[k];
             const int64_t a = (int64_t)mu + d.x, b = (int64_t)mv + d.y;
             if (a >= 0 && a < H && b >= 0 && b < W) {
-                key[q] = float_order_key(load_px<T>(raw, (size_t)a * W + b));
+                key[q] = MedKey<T>::key(raw, (size_t)a * W + b);
                 kor |= key[q];
                 kand &= key[q];
                 nv++;
@@ -1079,7 +1098,7 @@ __device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ ra
         kand &= __shfl_xor_sync(0xffffffffu, kand, o);
     }
     const uint32_t diff = kor ^ kand;
-    if (diff == 0u) return float_from_order_key(kand);
+    if (diff == 0u) return MedKey<T>::value(kand);
     const uint32_t want = (uint32_t)(nvalid / 2);
     const int hb = 31 - __clz(diff), lb = __ffs(diff) - 1;
     uint32_t prefix = kand & ~((2u << hb) - 1u);      // bits above hb: common to all keys
@@ -1094,7 +1113,7 @@ __device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ ra
         if ((uint32_t)c <= want) prefix = trial;
     }
     prefix |= kand & ((1u << lb) - 1u);                 // bits below lb: common to all keys
-    return float_from_order_key(prefix);
+    return MedKey<T>::value(prefix);
 }
 
 // Doughnut correction of one feature by one warp (src/execute_gpu.rs:717-790).
@@ -1104,9 +1123,26 @@ __device__ __forceinline__ void doughnut_warp(const T* __restrict__ raw, int H, 
     const int lane = threadIdx.x & 31;
     const int mu = sat_f2i(roundf(ft.x));
     const int mv = sat_f2i(roundf(ft.y));
-    // sequential sum in circle_inds order (Iterator::sum)
+    // sequential sum in circle_inds order (Iterator::sum); integer pixels
+    // make every partial sum an exact integer below 2^24, so a warp
+    // reduction gives the same value
     float sum = 0.0f;
     int nsig = 0;
+    if (!std::is_same<T, float>::value && n_sig <= 256) {
+        uint32_t acc = 0;
+        for (int b = 0; b < n_sig; b += 32) {
+            const int k = b + lane;
+            bool ok = false;
+            if (k < n_sig) {
+                const short2 d = sig[k];
+                const int64_t a = (int64_t)mu + d.x, bb = (int64_t)mv + d.y;
+                ok = (a >= 0 && a < H && bb >= 0 && bb < W);
+                if (ok) acc += (uint32_t)load_px<T>(raw, (size_t)a * W + bb);
+            }
+            nsig += __popc(__ballot_sync(0xffffffffu, ok));
+        }
+        sum = (float)__reduce_add_sync(0xffffffffu, acc);
+    } else
     for (int b = 0; b < n_sig; b += 32) {
         int k = b + lane;
         float val = 0.0f;
