@@ -110,6 +110,8 @@ def lib():
         L.gt_video_info.restype = i32
         L.gt_video_read.argtypes = [vp, P(i64), i64, i32, vp]
         L.gt_video_read.restype = i32
+        L.gt_video_read_device.argtypes = [vp, vp, P(i64), i64, i32, vp]
+        L.gt_video_read_device.restype = i32
         L.gt_video_close.argtypes = [vp]
         L.gt_video_last_error.restype = ctypes.c_char_p
         L.gt_last_walk_starts.argtypes = [vp]

@@ -44,8 +44,9 @@ class _Frames:
         self.frame_numbers = None
         if isinstance(obj, (str, os.PathLike)):
             if os.path.splitext(os.fspath(obj))[1].lower() in _VIDEO_EXT:
-                # decoded in the file's own dtype (u8/u16 stay integers)
-                obj = _read_video(obj, frames, channel)
+                # decoded in the file's own dtype (u8/u16 stay integers),
+                # on the GPU straight into device memory where one is usable
+                obj = _read_video(obj, frames, channel, device=_gpu_decode())
                 if frames is not None:
                     self.frame_numbers = np.asarray([int(k) for k in frames], np.int64)
                     frames = None
@@ -351,9 +352,22 @@ def connect(to_link1, to_link2, search_range, merge=True):
 _VIDEO_EXT = (".tif", ".tiff", ".ets", ".vsi")
 
 
-def _read_video(path, frames=None, channel=None, as_float=False):
-    """Decode a .tif/.tiff/.ets/.vsi video with the engine's frame providers
-    (host-side); (T, Y, X) in the file's dtype, or float32."""
+def _gpu_decode():
+    """Video files decode on the GPU unless GT_DECODE=host or no CUDA device
+    is usable from torch."""
+    if os.environ.get("GT_DECODE", "device") == "host":
+        return False
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except ImportError:
+        return False
+
+
+def _read_video(path, frames=None, channel=None, as_float=False, device=False):
+    """Decode a .tif/.tiff/.ets/.vsi video with the engine's frame providers;
+    (T, Y, X) in the file's dtype, or float32: a numpy array decoded on the
+    host, or (device=True) a CUDA tensor decoded on the GPU."""
     L = _ffi.lib()
     h = ctypes.c_void_p()
     st = L.gt_video_open(os.fsencode(os.fspath(path)), int(channel or 0), ctypes.byref(h))
@@ -365,6 +379,18 @@ def _read_video(path, frames=None, channel=None, as_float=False):
         keys = None if frames is None else np.ascontiguousarray([int(k) for k in frames], np.int64)
         n = T.value if keys is None else len(keys)
         code = DTYPE_F32 if as_float else dt.value
+        if device:
+            import torch
+            ctx = _ffi.context(_DEVICE)
+            t_dtype = {DTYPE_U16: torch.uint16, DTYPE_U8: torch.uint8, DTYPE_F32: torch.float32}[code]
+            out = torch.empty((n, H.value, W.value), dtype=t_dtype, device="cuda:%d" % _DEVICE)
+            torch.cuda.current_stream(out.device).synchronize()
+            st = L.gt_video_read_device(ctx.handle, h,
+                                        keys.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)) if keys is not None
+                                        else None, n, code, ctypes.c_void_p(out.data_ptr()))
+            if st != _ffi.GT_OK:
+                raise _ffi.to_exception(st, L.gt_video_last_error().decode())
+            return out
         np_dtype = {DTYPE_U16: np.uint16, DTYPE_U8: np.uint8, DTYPE_F32: np.float32}[code]
         out = np.empty((n, H.value, W.value), np_dtype)
         st = L.gt_video_read(h, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)) if keys is not None else None,

@@ -143,6 +143,7 @@ struct gt_ctx {
     DBuf illum_taps, illum_shared, illum_prof, illum_corr;  // illumination correction
     DBuf cnn_x, cnn_p, cnn_q, cnn_head;   // learned proposals: network input, activations, outputs
     DBuf walk_starts;                     // walk starts of the current call (u64)
+    DBuf vd_src, vd_dec, vd_blk, vd_bad;  // video files decoded on the device: streams, bytes, blocks, flag
     int64_t last_walk_starts = 0;
     int32_t illum_rint = 0;
     DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,

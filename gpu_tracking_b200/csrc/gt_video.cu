@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "gpu_tracking_b200.h"
+#include "gt_runtime.cuh"
 
 namespace {
 
@@ -472,6 +473,330 @@ std::string lower_ext(const std::string& p) {
 
 }  // namespace
 
+// ---- decoding on the GPU
+// The compressed strips or tiles of the requested frames are read from the
+// file on the host (only I/O), copied to the device in one piece and decoded
+// there: one CTA per strip or tile runs its LZW or PackBits stream on one
+// thread (both formats are sequential by construction) with the LZW
+// dictionary in shared memory, then the CTA undoes horizontal differencing
+// row by row and converts the samples into the output frames.  Deflate
+// blocks are inflated on the host (zlib) and travel as uncompressed ones.
+// The byte sequences, and so the samples, are those of the host decoder.
+namespace {
+
+enum BlockComp : uint32_t { kCompNone = 0, kCompPackBits = 1, kCompLzw = 2 };
+
+struct DecodeBlock {
+    uint64_t src;       // byte offset of the block's stream in the uploaded buffer
+    uint64_t dec;       // byte offset of its decoded bytes in the decode buffer
+    uint32_t src_len;   // stream bytes
+    uint32_t want;      // decoded bytes the block must yield (rows x bw x sample bytes)
+    uint32_t comp;      // BlockComp
+    int32_t frame;      // output frame (position in the requested list)
+    int32_t by, bx;     // first row / column of the block in the frame
+    int32_t rows, bw;   // rows and samples per row of the block
+    int32_t pred;       // TIFF predictor (2: horizontal differencing)
+    int32_t pad;
+};
+
+constexpr int kLzwCodes = 4096;
+constexpr int kDecodeThreads = 128;
+
+// TIFF 6.0 section 13 (LZW).  Every dictionary entry's string occurs in the
+// output already written: an entry made after code c is the previous code's
+// string followed by the first byte of c's string, which the output holds
+// contiguously where the previous code was emitted.  So an entry is an
+// (offset, length) pair and emitting a code copies bytes the block already
+// decoded.  Same codes, same widening rule and same outputs as the host
+// decoder; false on a malformed stream or a short result.
+__device__ bool lzw_decode_block(const uint8_t* __restrict__ in, uint32_t in_len, uint8_t* __restrict__ out,
+                                 uint32_t want, uint32_t* __restrict__ eoff, uint16_t* __restrict__ elen) {
+    int next = 258, width = 9, prev = -1;
+    uint32_t pos = 0, prev_pos = 0, prev_len = 0;
+    uint64_t bitpos = 0;
+    const uint64_t nbits = (uint64_t)in_len * 8;
+    while (bitpos + width <= nbits && pos < want) {
+        uint32_t code = 0;
+        for (int b = 0; b < width; b++, bitpos++)
+            code = (code << 1) | ((in[bitpos >> 3] >> (7 - (bitpos & 7))) & 1u);
+        if (code == 257) break;
+        if (code == 256) {
+            next = 258;
+            width = 9;
+            prev = -1;
+            continue;
+        }
+        uint32_t len;
+        const bool after_clear = prev < 0;
+        if (after_clear) {
+            if (code > 255) return false;
+            out[pos] = (uint8_t)code;
+            len = 1;
+        } else if ((int)code < next) {
+            if (code < 256) {
+                out[pos] = (uint8_t)code;
+                len = 1;
+            } else {
+                const uint32_t o = eoff[code];
+                len = elen[code];
+                for (uint32_t k = 0; k < len && pos + k < want; k++) out[pos + k] = out[o + k];
+            }
+            if (next < kLzwCodes) {
+                eoff[next] = prev_pos;
+                elen[next] = (uint16_t)(prev_len + 1);
+                next++;
+            }
+        } else if ((int)code == next && next < kLzwCodes) {
+            // the previous string and its own first byte
+            len = prev_len + 1;
+            for (uint32_t k = 0; k < prev_len && pos + k < want; k++) out[pos + k] = out[prev_pos + k];
+            if (pos + prev_len < want) out[pos + prev_len] = out[prev_pos];
+            eoff[next] = prev_pos;
+            elen[next] = (uint16_t)len;
+            next++;
+        } else {
+            return false;
+        }
+        prev = (int)code;
+        prev_pos = pos;
+        prev_len = len;
+        pos += len;
+        // TIFF's LZW widens the code one entry early (not after a clear code's first code)
+        if (!after_clear && next + 1 >= (1 << width) && width < 12) width++;
+    }
+    return pos >= want;
+}
+
+
+// TIFF 6.0 section 9 (PackBits), as the host decoder: whole runs, the result
+// at least `want` bytes (bytes past it are not stored).
+__device__ bool packbits_decode_block(const uint8_t* __restrict__ in, uint32_t in_len, uint8_t* __restrict__ out,
+                                      uint32_t want) {
+    uint32_t i = 0, pos = 0;
+    while (i < in_len && pos < want) {
+        const int n = (int)(int8_t)in[i++];
+        if (n >= 0) {
+            const uint32_t len = (uint32_t)n + 1;
+            if (i + len > in_len) return false;
+            for (uint32_t k = 0; k < len && pos + k < want; k++) out[pos + k] = in[i + k];
+            i += len;
+            pos += len;
+        } else if (n != -128) {
+            if (i >= in_len) return false;
+            const uint32_t len = (uint32_t)(1 - n);
+            const uint8_t byte = in[i++];
+            for (uint32_t k = 0; k < len && pos + k < want; k++) out[pos + k] = byte;
+            pos += len;
+        }
+    }
+    return pos >= want;
+}
+
+// One sample of a decoded block (file byte order) as the output type (the
+// host decoder's sample_as).
+template <typename O>
+__device__ __forceinline__ O sample_dev(const uint8_t* p, int code, bool be) {
+    switch (code) {
+        case 1: return (O)p[0];
+        case 3: return (O)(float)(int8_t)p[0];
+        case 2: return (O)(uint16_t)(be ? (p[0] << 8) | p[1] : p[0] | (p[1] << 8));
+        case 4: return (O)(float)(int16_t)(be ? (p[0] << 8) | p[1] : p[0] | (p[1] << 8));
+        default: {
+            const uint32_t u = be ? ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3]
+                                  : (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
+                                        ((uint32_t)p[3] << 24);
+            return (O)__uint_as_float(u);
+        }
+    }
+}
+
+// One CTA per block: decode (thread 0), undo horizontal differencing (a
+// thread per row, the host decoder's sample arithmetic), store the samples
+// into the block's place in its output frame.
+template <typename O>
+__global__ void __launch_bounds__(kDecodeThreads)
+decode_blocks_kernel(const uint8_t* __restrict__ src, const DecodeBlock* __restrict__ blocks, uint8_t* __restrict__ dec,
+                     O* __restrict__ dst, int32_t H, int32_t W, int code, int be, uint32_t* __restrict__ bad) {
+    __shared__ uint32_t eoff[kLzwCodes];
+    __shared__ uint16_t elen[kLzwCodes];
+    const DecodeBlock b = blocks[blockIdx.x];
+    const uint8_t* in = src + b.src;
+    uint8_t* out = dec + b.dec;
+    const int tid = threadIdx.x;
+    if (b.comp == kCompNone) {
+        for (uint32_t i = tid; i < b.want; i += blockDim.x) out[i] = in[i];
+    } else if (tid == 0) {
+        const bool ok = b.comp == kCompLzw ? lzw_decode_block(in, b.src_len, out, b.want, eoff, elen)
+                                           : packbits_decode_block(in, b.src_len, out, b.want);
+        if (!ok) atomicExch(bad, 1u);
+    }
+    __syncthreads();
+    const int bs = (code == 1 || code == 3) ? 1 : (code == 5 ? 4 : 2);
+    if (b.pred == 2) {
+        // TIFF 6.0 section 14: running sums along each row, modulo the sample width
+        for (int r = tid; r < b.rows; r += blockDim.x) {
+            uint8_t* row = out + (size_t)r * b.bw * bs;
+            if (bs == 1) {
+                for (int c = 1; c < b.bw; c++) row[c] = (uint8_t)(row[c] + row[c - 1]);
+            } else {
+                uint32_t prev = be ? ((row[0] << 8) | row[1]) : (row[0] | (row[1] << 8));
+                for (int c = 1; c < b.bw; c++) {
+                    uint8_t* q = row + 2 * c;
+                    const uint32_t cur = be ? ((q[0] << 8) | q[1]) : (q[0] | (q[1] << 8));
+                    const uint32_t x = (cur + prev) & 0xFFFFu;
+                    if (be) {
+                        q[0] = (uint8_t)(x >> 8);
+                        q[1] = (uint8_t)x;
+                    } else {
+                        q[0] = (uint8_t)x;
+                        q[1] = (uint8_t)(x >> 8);
+                    }
+                    prev = x;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const int64_t n = (int64_t)b.rows * b.bw;
+    O* frame = dst + (size_t)b.frame * H * W;
+    for (int64_t i = tid; i < n; i += blockDim.x) {
+        const int y = (int)(i / b.bw), x = (int)(i - (int64_t)y * b.bw);
+        if (b.by + y < H && b.bx + x < W)
+            frame[(size_t)(b.by + y) * W + b.bx + x] = sample_dev<O>(out + (size_t)i * bs, code, be != 0);
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// Reads the streams of the requested frames (host I/O; Deflate inflated on
+// the host) and decodes them on the context's device into d_dst, in batches
+// of about kDecodeBatchBytes of streams.
+constexpr size_t kDecodeBatchBytes = 256u << 20;
+
+template <typename O>
+gt_status read_frames_device(gt_video* v, gt_ctx* ctx, const int64_t* keys, int64_t n, O* d_dst) {
+    using gt::rt::DBuf;
+    const int64_t T = v->kind == Kind::Tiff ? (int64_t)v->images.size() : (int64_t)v->ets_frames.size();
+    const int code = v->src_type;
+    const size_t bs = bytes_of(code);
+    std::vector<uint8_t> hsrc, raw, dec;
+    std::vector<DecodeBlock> blocks;
+    uint64_t dec_bytes = 0;
+    auto flush = [&]() -> gt_status {
+        if (blocks.empty()) return GT_OK;
+        auto cuda_err = [](cudaError_t e) { return verr(GT_ERR_CUDA, std::string("CUDA error ") + cudaGetErrorString(e)); };
+        cudaError_t e;
+        if ((e = ctx->vd_src.ensure(std::max<size_t>(hsrc.size(), 16))) != cudaSuccess) return cuda_err(e);
+        if ((e = ctx->vd_dec.ensure(std::max<uint64_t>(dec_bytes, 16))) != cudaSuccess) return cuda_err(e);
+        if ((e = ctx->vd_blk.ensure(blocks.size() * sizeof(DecodeBlock))) != cudaSuccess) return cuda_err(e);
+        if ((e = ctx->vd_bad.ensure(4)) != cudaSuccess) return cuda_err(e);
+        if ((e = cudaMemsetAsync(ctx->vd_bad.p, 0, 4, ctx->st)) != cudaSuccess) return cuda_err(e);
+        if (!hsrc.empty() &&
+            (e = cudaMemcpyAsync(ctx->vd_src.p, hsrc.data(), hsrc.size(), cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess)
+            return cuda_err(e);
+        if ((e = cudaMemcpyAsync(ctx->vd_blk.p, blocks.data(), blocks.size() * sizeof(DecodeBlock),
+                                 cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess)
+            return cuda_err(e);
+        decode_blocks_kernel<O><<<(unsigned)blocks.size(), kDecodeThreads, 0, ctx->st>>>(
+            ctx->vd_src.as<uint8_t>(), ctx->vd_blk.as<DecodeBlock>(), ctx->vd_dec.as<uint8_t>(), d_dst, v->H, v->W,
+            code, v->big_endian ? 1 : 0, ctx->vd_bad.as<uint32_t>());
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e);
+        uint32_t bad = 0;
+        if ((e = cudaMemcpyAsync(&bad, ctx->vd_bad.p, 4, cudaMemcpyDeviceToHost, ctx->st)) != cudaSuccess)
+            return cuda_err(e);
+        if ((e = cudaStreamSynchronize(ctx->st)) != cudaSuccess) return cuda_err(e);
+        if (bad) return verr(GT_ERR_READ, "corrupt compressed TIFF data");
+        hsrc.clear();
+        blocks.clear();
+        dec_bytes = 0;
+        return GT_OK;
+    };
+    auto add = [&](const uint8_t* stream, size_t len, uint32_t comp, uint32_t want, int32_t frame, int32_t by,
+                   int32_t bx, int32_t rows, int32_t bw, int32_t pred) {
+        DecodeBlock b;
+        b.src = hsrc.size();
+        b.dec = dec_bytes;
+        b.src_len = (uint32_t)len;
+        b.want = want;
+        b.comp = comp;
+        b.frame = frame;
+        b.by = by;
+        b.bx = bx;
+        b.rows = rows;
+        b.bw = bw;
+        b.pred = pred;
+        b.pad = 0;
+        hsrc.insert(hsrc.end(), stream, stream + len);
+        hsrc.resize((hsrc.size() + 15) & ~(size_t)15);
+        dec_bytes += ((uint64_t)want + 15) & ~(uint64_t)15;
+        blocks.push_back(b);
+    };
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t k = keys ? keys[i] : i;
+        if (k < 0 || k >= T)
+            return verr(GT_ERR_FRAME_OUT_OF_BOUNDS, "tried to access frame " + std::to_string(k) +
+                                                        " of a video with " + std::to_string(T) + " frames");
+        if (v->kind == Kind::Ets) {
+            const size_t want = (size_t)v->H * v->W * bs;
+            raw.resize(want);
+            if (!v->file.read_at((int64_t)v->ets_frames[(size_t)k], raw.data(), want))
+                return verr(GT_ERR_READ, "ETS frame outside the file");
+            // ETS samples are little endian: the kernel reads them with the video's byte order flag (false)
+            add(raw.data(), want, kCompNone, (uint32_t)want, (int32_t)i, 0, 0, v->H, v->W, 1);
+        } else {
+            const TiffImage& im = v->images[(size_t)k];
+            const bool tiled = im.tile_w > 0 && im.tile_h > 0;
+            const uint32_t bw = tiled ? im.tile_w : im.width;
+            const uint32_t bh = tiled ? im.tile_h : im.rows_per_strip;
+            const uint32_t across = tiled ? (im.width + bw - 1) / bw : 1;
+            for (size_t b = 0; b < im.offsets.size(); b++) {
+                const uint32_t by = (uint32_t)(b / across) * bh, bx = (uint32_t)(b % across) * bw;
+                if (by >= im.height) break;
+                const uint32_t rows = tiled ? bh : std::min(bh, im.height - by);
+                const size_t want = (size_t)rows * bw * bs;
+                if (want >= (1ull << 32)) return verr(GT_ERR_READ, "TIFF strip or tile too large");
+                raw.resize((size_t)im.counts[b]);
+                if (im.counts[b] > (uint64_t)v->file.size ||
+                    !v->file.read_at((int64_t)im.offsets[b], raw.data(), raw.size()))
+                    return verr(GT_ERR_READ, "TIFF strip or tile outside the file");
+                switch (im.compression) {
+                    case 1:
+                        if (raw.size() < want) return verr(GT_ERR_READ, "corrupt compressed TIFF data");
+                        add(raw.data(), want, kCompNone, (uint32_t)want, (int32_t)i, (int32_t)by, (int32_t)bx,
+                            (int32_t)rows, (int32_t)bw, (int32_t)im.predictor);
+                        break;
+                    case 32773:
+                    case 5:
+                        add(raw.data(), raw.size(), im.compression == 5 ? kCompLzw : kCompPackBits, (uint32_t)want,
+                            (int32_t)i, (int32_t)by, (int32_t)bx, (int32_t)rows, (int32_t)bw, (int32_t)im.predictor);
+                        break;
+                    default:
+                        if (!inflate_all(raw, dec, want)) return verr(GT_ERR_READ, "corrupt compressed TIFF data");
+                        add(dec.data(), want, kCompNone, (uint32_t)want, (int32_t)i, (int32_t)by, (int32_t)bx,
+                            (int32_t)rows, (int32_t)bw, (int32_t)im.predictor);
+                        break;
+                }
+                if (hsrc.size() >= kDecodeBatchBytes) {
+                    gt_status st = flush();
+                    if (st != GT_OK) return st;
+                }
+            }
+        }
+        if (hsrc.size() >= kDecodeBatchBytes) {
+            gt_status st = flush();
+            if (st != GT_OK) return st;
+        }
+    }
+    return flush();
+}
+
+}  // namespace
+
+// the span check of the context unit (gt_api.cu)
+extern "C" gt_status gt__device_span_check(gt_ctx* ctx, const void* p, size_t bytes, const char* what);
+
 extern "C" {
 
 GT_API gt_status gt_video_open(const char* path, int32_t channel, gt_video** out) {
@@ -520,6 +845,21 @@ GT_API gt_status gt_video_read(gt_video* v, const int64_t* frames, int64_t n, in
     if (dtype != v->dtype) return verr(GT_ERR_INVALID_ARGUMENT, "frames decode to their own dtype or to f32");
     if (dtype == GT_DTYPE_U16) return read_frames<uint16_t>(v, frames, n, (uint16_t*)dst);
     return read_frames<uint8_t>(v, frames, n, (uint8_t*)dst);
+}
+
+GT_API gt_status gt_video_read_device(gt_ctx* ctx, gt_video* v, const int64_t* frames, int64_t n, int32_t dtype,
+                                      void* dst) {
+    if (!ctx || !v || (!dst && n > 0) || n < 0) return verr(GT_ERR_INVALID_ARGUMENT, "null argument");
+    if (dtype != GT_DTYPE_F32 && dtype != v->dtype)
+        return verr(GT_ERR_INVALID_ARGUMENT, "frames decode to their own dtype or to f32");
+    if (n == 0) return GT_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return verr(GT_ERR_CUDA, "cudaSetDevice failed");
+    const size_t eb = dtype == GT_DTYPE_F32 ? 4 : dtype == GT_DTYPE_U16 ? 2 : 1;
+    if (gt__device_span_check(ctx, dst, (size_t)n * v->H * v->W * eb, "frames") != GT_OK)
+        return verr(GT_ERR_INVALID_ARGUMENT, gt_last_error(ctx));
+    if (dtype == GT_DTYPE_F32) return read_frames_device<float>(v, ctx, frames, n, (float*)dst);
+    if (dtype == GT_DTYPE_U16) return read_frames_device<uint16_t>(v, ctx, frames, n, (uint16_t*)dst);
+    return read_frames_device<uint8_t>(v, ctx, frames, n, (uint8_t*)dst);
 }
 
 GT_API void gt_video_close(gt_video* v) { delete v; }

@@ -302,8 +302,9 @@ GT_API int64_t gt_last_walk_starts(const gt_ctx* ctx);
  * classic or BigTIFF, strips or tiles, one sample per pixel, 8/16-bit
  * integers or 32-bit floats, uncompressed / PackBits / LZW / Deflate, with or
  * without horizontal differencing), Olympus .ets (one channel's frames) and
- * .vsi (the .ets at _<stem>_/stack1/frame_t_0.ets beside it).  Host-side
- * decoding, no device needed.  u8 and u16 files keep their dtype; other
+ * .vsi (the .ets at _<stem>_/stack1/frame_t_0.ets beside it), decoded on
+ * the host (gt_video_read, no device needed) or on a GPU
+ * (gt_video_read_device).  u8 and u16 files keep their dtype; other
  * sample types decode to f32.
  */
 typedef struct gt_video gt_video;
@@ -312,6 +313,14 @@ GT_API gt_status gt_video_info(const gt_video* v, int64_t* T, int32_t* H, int32_
 /* Decode frames (frame indices, or the first n when frames is NULL) into dst,
  * (n, H, W) of `dtype` (the video's own dtype or GT_DTYPE_F32). */
 GT_API gt_status gt_video_read(gt_video* v, const int64_t* frames, int64_t n, int32_t dtype, void* dst);
+/* The same frames decoded on the context's GPU into device memory `dst`
+ * (n x H x W of `dtype`): the file's strips, tiles or ETS frames are read on
+ * the host, copied to the device and decompressed there (LZW, PackBits;
+ * Deflate is inflated on the host), with the predictor and the sample
+ * conversion on the device.  Same values as gt_video_read.  Replaces the
+ * decode half of the frame providers (src/decoderiter.rs:64-481). */
+GT_API gt_status gt_video_read_device(gt_ctx* ctx, gt_video* v, const int64_t* frames, int64_t n, int32_t dtype,
+                                      void* dst);
 GT_API void gt_video_close(gt_video* v);
 /* Message of the last failing gt_video_* call of this thread. */
 GT_API const char* gt_video_last_error(void);
