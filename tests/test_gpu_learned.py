@@ -2,7 +2,8 @@
 learned seeds against the plain method.
 
 * forward: the tcgen05 convolutions give the oracle's outputs (BF16
-  operands, FP32 accumulation; tolerance for the accumulation order);
+  operands, FP32 accumulation; relative tolerance 1e-4 for the accumulation
+  order);
 * gradients: loss and every parameter gradient of one batch against the
   oracle's backward pass;
 * training: the network trained by the engine's own kernels on the plain
@@ -61,8 +62,10 @@ def test_forward_matches_oracle(dtype, shape):
     x = co.cells(frames, mean, scale)
     _, head = co.forward(p, x)
     assert got.shape == head.shape[:3] + (4,)
+    # the oracle rounds at the GPU's BF16 points; what remains is the FP32
+    # accumulation order (observed relative errors 1e-7 .. 2e-5)
     for ch in range(3):
-        assert rel_err(got[..., ch], head[..., ch]) < 2e-2, ch
+        assert rel_err(got[..., ch], head[..., ch]) < 1e-4, ch
     assert np.all(got[..., 3] == 0)
 
 
