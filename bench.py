@@ -305,6 +305,10 @@ def run_ragged(args):
         if k:
             parts[name] = {"count": k, "ms": kms}
     ctx.profile(False)
+    # the wave shape the autotuner chose (tile rows, processed bytes per wave)
+    L.gt__ragged_shape.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i64)]
+    seg, budget = i32(), i64()
+    L.gt__ragged_shape(ctx.handle, ctypes.byref(seg), ctypes.byref(budget))
     line = {"metric": "frames/s, 64 ragged videos (one gt_batch_videos call)", "value": frames / (ms / 1000.0),
             "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -313,6 +317,7 @@ def run_ragged(args):
             "features_per_s": rows / (ms / 1000.0), "features": rows,
             "loop_of_gt_batch": {"value": frames / (ms_loop / 1000.0), "ms_per_step": ms_loop},
             "profile_one_call": parts,
+            "tuned_wave_shape": {"tile_rows": seg.value, "wave_bytes": budget.value},
             "gpu_launches": launches, "clocks": clk}
     print(json.dumps(line))
     return 0

@@ -1264,7 +1264,7 @@ gt_status charpoints_impl(gt_ctx* ctx, const gt_params& p0, const T* frames, boo
 // graph and replayed for every wave after the tables are rewritten.  Tile
 // height and wave budget come from the autotuner below.  Results equal one
 // gt_batch call per video (same kernels per tile and per frame).
-constexpr int kRaggedSlots = 256;
+constexpr int kRaggedSlots = 512;
 
 struct RaggedShape {
     int32_t seg;       // rows per strip tile
@@ -1273,8 +1273,10 @@ struct RaggedShape {
 
 // Candidate shapes: tall tiles waste the fewest halo rows, short ones balance
 // the persistent CTAs better on small frames; a small wave keeps its
-// processed images in L2 for the walk, a large one fills the GPU with tiles.
-const RaggedShape kRaggedShapes[] = {{512, 1LL << 30}, {256, 1LL << 30}, {128, 1LL << 30},
+// processed images in L2 for the walk, a large one fills the GPU with tiles
+// and gives finalize (one CTA per frame) many frames at once.
+const RaggedShape kRaggedShapes[] = {{512, 4LL << 30},   {256, 4LL << 30},   {128, 4LL << 30},
+                                     {512, 1LL << 30},   {256, 1LL << 30},   {128, 1LL << 30},
                                      {512, 192LL << 20}, {256, 192LL << 20}, {128, 192LL << 20}};
 constexpr int kRaggedNShapes = (int)(sizeof(kRaggedShapes) / sizeof(kRaggedShapes[0]));
 
@@ -1304,8 +1306,12 @@ gt_status batch_videos_ragged(gt_ctx* ctx, const gt_params& p, const LocateConst
     const int64_t NT = vslot[(size_t)nv];
     int64_t max_px = 0;
     for (int32_t v = 0; v < nv; v++) max_px = std::max<int64_t>(max_px, (int64_t)H_[v] * W_[v]);
+    // a wave never holds more than the call's frames
+    int64_t all_px = 0;
+    for (int32_t v = 0; v < nv; v++) all_px += T_[v] * (int64_t)H_[v] * W_[v];
     int64_t max_budget = 0;
     for (const auto& s : kRaggedShapes) max_budget = std::max(max_budget, s.budget);
+    max_budget = std::min<int64_t>(max_budget, all_px * 4);
     max_budget = std::max<int64_t>(max_budget, max_px * 4);
     ctx->total = NT;
     ctx->done = 0;
