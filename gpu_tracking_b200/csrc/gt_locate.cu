@@ -1168,6 +1168,14 @@ __device__ __forceinline__ void doughnut_warp(const T* __restrict__ raw, int H, 
     ft.d_corr = __fsub_rn(sum, __fmul_rn(med, (float)nsig));
 }
 
+// Shared memory of finalize: sort keys, permutation, order, keep flags and
+// a histogram, then the filter_close positions and masses of up to
+// kFinalizeFcSmem detections.
+constexpr int kFinalizeFcSmem = 4096;
+__host__ __device__ constexpr size_t finalize_smem_core_bytes() {
+    return (size_t)kFinalizeSmemSort * (8 + 4 + 4 + 1) + 32 * 256 * sizeof(uint32_t);
+}
+
 // One CTA per frame: canonical order, filter_close / prune_blobs_log, the
 // doughnut correction and compaction of the kept rows in output order.
 template <typename T>
@@ -1234,6 +1242,21 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
     if (!fc.log_style) {
         // 2a. filter_close_trackpy (src/execute_gpu.rs:556-590) in canonical order
         if (fc.filter_close) {
+            // positions and masses in canonical order, in shared memory when
+            // they fit: the neighbour scans then read no global memory
+            const bool fc_smem = np2 <= kFinalizeSmemSort && n <= kFinalizeFcSmem;
+            float* const fcx = (float*)((uint8_t*)fsm + finalize_smem_core_bytes());
+            float* const fcy = fcx + kFinalizeFcSmem;
+            float* const fcm = fcy + kFinalizeFcSmem;
+            if (fc_smem) {
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    const Feature& ft = F[perm[i]];
+                    fcx[i] = ft.x;
+                    fcy[i] = ft.y;
+                    fcm[i] = ft.mass;
+                }
+                __syncthreads();
+            }
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
                 const Feature& q = F[perm[i]];
                 int lo = 0, hi = n;
@@ -1251,13 +1274,24 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
                     hi = a;
                 }
                 bool kp = true;
-                for (int j = lo; j < hi && kp; j++) {
-                    if (j == i) continue;
-                    const Feature& nb = F[perm[j]];
-                    float dist;
-                    if (!within_rd2(nb.x, nb.y, q.x, q.y, fc.separation, &dist)) continue;
-                    if (q.mass < nb.mass) kp = false;
-                    else if (q.mass == nb.mass && i > j) kp = false;
+                if (fc_smem) {
+                    const float qx = fcx[i], qy = fcy[i], qm = fcm[i];
+                    for (int j = lo; j < hi && kp; j++) {
+                        if (j == i) continue;
+                        float dist;
+                        if (!within_rd2(fcx[j], fcy[j], qx, qy, fc.separation, &dist)) continue;
+                        if (qm < fcm[j]) kp = false;
+                        else if (qm == fcm[j] && i > j) kp = false;
+                    }
+                } else {
+                    for (int j = lo; j < hi && kp; j++) {
+                        if (j == i) continue;
+                        const Feature& nb = F[perm[j]];
+                        float dist;
+                        if (!within_rd2(nb.x, nb.y, q.x, q.y, fc.separation, &dist)) continue;
+                        if (q.mass < nb.mass) kp = false;
+                        else if (q.mass == nb.mass && i > j) kp = false;
+                    }
                 }
                 keep[i] = kp ? 1 : 0;
             }
@@ -1382,9 +1416,7 @@ size_t bandpass_smem_bytes(int R, int kd, bool cand) {
     return fl * sizeof(float);
 }
 
-size_t finalize_smem_bytes() {
-    return (size_t)kFinalizeSmemSort * (8 + 4 + 4 + 1) + 32 * 256 * sizeof(uint32_t);
-}
+size_t finalize_smem_bytes() { return finalize_smem_core_bytes() + (size_t)kFinalizeFcSmem * 3 * sizeof(float); }
 
 template <typename T>
 cudaError_t launch_bandpass(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c,
