@@ -300,6 +300,7 @@ struct PipeLink {
     int K = 1;
     int64_t C = 0, list_cap = 0, max_items = 0;
     size_t scan_bytes = 0;
+    int64_t nwin = 0;   // windows issued in this call
 
     gt_status setup(gt_ctx* c, int64_t NT, uint32_t feat_cap, int SC, float radius, int memory,
                     const std::vector<uint8_t>& reset) {
@@ -312,13 +313,18 @@ struct PipeLink {
         if (ctx->w_edge_cap <= 0) ctx->w_edge_cap = std::max<int64_t>(C * 16, 1 << 16);
         list_cap = ctx->w_list_cap;
         CK(ctx->w_srt.ensure(NS * 4));
-        CK(ctx->w_fcnt.ensure(max_items * 8));
-        CK(ctx->w_bcnt.ensure(max_items * 8));
-        CK(ctx->w_foff.ensure(max_items * 8));
-        CK(ctx->w_boff.ensure(max_items * 8));
-        CK(ctx->w_fpts.ensure(list_cap * 4));
-        CK(ctx->w_bpts.ensure(list_cap * 4));
-        CK(ctx->w_bdist.ensure(list_cap * 4));
+        // the previous call's list kernels may still read the buffers
+        CK(cudaStreamSynchronize(ctx->ls));
+        for (int b = 0; b < 2; b++) {
+            CK(ctx->w_fcnt[b].ensure(max_items * 8));
+            CK(ctx->w_bcnt[b].ensure(max_items * 8));
+            CK(ctx->w_foff[b].ensure(max_items * 8));
+            CK(ctx->w_boff[b].ensure(max_items * 8));
+            CK(ctx->w_fpts[b].ensure(list_cap * 4));
+            CK(ctx->w_bpts[b].ensure(list_cap * 4));
+            CK(ctx->w_bdist[b].ensure(list_cap * 4));
+        }
+        nwin = 0;
         CK(ctx->w_ids.ensure(NS * 8));
         CK(ctx->w_dur.ensure(NS * 8));
         CK(ctx->w_state.ensure(sizeof(LinkState)));
@@ -333,8 +339,8 @@ struct PipeLink {
         CK(ctx->w_scratch.ensure(S.bytes_per_video));
         S.base = ctx->w_scratch.as<uint8_t>();
         scan_bytes = 0;
-        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, ctx->w_fcnt.as<int64_t>(), ctx->w_foff.as<int64_t>(),
-                                         max_items, ctx->lk));
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, ctx->w_fcnt[0].as<int64_t>(),
+                                         ctx->w_foff[0].as<int64_t>(), max_items, ctx->ls));
         CK(ctx->w_scan.ensure(scan_bytes));
 
         const int32_t vg[2] = {0, (int32_t)NT};
@@ -349,7 +355,7 @@ struct PipeLink {
         CK(cudaMemsetAsync(ctx->w_flags.p, 0, 4, ctx->lk));
         CK(cudaMemsetAsync(ctx->w_cnt.p, 0, 8, ctx->lk));
         // the host buffers above are read before the call returns
-        CK(cudaStreamSynchronize(ctx->lk));
+        CK(sync_link_streams(ctx));
 
         in = LinkInput();
         const float* f = (const float*)ctx->feats_out.p;
@@ -373,46 +379,53 @@ struct PipeLink {
         return GT_OK;
     }
 
-    // frames [s0, s1) have been located on the compute stream
+    // frames [s0, s1) have been located on the compute stream.  The window's
+    // sort and neighbour lists run on the lists stream into list set b (the
+    // set window w - 2 used, once its linker is done with it), so they overlap
+    // the linker of window w - 1; the linker of this window waits for them.
     gt_status window(int s0, int s1, bool first, bool last) {
         const int LA = std::max(0, s0 - K);
         const int64_t p0 = (int64_t)LA * C, p1 = (int64_t)s1 * C;
         const int64_t items = (p1 - p0) * K + 1;
         if (items > max_items) return set_err(ctx, GT_ERR_INTERNAL, "link window larger than its buffers");
+        const int b = (int)(nwin & 1);
         CK(cudaEventRecord(ctx->located, ctx->st));
-        CK(cudaStreamWaitEvent(ctx->lk, ctx->located, 0));
+        CK(cudaStreamWaitEvent(ctx->ls, ctx->located, 0));
+        if (nwin >= 2) CK(cudaStreamWaitEvent(ctx->ls, ctx->w_linked[b], 0));
+        nwin++;
         in.groups_ready = s1;
         uint32_t* srt = ctx->w_srt.as<uint32_t>();
         {
-            Prof pf(ctx, "link_sort", ctx->lk);
-            CK(link_sort_groups_range(in, srt, s0, s1, ctx->lk));
+            Prof pf(ctx, "link_sort", ctx->ls);
+            CK(link_sort_groups_range(in, srt, s0, s1, ctx->ls));
         }
-        CK(cudaMemsetAsync(ctx->w_fcnt.p, 0, items * 8, ctx->lk));
-        CK(cudaMemsetAsync(ctx->w_bcnt.p, 0, items * 8, ctx->lk));
+        int64_t* fcnt = ctx->w_fcnt[b].as<int64_t>();
+        int64_t* bcnt = ctx->w_bcnt[b].as<int64_t>();
+        CK(cudaMemsetAsync(fcnt, 0, items * 8, ctx->ls));
+        CK(cudaMemsetAsync(bcnt, 0, items * 8, ctx->ls));
         {
-            Prof pf(ctx, "link_lists", ctx->lk);
-            CK(link_count_lists_range(in, srt, p0, p1, ctx->w_fcnt.as<int64_t>(), ctx->w_bcnt.as<int64_t>(),
-                                      out.flags, ctx->lk));
+            Prof pf(ctx, "link_lists", ctx->ls);
+            CK(link_count_lists_range(in, srt, p0, p1, fcnt, bcnt, out.flags, ctx->ls));
         }
         size_t tb = scan_bytes;
-        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, ctx->w_fcnt.as<int64_t>(), ctx->w_foff.as<int64_t>(),
-                                         items, ctx->lk));
-        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, ctx->w_bcnt.as<int64_t>(), ctx->w_boff.as<int64_t>(),
-                                         items, ctx->lk));
+        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, fcnt, ctx->w_foff[b].as<int64_t>(), items, ctx->ls));
+        CK(cub::DeviceScan::ExclusiveSum(ctx->w_scan.p, tb, bcnt, ctx->w_boff[b].as<int64_t>(), items, ctx->ls));
         LinkLists L;
-        L.f_off = ctx->w_foff.as<int64_t>();
-        L.b_off = ctx->w_boff.as<int64_t>();
-        L.f_pts = ctx->w_fpts.as<int32_t>();
-        L.b_pts = ctx->w_bpts.as<int32_t>();
-        L.b_dist = ctx->w_bdist.as<float>();
+        L.f_off = ctx->w_foff[b].as<int64_t>();
+        L.b_off = ctx->w_boff[b].as<int64_t>();
+        L.f_pts = ctx->w_fpts[b].as<int32_t>();
+        L.b_pts = ctx->w_bpts[b].as<int32_t>();
+        L.b_dist = ctx->w_bdist[b].as<float>();
         L.srt = srt;
         L.pbase = p0;
         L.f_cap = list_cap;
         L.b_cap = list_cap;
         {
-            Prof pf(ctx, "link_lists", ctx->lk);
-            CK(link_fill_lists_range(in, L, p1, out.flags, ctx->lk));
+            Prof pf(ctx, "link_lists", ctx->ls);
+            CK(link_fill_lists_range(in, L, p1, out.flags, ctx->ls));
         }
+        CK(cudaEventRecord(ctx->listed[b], ctx->ls));
+        CK(cudaStreamWaitEvent(ctx->lk, ctx->listed[b], 0));
         LinkWindow w;
         w.g0 = s0;
         w.g1 = s1;
@@ -424,6 +437,7 @@ struct PipeLink {
             Prof pf(ctx, "link_video", ctx->lk);
             CK(link_run_window(in, L, S, out, w, ctx->lk));
         }
+        CK(cudaEventRecord(ctx->w_linked[b], ctx->lk));
         return GT_OK;
     }
 };
@@ -684,7 +698,7 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
         if (interrupted(ctx)) {
             cudaStreamSynchronize(ctx->st);
             cudaStreamSynchronize(ctx->cp);
-            cudaStreamSynchronize(ctx->lk);
+            sync_link_streams(ctx);
             return set_err(ctx, GT_ERR_INTERRUPTED, "Keyboard Interrupt, my custom version");
         }
         const int64_t s0 = (int64_t)sc * SC;
@@ -961,17 +975,17 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         gt_status st = locate_pass<T>(ctx, p, frames, on_device, NT, H, W, c, log_style ? &lt : nullptr, F, &fl,
                                       windowed ? &pl : nullptr, &reset, net);
         if (st != GT_OK) {
-            cudaStreamSynchronize(ctx->lk);
+            sync_link_streams(ctx);
             return st;
         }
         if (fl & (kFlagTensorTimeout | kFlagLocalWalk)) {
-            cudaStreamSynchronize(ctx->lk);
+            sync_link_streams(ctx);
             return set_err(ctx, GT_ERR_INTERNAL,
                            (fl & kFlagTensorTimeout) ? "a tensor-core kernel timed out waiting for its UMMAs"
                                                      : "a learned seed's walk did not finish");
         }
         if (!(fl & (kFlagCandOverflow | kFlagFeatOverflow))) break;
-        CK(cudaStreamSynchronize(ctx->lk));
+        CK(sync_link_streams(ctx));
         const uint64_t npx = (uint64_t)H * W;
         if (attempt > 8) return set_err(ctx, GT_ERR_CAPACITY_EXCEEDED, "per-frame capacity exceeded");
         if (fl & kFlagCandOverflow) {
@@ -992,7 +1006,7 @@ gt_status batch_impl(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_d
         HostSpan hs(ctx, "host_assemble");
         gt_status st = assemble_table(ctx, NT, fnum, log_style, tab, row_off);
         if (st != GT_OK) {
-            cudaStreamSynchronize(ctx->lk);
+            sync_link_streams(ctx);
             return st;
         }
     }
@@ -1894,14 +1908,20 @@ gt_status gt_create(int32_t device, gt_ctx** out) {
     if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->cp, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->lk, cudaStreamNonBlocking, link_stream_priority()) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->ls, cudaStreamNonBlocking, link_stream_priority()) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->located, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->linked, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
         return GT_ERR_CUDA;
     }
     for (int i = 0; i < 2; i++) {
-        cudaEventCreateWithFlags(&ctx->used[i], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&ctx->filled[i], cudaEventDisableTiming);
+        if (cudaEventCreateWithFlags(&ctx->used[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->filled[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->listed[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->w_linked[i], cudaEventDisableTiming) != cudaSuccess) {
+            gt_destroy(ctx);
+            return GT_ERR_CUDA;
+        }
     }
     *out = ctx;
     return GT_OK;
@@ -1912,12 +1932,14 @@ void gt_destroy(gt_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->st);
     cudaStreamSynchronize(ctx->cp);
-    cudaStreamSynchronize(ctx->lk);
+    sync_link_streams(ctx);
     drain_profile(ctx);
     for (auto e : ctx->event_pool) cudaEventDestroy(e);
     for (int i = 0; i < 2; i++) {
-        cudaEventDestroy(ctx->used[i]);
-        cudaEventDestroy(ctx->filled[i]);
+        if (ctx->used[i]) cudaEventDestroy(ctx->used[i]);
+        if (ctx->filled[i]) cudaEventDestroy(ctx->filled[i]);
+        if (ctx->listed[i]) cudaEventDestroy(ctx->listed[i]);
+        if (ctx->w_linked[i]) cudaEventDestroy(ctx->w_linked[i]);
     }
     if (ctx->rg_graph) cudaGraphExecDestroy(ctx->rg_graph);
     cudaEventDestroy(ctx->located);
@@ -1925,6 +1947,7 @@ void gt_destroy(gt_ctx* ctx) {
     cudaStreamDestroy(ctx->st);
     cudaStreamDestroy(ctx->cp);
     cudaStreamDestroy(ctx->lk);
+    cudaStreamDestroy(ctx->ls);
     delete ctx;
 }
 
@@ -1966,7 +1989,7 @@ gt_status gt_batch(gt_ctx* ctx, const gt_params* params, const void* frames, int
     if (st != GT_OK) {
         // no kernel may still write the table when its columns go back to the pool
         cudaStreamSynchronize(ctx->st);
-        cudaStreamSynchronize(ctx->lk);
+        sync_link_streams(ctx);
         return st;
     }
     *out = tab.release();
@@ -2004,7 +2027,7 @@ gt_status gt_batch_learned(gt_ctx* ctx, const gt_params* params, const gt_propos
                                  linker_reset_points, n_reset, tab.get(), net);
     if (st != GT_OK) {
         cudaStreamSynchronize(ctx->st);
-        cudaStreamSynchronize(ctx->lk);
+        sync_link_streams(ctx);
         return st;
     }
     *out = tab.release();
@@ -2033,7 +2056,7 @@ gt_status gt_batch_videos(gt_ctx* ctx, const gt_params* params, int32_t n_videos
         st = batch_videos_impl<uint8_t>(ctx, *params, n_videos, frames, T, H, W, raw.data());
     if (st != GT_OK) {
         cudaStreamSynchronize(ctx->st);
-        cudaStreamSynchronize(ctx->lk);
+        sync_link_streams(ctx);
         return st;
     }
     for (int32_t v = 0; v < n_videos; v++) out[v] = tabs[(size_t)v].release();
@@ -2063,7 +2086,7 @@ gt_status gt_characterize_points(gt_ctx* ctx, const gt_params* params, const voi
     if (st != GT_OK) {
         // no kernel may still write the table when its columns go back to the pool
         cudaStreamSynchronize(ctx->st);
-        cudaStreamSynchronize(ctx->lk);
+        sync_link_streams(ctx);
         return st;
     }
     *out = tab.release();

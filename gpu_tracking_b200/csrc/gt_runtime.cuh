@@ -121,7 +121,10 @@ struct gt_ctx {
     cudaStream_t st = nullptr;   // compute
     cudaStream_t cp = nullptr;   // host -> device copies
     cudaStream_t lk = nullptr;   // linking of located frames, overlapped with locating
+    cudaStream_t ls = nullptr;   // neighbour lists of the next link window, beside the linker
     cudaEvent_t located = nullptr, linked = nullptr;
+    cudaEvent_t listed[2] = {nullptr, nullptr};    // list set b holds its window's lists
+    cudaEvent_t w_linked[2] = {nullptr, nullptr};  // the linker finished with list set b
     cudaEvent_t used[2] = {nullptr, nullptr};    // compute finished with staging buffer b
     cudaEvent_t filled[2] = {nullptr, nullptr};  // staging buffer b holds its chunk
     std::string err;
@@ -146,8 +149,10 @@ struct gt_ctx {
     DBuf vd_src, vd_dec, vd_blk, vd_bad;  // video files decoded on the device: streams, bytes, blocks, flag
     int64_t last_walk_starts = 0;
     int32_t illum_rint = 0;
-    DBuf w_srt, w_fcnt, w_bcnt, w_foff, w_boff, w_fpts, w_bpts, w_bdist, w_scan, w_scratch, w_ids, w_dur, w_state,
-        w_cnt, w_flags, w_vgrp, w_reset;
+    DBuf w_srt, w_scan, w_scratch, w_ids, w_dur, w_state, w_cnt, w_flags, w_vgrp, w_reset;
+    // two sets of window neighbour lists: the lists of window w + 1 are built
+    // while the linker reads those of window w
+    DBuf w_fcnt[2], w_bcnt[2], w_foff[2], w_boff[2], w_fpts[2], w_bpts[2], w_bdist[2];
     // ragged batches (gt_batch_videos): frame / task tables of the current
     // wave, the captured stage graph (valid while the buffers it names stay
     // where they are: rg_graph_key) and the tuned wave shape per workload
@@ -183,6 +188,13 @@ struct gt_table {
 
 namespace gt {
 namespace rt {
+
+// Waits for the link-side streams (neighbour lists and linker) to finish.
+inline cudaError_t sync_link_streams(gt_ctx* ctx) {
+    const cudaError_t a = cudaStreamSynchronize(ctx->ls);
+    const cudaError_t b = cudaStreamSynchronize(ctx->lk);
+    return a != cudaSuccess ? a : b;
+}
 
 inline gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
     char buf[512];
