@@ -35,7 +35,6 @@ namespace gt {
 namespace {
 
 constexpr int kSSTH = 16, kSSTW = 128, kSSThreads = 256;
-constexpr int kSSRG = (kSSTH + 2) / 2;   // pass A rows per task (two row groups)
 constexpr int kSSCB = 5;                 // pass B columns per task ((TW + 2) = 26 * 5)
 static_assert((kSSTW + 2) % kSSCB == 0, "pass B column blocks");
 constexpr int kSSPW = kSSTW + 2;         // plane tile width (tile +- 1)
@@ -67,6 +66,24 @@ struct SSChunk {
     static constexpr int value = R > 23 ? 4 : (R > 20 ? 8 : 16);
 };
 
+// Rows per pass A task for radius R: the plane's kSSPH rows of each of its
+// kSSPW + 2R columns are split into tasks of RG rows; RG (a divisor of
+// kSSPH) minimises the thread rounds ceil(tasks / threads) * RG, the larger
+// RG on a tie (a longer register window per loaded value).
+template <int R>
+struct SSRows {
+    static constexpr int C = kSSPW + 2 * R;
+    static constexpr int rounds(int rg) { return ((kSSPH / rg) * C + kSSThreads - 1) / kSSThreads * rg; }
+    static constexpr int pick() {
+        int best = 9;
+        for (int rg : {6, 3, 2})
+            if (rounds(rg) < rounds(best)) best = rg;
+        return best;
+    }
+    static constexpr int value = pick();
+    static_assert(kSSPH % value == 0, "row groups tile the plane rows");
+};
+
 // pass A of one radius: column `col` of the pass A planes, rows grp*RG ..
 template <int R>
 __device__ __forceinline__ void ss_pass_a(const float* __restrict__ raw, const SSGeom& g, float* __restrict__ sa,
@@ -74,9 +91,10 @@ __device__ __forceinline__ void ss_pass_a(const float* __restrict__ raw, const S
                                           const float* __restrict__ td, float ng, float nd) {
     constexpr int NT = 2 * R + 1;
     constexpr int kSSChunk = SSChunk<R>::value;
+    constexpr int kSSRG = SSRows<R>::value, NGRP = kSSPH / kSSRG;
     const int ncols = kSSPW + 2 * R;
-    for (int task = threadIdx.x; task < 2 * ncols; task += kSSThreads) {
-        const int grp = task >= ncols ? 1 : 0;
+    for (int task = threadIdx.x; task < NGRP * ncols; task += kSSThreads) {
+        const int grp = task / ncols;
         const int col = task - grp * ncols;
         const int u0 = grp * kSSRG;
         // plane row u0 + k, column col <-> raw row u0 + k + RMAX - R + i, raw column col + RMAX - R
