@@ -207,6 +207,141 @@ __device__ __forceinline__ void flush_tile_cands(const int tid, uint32_t* cbuf_n
     __syncthreads();
 }
 
+// Raw rows of one 8-row step of a tile: loaded into registers (4 pixels per
+// aligned load, or one clamped pixel each at the frame's edges) while the
+// previous step is being filtered, then stored to the staging rows as exact
+// floats.  Rows and columns outside the frame read the nearest edge pixel.
+template <typename T, int R, int KD>
+struct RawRows {
+    using G = StripGeom<R, KD>;
+    typename Quad<T>::V pv[G::RAWVPT];
+    float px[G::RAWPT];
+
+    __device__ __forceinline__ void load(const T* __restrict__ img, const int H, const int W, const int x0,
+                                         const int xa, const bool vec, const int s) {
+        const int tid = threadIdx.x;
+        const int rbase = x0 + kStepRows * s;
+        if (vec) {
+#pragma unroll
+            for (int q = 0; q < G::RAWVPT; q++) {
+                const int v = tid + q * kStripThreads;
+                if (v < G::RAWV) {
+                    const int j = v / G::RW4, k4 = v - j * G::RW4;
+                    const int gr = min(max(rbase + j, 0), H - 1);
+                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < G::RAWPT; q++) {
+                const int idx = tid + q * kStripThreads;
+                float v = 0.0f;
+                if (idx < G::RAWN) {
+                    const int j = idx / G::RWp, k = idx - j * G::RWp;
+                    const int gr = min(max(rbase + j, 0), H - 1);
+                    const int gc = min(max(xa + k, 0), W - 1);
+                    v = load_px<T>(img, (size_t)gr * W + gc);
+                }
+                px[q] = v;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void store(float* __restrict__ stage, const bool vec) const {
+        const int tid = threadIdx.x;
+        if (vec) {
+#pragma unroll
+            for (int q = 0; q < G::RAWVPT; q++) {
+                const int v = tid + q * kStripThreads;
+                if (v < G::RAWV) {
+                    const int j = v / G::RW4, k4 = v - j * G::RW4;
+                    *(float4*)(stage + j * G::RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < G::RAWPT; q++) {
+                const int idx = tid + q * kStripThreads;
+                if (idx < G::RAWN) stage[idx] = px[q];
+            }
+        }
+    }
+};
+
+// Stage E of one step (extract_max.wgsl): for the step's 8 dilation rows
+// d = dbase + jj, 4 columns per thread, the horizontal maximum of the
+// vertical maxima vb, the candidate test of every column without branches
+// (columns and rows inside the margin need no bounds test) and the store of
+// the processed row to HBM; center_row(jj) is the shared-memory row that
+// holds processed row dbase + jj.
+template <int R, int KD, typename CenterRow>
+__device__ __forceinline__ void extract_step(const int tid, const float* vb, CenterRow center_row, const int dbase,
+                                             const int R0, const int R1, const int c0, const int H, const int W,
+                                             const LocateConsts& c, const float thr, const bool st4,
+                                             float* __restrict__ proc, uint32_t* cbuf_n, uint32_t* cbuf,
+                                             uint32_t* __restrict__ cand_slot, uint32_t* __restrict__ cout,
+                                             const uint32_t cand_cap, uint32_t* __restrict__ flags) {
+    using G = StripGeom<R, KD>;
+    constexpr int O = G::O, PWp = G::PWp, SH4 = G::SH4;
+    int cnt = 0;
+    uint32_t cmask = 0;
+    int cd = 0, ccol = 0;
+    if (tid < kStepRows * (kStripTW / 4)) {
+        const int jj = tid / (kStripTW / 4), cg = tid - jj * (kStripTW / 4);
+        const int d = dbase + jj;
+        const int cc = 4 * cg;  // interior column offset; processed column = cc + O (pc0-relative)
+        if (d >= R0 && d < R1) {
+            const float4* src = (const float4*)(vb + jj * PWp + cc);
+            float a[4 * G::NV4];
+#pragma unroll
+            for (int i = 0; i < G::NV4; i++) {
+                const float4 v = src[i];
+                a[4 * i] = v.x;
+                a[4 * i + 1] = v.y;
+                a[4 * i + 2] = v.z;
+                a[4 * i + 3] = v.w;
+            }
+            const float mid = Tree<KD - 3>::max(a + 3);
+            float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
+            float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
+            float m[4] = {fmaxf(s0, mid), fmaxf(fmaxf(s1, mid), p1), fmaxf(fmaxf(s2, mid), p2), fmaxf(mid, p3)};
+            const float* cen = center_row(jj) + SH4 + O + cc;
+            float cv[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) cv[k] = cen[k];
+            const int gc0 = c0 + cc;
+            float* dst = proc + (size_t)d * W + gc0;
+            if (st4 && gc0 + 3 < W) {
+                *(float4*)dst = make_float4(cv[0], cv[1], cv[2], cv[3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (gc0 + k < W) dst[k] = cv[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float center = cv[k];
+                bool ok = !(center < thr) && !(m[k] > center);
+                if (c.skip_zero) ok = ok && (center != 0.0f);
+                cmask |= (uint32_t)ok << k;
+            }
+            const bool inner = d >= c.margin && d < H - c.margin && gc0 >= c.margin && gc0 + 3 < W - c.margin;
+            if (!inner) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int gc = gc0 + k;
+                    if (gc >= W || d < c.margin || d >= H - c.margin || gc < c.margin || gc >= W - c.margin)
+                        cmask &= ~(1u << k);
+                }
+            }
+            cnt = __popc(cmask);
+            cd = d;
+            ccol = gc0;
+        }
+    }
+    append_cands(tid, cnt, cmask, cd, ccol, W, cbuf_n, cbuf, cand_slot, cout, cand_cap, flags);
+}
+
 // One tile: the strip of output columns [c0, c0 + 128) and rows [R0, R1) of
 // an H x W frame (img: its pixels, proc: its processed image), candidates
 // appended to the list counted by *cand_slot (keys at cout).
@@ -242,37 +377,9 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
     // ---- A: staging of raw rows (registers hold the next step's pixels)
-    typename Quad<T>::V pv[G::RAWVPT];
-    float ps_[G::RAWPT];
-    auto load_raw = [&](int s) {
-        const int rbase = x0 + kStepRows * s;
-        if (vec) {
-#pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
-                const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
-                    const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    const int gr = min(max(rbase + j, 0), H - 1);
-                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < G::RAWPT; q++) {
-                const int idx = tid + q * kStripThreads;
-                float v = 0.0f;
-                if (idx < G::RAWN) {
-                    const int j = idx / RWp, k = idx - j * RWp;
-                    const int gr = min(max(rbase + j, 0), H - 1);
-                    const int gc = min(max(xa + k, 0), W - 1);
-                    v = load_px<T>(img, (size_t)gr * W + gc);
-                }
-                ps_[q] = v;
-            }
-        }
-    };
+    RawRows<T, R, KD> raw;
     if (tid == 0) *cbuf_n = 0;
-    load_raw(0);
+    raw.load(img, H, W, x0, xa, vec, 0);
     // The first column-pass groups read row-pass rows above x0 that no step
     // writes.  The outputs that need them are never used, but the sliding
     // boxcar sum of a group carries its first window into the rows after it
@@ -283,24 +390,9 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
     const float trunc_thr = 1.0f / 255.0f;
 
     for (int s = 0; s < nsteps; s++) {
-        if (vec) {
-#pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
-                const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
-                    const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    *(float4*)(stage + j * RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < G::RAWPT; q++) {
-                const int idx = tid + q * kStripThreads;
-                if (idx < G::RAWN) stage[idx] = ps_[q];
-            }
-        }
+        raw.store(stage, vec);
         __syncthreads();
-        if (s + 1 < nsteps) load_raw(s + 1);
+        if (s + 1 < nsteps) raw.load(img, H, W, x0, xa, vec, s + 1);
 
         // ---- B: row pass (preprocess_rows.wgsl), 8 rows x PWp columns, 4 per thread
         {
@@ -440,72 +532,11 @@ __device__ __forceinline__ void strip_tile(const T* __restrict__ img, float* __r
         }
         __syncthreads();
 
-        // ---- E: horizontal maximum and the candidate test (extract_max.wgsl);
-        // the processed rows of the segment go to HBM from here, 4 columns
-        // per thread
-        {
-            const int t = tid;
-            int cnt = 0;
-            uint32_t cmask = 0;
-            int cd = 0, ccol = 0;
-            if (t < kStepRows * (kStripTW / 4)) {
-                const int jj = t / (kStripTW / 4), cg = t - jj * (kStripTW / 4);
-                const int d = dbase + jj;
-                const int cc = 4 * cg;  // interior column offset; processed column = cc + O (pc0-relative)
-                if (d >= R0 && d < R1) {
-                    const float4* src = (const float4*)(vb + jj * PWp + cc);
-                    float a[4 * G::NV4];
-#pragma unroll
-                    for (int i = 0; i < G::NV4; i++) {
-                        const float4 v = src[i];
-                        a[4 * i] = v.x;
-                        a[4 * i + 1] = v.y;
-                        a[4 * i + 2] = v.z;
-                        a[4 * i + 3] = v.w;
-                    }
-                    const float mid = Tree<KD - 3>::max(a + 3);
-                    float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
-                    float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
-                    float m[4] = {fmaxf(s0, mid), fmaxf(fmaxf(s1, mid), p1), fmaxf(fmaxf(s2, mid), p2),
-                                  fmaxf(mid, p3)};
-                    int prow = (kStepRows * s + jj + (PR - E)) % PR;   // relative index of row d: 8s + jj - E
-                    const float* cen = pr + prow * PWp + SH4 + O + cc;
-                    float cv[4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) cv[k] = cen[k];
-                    const int gc0 = c0 + cc;
-                    float* dst = proc + (size_t)d * W + gc0;
-                    if (st4 && gc0 + 3 < W) {
-                        *(float4*)dst = make_float4(cv[0], cv[1], cv[2], cv[3]);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 4; k++)
-                            if (gc0 + k < W) dst[k] = cv[k];
-                    }
-                    // columns and rows inside the margin need no per-column test
-                    const bool inner = d >= c.margin && d < H - c.margin && gc0 >= c.margin &&
-                                       gc0 + 3 < W - c.margin;
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        if (!inner) {
-                            const int gc = gc0 + k;
-                            if (gc >= W || d < c.margin || d >= H - c.margin || gc < c.margin ||
-                                gc >= W - c.margin)
-                                continue;
-                        }
-                        const float center = cv[k];
-                        if (center < thr) continue;
-                        if (c.skip_zero && center == 0.0f) continue;
-                        if (m[k] > center) continue;
-                        cmask |= 1u << k;
-                        cnt++;
-                    }
-                    cd = d;
-                    ccol = gc0;
-                }
-            }
-            append_cands(tid, cnt, cmask, cd, ccol, W, cbuf_n, cbuf, cand_slot, cout, cand_cap, flags);
-        }
+        // ---- E: horizontal maximum, the candidate test and the processed rows
+        // (processed row d = dbase + jj is ring row (8s + jj - E) mod PR)
+        extract_step<R, KD>(tid, vb, [&](int jj) { return pr + ((kStepRows * s + jj + (PR - E)) % PR) * PWp; },
+                            dbase, R0, R1, c0, H, W, c, thr, st4, proc, cbuf_n, cbuf, cand_slot, cout, cand_cap,
+                            flags);
         __syncthreads();
     }
     __syncthreads();
@@ -587,37 +618,9 @@ __device__ __forceinline__ void ring_tile(const T* __restrict__ img, float* __re
     const int nsteps = (R1 - x0 + R + E + kStepRows - 1) / kStepRows;
 
     // ---- A: staging of raw rows (registers hold the next step's pixels)
-    typename Quad<T>::V pv[G::RAWVPT];
-    float ps_[G::RAWPT];
-    auto load_raw = [&](int s) {
-        const int rbase = x0 + kStepRows * s;
-        if (vec) {
-#pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
-                const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
-                    const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    const int gr = min(max(rbase + j, 0), H - 1);
-                    pv[q] = Quad<T>::load(img + (size_t)gr * W + xa + 4 * k4);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < G::RAWPT; q++) {
-                const int idx = tid + q * kStripThreads;
-                float v = 0.0f;
-                if (idx < G::RAWN) {
-                    const int j = idx / RWp, k = idx - j * RWp;
-                    const int gr = min(max(rbase + j, 0), H - 1);
-                    const int gc = min(max(xa + k, 0), W - 1);
-                    v = load_px<T>(img, (size_t)gr * W + gc);
-                }
-                ps_[q] = v;
-            }
-        }
-    };
+    RawRows<T, R, KD> raw;
     if (tid == 0) *cbuf_n = 0;
-    load_raw(0);
+    raw.load(img, H, W, x0, xa, vec, 0);
     // The first column-pass groups read row-pass rows above x0 that no step
     // writes; the sliding boxcar sum carries their values into the rows after
     // them, so the rings start as zeros.
@@ -628,24 +631,9 @@ __device__ __forceinline__ void ring_tile(const T* __restrict__ img, float* __re
     int phase = 0;   // s % PER
     for (int s = 0; s < nsteps; s++) {
         const int P8 = kStepRows * phase;   // first ring row of this step
-        if (vec) {
-#pragma unroll
-            for (int q = 0; q < G::RAWVPT; q++) {
-                const int v = tid + q * kStripThreads;
-                if (v < G::RAWV) {
-                    const int j = v / G::RW4, k4 = v - j * G::RW4;
-                    *(float4*)(stage + j * RWp + 4 * k4) = Quad<T>::cvt(pv[q]);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < G::RAWPT; q++) {
-                const int idx = tid + q * kStripThreads;
-                if (idx < G::RAWN) stage[idx] = ps_[q];
-            }
-        }
+        raw.store(stage, vec);
         __syncthreads();
-        if (s + 1 < nsteps) load_raw(s + 1);
+        if (s + 1 < nsteps) raw.load(img, H, W, x0, xa, vec, s + 1);
 
         // ---- B: row pass (preprocess_rows.wgsl), 8 rows x PWp columns, 4 per thread
         for (int t = tid; t < kStepRows * G::NG; t += kStripThreads) {
@@ -762,75 +750,16 @@ __device__ __forceinline__ void ring_tile(const T* __restrict__ img, float* __re
         });
         __syncthreads();
 
-        // ---- E: horizontal maximum and the candidate test (extract_max.wgsl);
-        // the processed rows of the segment go to HBM from here, 4 columns
-        // per thread
-        {
-            int cnt = 0;
-            uint32_t cmask = 0;
-            int cd = 0, ccol = 0;
-            if (tid < kStepRows * (kStripTW / 4)) {
-                const int jj = tid / (kStripTW / 4), cg = tid - jj * (kStripTW / 4);
-                const int d = dbase + jj;
-                const int cc = 4 * cg;  // interior column offset; processed column = cc + O (pc0-relative)
-                if (d >= R0 && d < R1) {
-                    const float4* src = (const float4*)(vb + jj * PWp + cc);
-                    float a[4 * G::NV4];
-#pragma unroll
-                    for (int i = 0; i < G::NV4; i++) {
-                        const float4 v = src[i];
-                        a[4 * i] = v.x;
-                        a[4 * i + 1] = v.y;
-                        a[4 * i + 2] = v.z;
-                        a[4 * i + 3] = v.w;
-                    }
-                    const float mid = Tree<KD - 3>::max(a + 3);
-                    float s2 = a[2], s1 = fmaxf(a[1], s2), s0 = fmaxf(a[0], s1);
-                    float p1 = a[KD], p2 = fmaxf(p1, a[KD + 1]), p3 = fmaxf(p2, a[KD + 2]);
-                    float m[4] = {fmaxf(s0, mid), fmaxf(fmaxf(s1, mid), p1), fmaxf(fmaxf(s2, mid), p2),
-                                  fmaxf(mid, p3)};
-                    int prow = P8 + jj - E;   // ring row of processed row d
-                    if (prow < 0) prow += RING;
-                    const float* cen = pr + prow * PWp + SH4 + O + cc;
-                    float cv[4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) cv[k] = cen[k];
-                    const int gc0 = c0 + cc;
-                    float* dst = proc + (size_t)d * W + gc0;
-                    if (st4 && gc0 + 3 < W) {
-                        *(float4*)dst = make_float4(cv[0], cv[1], cv[2], cv[3]);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 4; k++)
-                            if (gc0 + k < W) dst[k] = cv[k];
-                    }
-                    // the test of every column without branches; columns
-                    // and rows inside the margin need no bounds test
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        const float center = cv[k];
-                        bool ok = !(center < thr) && !(m[k] > center);
-                        if (c.skip_zero) ok = ok && (center != 0.0f);
-                        cmask |= (uint32_t)ok << k;
-                    }
-                    const bool inner = d >= c.margin && d < H - c.margin && gc0 >= c.margin &&
-                                       gc0 + 3 < W - c.margin;
-                    if (!inner) {
-#pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            const int gc = gc0 + k;
-                            if (gc >= W || d < c.margin || d >= H - c.margin || gc < c.margin ||
-                                gc >= W - c.margin)
-                                cmask &= ~(1u << k);
-                        }
-                    }
-                    cnt = __popc(cmask);
-                    cd = d;
-                    ccol = gc0;
-                }
-            }
-            append_cands(tid, cnt, cmask, cd, ccol, W, cbuf_n, cbuf, cand_slot, cout, cand_cap, flags);
-        }
+        // ---- E: horizontal maximum, the candidate test and the processed rows
+        // (processed row d = dbase + jj is ring row 8 * phase + jj - E, mod RING)
+        extract_step<R, KD>(tid, vb,
+                            [&](int jj) {
+                                int prow = P8 + jj - E;
+                                if (prow < 0) prow += RING;
+                                return pr + prow * PWp;
+                            },
+                            dbase, R0, R1, c0, H, W, c, thr, st4, proc, cbuf_n, cbuf, cand_slot, cout, cand_cap,
+                            flags);
         __syncthreads();
         phase = (phase + 1 == PER) ? 0 : phase + 1;
     }
