@@ -36,6 +36,7 @@ namespace {
 
 constexpr int kSSTH = 16, kSSTW = 128, kSSThreads = 256;
 constexpr int kSSCB = 5;                 // pass B columns per task ((TW + 2) = 26 * 5)
+constexpr int kSSBatch = 8;              // raw-tile loads a thread keeps in flight
 static_assert((kSSTW + 2) % kSSCB == 0, "pass B column blocks");
 constexpr int kSSPW = kSSTW + 2;         // plane tile width (tile +- 1)
 constexpr int kSSPH = kSSTH + 2;
@@ -264,14 +265,24 @@ log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const
         stg[i] = taps_g[i];
         std_[i] = taps_d[i];
     }
-    // raw tile: rows r0 - 1 - RMAX .., columns c0 - 1 - RMAX .., zero outside the frame
+    // raw tile: rows r0 - 1 - RMAX .., columns c0 - 1 - RMAX .., zero outside
+    // the frame; kSSBatch independent loads per thread are in flight before
+    // their shared-memory stores
     const int gr0 = r0 - 1 - rmax, gc0 = c0 - 1 - rmax;
-    for (int rr = 0; rr < g.RH; rr++) {
-        const int gr = gr0 + rr;
-        const bool row_in = gr >= 0 && gr < H;
-        for (int cc = threadIdx.x; cc < g.RW; cc += kSSThreads) {
-            const int gc = gc0 + cc;
-            raw[rr * g.RW + cc] = (row_in && gc >= 0 && gc < W) ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+    const int nraw = g.RH * g.RW;
+    for (int i0 = 0; i0 < nraw; i0 += kSSBatch * kSSThreads) {
+        float v[kSSBatch];
+#pragma unroll
+        for (int b = 0; b < kSSBatch; b++) {
+            const int i = i0 + b * kSSThreads + threadIdx.x;
+            const int rr = i / g.RW, cc = i - rr * g.RW;
+            const int gr = gr0 + rr, gc = gc0 + cc;
+            v[b] = (i < nraw && gr >= 0 && gr < H && gc >= 0 && gc < W) ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+        }
+#pragma unroll
+        for (int b = 0; b < kSSBatch; b++) {
+            const int i = i0 + b * kSSThreads + threadIdx.x;
+            if (i < nraw) raw[i] = v[b];
         }
     }
     __syncthreads();
