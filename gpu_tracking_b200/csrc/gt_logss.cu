@@ -40,9 +40,12 @@ constexpr int kSSBatch = 8;              // raw-tile loads a thread keeps in fli
 static_assert((kSSTW + 2) % kSSCB == 0, "pass B column blocks");
 constexpr int kSSPW = kSSTW + 2;         // plane tile width (tile +- 1)
 constexpr int kSSPH = kSSTH + 2;
+// row stride of the raw tile and the pass A planes: fixed for every largest
+// radius, so the vertical pass's tap loads are constant offsets
+constexpr int kSSRW = kSSPW + 2 * kLogSSMaxR;
 
 struct SSGeom {
-    int RMAX, RH, RW;   // raw tile: RH x RW, also the row stride of the pass A planes
+    int RMAX, RH, RW;   // raw tile: RH rows of RW used columns (row stride kSSRW, as the pass A planes)
     size_t off_a, off_b, off_ring, off_taps, floats;
 };
 
@@ -51,9 +54,9 @@ __host__ __device__ inline SSGeom ss_geom(int rmax, int ntaps_total) {
     g.RMAX = rmax;
     g.RH = kSSPH + 2 * rmax;
     g.RW = kSSPW + 2 * rmax;
-    g.off_a = (size_t)g.RH * g.RW;
-    g.off_b = g.off_a + (size_t)kSSPH * g.RW;
-    g.off_ring = g.off_b + (size_t)kSSPH * g.RW;
+    g.off_a = (size_t)g.RH * kSSRW;
+    g.off_b = g.off_a + (size_t)kSSPH * kSSRW;
+    g.off_ring = g.off_b + (size_t)kSSPH * kSSRW;
     g.off_taps = g.off_ring + 3 * (size_t)kSSPH * kSSPW;
     g.floats = g.off_taps + 2 * (size_t)ntaps_total;
     return g;
@@ -99,7 +102,7 @@ __device__ __forceinline__ void ss_pass_a(const float* __restrict__ raw, const S
         const int col = task - grp * ncols;
         const int u0 = grp * kSSRG;
         // plane row u0 + k, column col <-> raw row u0 + k + RMAX - R + i, raw column col + RMAX - R
-        const float* src = raw + (size_t)(u0 + g.RMAX - R) * g.RW + (col + g.RMAX - R);
+        const float* src = raw + (size_t)(u0 + g.RMAX - R) * kSSRW + (col + g.RMAX - R);
         float aa[kSSRG], bb[kSSRG];
 #pragma unroll
         for (int k = 0; k < kSSRG; k++) aa[k] = bb[k] = 0.0f;
@@ -109,7 +112,7 @@ __device__ __forceinline__ void ss_pass_a(const float* __restrict__ raw, const S
             float x[NXC];
 #pragma unroll
             for (int m = 0; m < NXC; m++)
-                if (i0 + m < NT + kSSRG - 1) x[m] = src[(i0 + m) * g.RW];
+                if (i0 + m < NT + kSSRG - 1) x[m] = src[(i0 + m) * kSSRW];
 #pragma unroll
             for (int ii = 0; ii < kSSChunk; ii++) {
                 if (i0 + ii < NT) {
@@ -124,8 +127,8 @@ __device__ __forceinline__ void ss_pass_a(const float* __restrict__ raw, const S
         }
 #pragma unroll
         for (int k = 0; k < kSSRG; k++) {
-            sa[(u0 + k) * g.RW + col] = __fmul_rn(aa[k], nd);
-            sb[(u0 + k) * g.RW + col] = __fmul_rn(bb[k], ng);
+            sa[(u0 + k) * kSSRW + col] = __fmul_rn(aa[k], nd);
+            sb[(u0 + k) * kSSRW + col] = __fmul_rn(bb[k], ng);
         }
     }
 }
@@ -166,8 +169,8 @@ __device__ __forceinline__ void ss_pass_b(const float* __restrict__ sa, const fl
         const int v0 = (task - u * NB) * kSSCB;
         // plane column v, tap j <-> pass A column v + j
         float ra[kSSCB], rb[kSSCB];
-        ss_hchain<R>(sa + (size_t)u * g.RW + v0, tg, ra);
-        ss_hchain<R>(sb + (size_t)u * g.RW + v0, td, rb);
+        ss_hchain<R>(sa + (size_t)u * kSSRW + v0, tg, ra);
+        ss_hchain<R>(sb + (size_t)u * kSSRW + v0, td, rb);
 #pragma unroll
         for (int c = 0; c < kSSCB; c++) {
             float L = __fsub_rn(0.0f, __fmul_rn(ra[c], ng));
@@ -282,7 +285,8 @@ log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const
 #pragma unroll
         for (int b = 0; b < kSSBatch; b++) {
             const int i = i0 + b * kSSThreads + threadIdx.x;
-            if (i < nraw) raw[i] = v[b];
+            const int rr = i / g.RW, cc = i - rr * g.RW;
+            if (i < nraw) raw[rr * kSSRW + cc] = v[b];
         }
     }
     __syncthreads();
