@@ -1313,20 +1313,50 @@ finalize_kernel(const Feature* __restrict__ feats, const uint32_t* __restrict__ 
         block_sort_u64(keys, np2);
         for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = (int32_t)(keys[i] & 0xFFFFFFull);
         __syncthreads();
-        // prune_blobs_log (src/execute_gpu.rs:592-669): greedy in priority order
-        for (int q = 0; q < n; q++) {
-            if (!keep[q]) continue;  // uniform: keep[] only changes between barriers
-            const Feature& Q = F[perm[order[q]]];
-            const float qr = __fmul_rn(Q.r, 2.0f);
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                if (j == q || !keep[j]) continue;
-                const Feature& Nb = F[perm[order[j]]];
-                float d2;
-                if (!within_rd2(Nb.x, Nb.y, Q.x, Q.y, qr, &d2)) continue;
-                float ov = blob_overlap(Q.r, Nb.r, __fsqrt_rn(d2));
-                if (ov > fc.overlap_threshold) keep[j] = 0;
+        // prune_blobs_log (src/execute_gpu.rs:592-669): greedy in priority
+        // order, one step per kept blob.  Positions and radii in priority
+        // order sit in shared memory when they fit, so a step's scan reads no
+        // global memory.
+        const bool pr_smem = np2 <= kFinalizeSmemSort && n <= kFinalizeFcSmem;
+        if (pr_smem) {
+            float* const bx = (float*)((uint8_t*)fsm + finalize_smem_core_bytes());
+            float* const by = bx + kFinalizeFcSmem;
+            float* const br = by + kFinalizeFcSmem;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const Feature& ft = F[perm[order[i]]];
+                bx[i] = ft.x;
+                by[i] = ft.y;
+                br[i] = ft.r;
             }
             __syncthreads();
+            for (int q = 0; q < n; q++) {
+                if (!keep[q]) continue;  // uniform: keep[] only changes between barriers
+                const float Qx = bx[q], Qy = by[q], Qr = br[q];
+                const float qr = __fmul_rn(Qr, 2.0f);
+                for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                    if (j == q || !keep[j]) continue;
+                    float d2;
+                    if (!within_rd2(bx[j], by[j], Qx, Qy, qr, &d2)) continue;
+                    float ov = blob_overlap(Qr, br[j], __fsqrt_rn(d2));
+                    if (ov > fc.overlap_threshold) keep[j] = 0;
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int q = 0; q < n; q++) {
+                if (!keep[q]) continue;  // uniform: keep[] only changes between barriers
+                const Feature& Q = F[perm[order[q]]];
+                const float qr = __fmul_rn(Q.r, 2.0f);
+                for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                    if (j == q || !keep[j]) continue;
+                    const Feature& Nb = F[perm[order[j]]];
+                    float d2;
+                    if (!within_rd2(Nb.x, Nb.y, Q.x, Q.y, qr, &d2)) continue;
+                    float ov = blob_overlap(Q.r, Nb.r, __fsqrt_rn(d2));
+                    if (ov > fc.overlap_threshold) keep[j] = 0;
+                }
+                __syncthreads();
+            }
         }
     }
 
