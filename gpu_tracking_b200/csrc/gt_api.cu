@@ -301,9 +301,10 @@ struct PipeLink {
     int64_t C = 0, list_cap = 0, max_items = 0;
     size_t scan_bytes = 0;
     int64_t nwin = 0;   // windows issued in this call
+    float bin_w = 1.0f;  // row-bin width of the neighbour search index
 
     gt_status setup(gt_ctx* c, int64_t NT, uint32_t feat_cap, int SC, float radius, int memory,
-                    const std::vector<uint8_t>& reset) {
+                    const std::vector<uint8_t>& reset, int32_t H) {
         ctx = c;
         C = feat_cap;
         K = memory + 1;
@@ -313,6 +314,11 @@ struct PipeLink {
         if (ctx->w_edge_cap <= 0) ctx->w_edge_cap = std::max<int64_t>(C * 16, 1 << 16);
         list_cap = ctx->w_list_cap;
         CK(ctx->w_srt.ensure(NS * 4));
+        // row bins of at least the search radius over the frame height: a
+        // neighbour search reads two bin offsets and scans about three bins
+        CK(ctx->w_bins.ensure((size_t)NT * (kLinkRowBins + 1) * 4));
+        bin_w = std::max(radius, (float)H / (float)kLinkRowBins);
+        if (!(bin_w > 0.0f) || !std::isfinite(bin_w)) bin_w = 1.0f;
         // the previous call's list kernels may still read the buffers
         CK(cudaStreamSynchronize(ctx->ls));
         for (int b = 0; b < 2; b++) {
@@ -397,7 +403,7 @@ struct PipeLink {
         uint32_t* srt = ctx->w_srt.as<uint32_t>();
         {
             Prof pf(ctx, "link_sort", ctx->ls);
-            CK(link_sort_groups_range(in, srt, s0, s1, ctx->ls));
+            CK(link_sort_groups_range(in, srt, s0, s1, ctx->w_bins.as<int32_t>(), bin_w, ctx->ls));
         }
         int64_t* fcnt = ctx->w_fcnt[b].as<int64_t>();
         int64_t* bcnt = ctx->w_bcnt[b].as<int64_t>();
@@ -417,6 +423,8 @@ struct PipeLink {
         L.b_pts = ctx->w_bpts[b].as<int32_t>();
         L.b_dist = ctx->w_bdist[b].as<float>();
         L.srt = srt;
+        L.bins = ctx->w_bins.as<int32_t>();
+        L.bin_w = bin_w;
         L.pbase = p0;
         L.f_cap = list_cap;
         L.b_cap = list_cap;
@@ -559,7 +567,7 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
     CK(cudaMemsetAsync(ctx->flags.p, 0, 16, ctx->st));
     CK(ctx->walk_starts.ensure(8));
     CK(cudaMemsetAsync(ctx->walk_starts.p, 0, 8, ctx->st));
-    if (pl) CKS(pl->setup(ctx, NT, feat_cap, SC, p.search_range, (int)p.memory, *reset));
+    if (pl) CKS(pl->setup(ctx, NT, feat_cap, SC, p.search_range, (int)p.memory, *reset, H));
     // finalize scratch for frames with more detections than shared memory sorts
     size_t fin_per_frame = 0;
     if (feat_cap > (uint32_t)kFinalizeSmemSort) {

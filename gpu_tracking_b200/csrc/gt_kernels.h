@@ -10,6 +10,7 @@
 namespace gt {
 
 constexpr int kMaxRadii = 256;
+constexpr int kLinkRowBins = 512;   // row bins per group of the windowed linker's neighbour search
 
 struct FinalizeConsts {
     int32_t H, W;
@@ -257,6 +258,12 @@ struct LinkLists {
     int64_t pbase = 0;            // first point the offset arrays cover
     int64_t f_cap = -1, b_cap = -1;  // entries f_pts / b_pts hold (-1: sized exactly)
     int64_t f_entries = -1;          // forward entries of lists sized exactly (-1: not known)
+    // optional row-bin index of the sorted groups: for group g, entry
+    // g * (kLinkRowBins + 1) + b is the first sorted position whose row falls
+    // in bin b or later (bin = clamp(floor(row / bin_w), 0, kLinkRowBins - 1),
+    // rows that are NaN after every bin); nullptr = bisect the rows instead
+    const int32_t* bins = nullptr;
+    float bin_w = 0.0f;
 };
 
 struct LinkScratch {
@@ -292,7 +299,9 @@ struct LinkOutput {
 cudaError_t link_sort_groups(const LinkInput& in, uint32_t* srt, uint8_t* scratch, size_t scratch_per_group,
                              int max_group, cudaStream_t st);
 // groups [g0, g1) only
-cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, cudaStream_t st);
+// groups [g0, g1) only; with bins, also their row-bin index (LinkLists::bins)
+cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, int32_t* bins, float bin_w,
+                                   cudaStream_t st);
 cudaError_t link_count_lists(const LinkInput& in, const uint32_t* srt, int64_t* f_cnt, int64_t* b_cnt,
                              cudaStream_t st);
 cudaError_t link_fill_lists(const LinkInput& in, const LinkLists& L, cudaStream_t st);

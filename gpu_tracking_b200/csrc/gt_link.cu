@@ -68,13 +68,27 @@ __device__ __forceinline__ int64_t lix(const LinkLists& L, int64_t p, int K, int
 }
 
 // ------------------------------------------------------------ group sorting
+// Row bin of a row key (monotone in the row; NaN after every bin).
+__device__ __forceinline__ int row_bin(float row, float bin_w) {
+    if (row != row) return kLinkRowBins;
+    const float t = floorf(__fdiv_rn(row, bin_w));
+    if (!(t >= 0.0f)) return 0;
+    if (t >= (float)(kLinkRowBins - 1)) return kLinkRowBins - 1;
+    return (int)t;
+}
+
 __global__ void __launch_bounds__(kLinkThreads)
 sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restrict__ scratch, size_t per_group,
-                   int g0) {
+                   int g0, int32_t* __restrict__ bins, float bin_w) {
     __shared__ uint64_t sk[kSortSmem];
     const int g = g0 + blockIdx.x;
     const int64_t a = gbase(in, g), n = gsize(in, g);
-    if (n == 0) return;
+    int32_t* const off = bins ? bins + (size_t)g * (kLinkRowBins + 1) : nullptr;
+    if (n == 0) {
+        if (off)
+            for (int b = threadIdx.x; b <= kLinkRowBins; b += blockDim.x) off[b] = 0;
+        return;
+    }
     int np2 = 1;
     while (np2 < n) np2 <<= 1;
     uint64_t* keys = (np2 <= kSortSmem) ? sk : scratch + (size_t)blockIdx.x * per_group;
@@ -83,11 +97,33 @@ sort_groups_kernel(LinkInput in, uint32_t* __restrict__ srt, uint64_t* __restric
     __syncthreads();
     block_sort_u64(keys, np2);
     for (int i = threadIdx.x; i < n; i += blockDim.x) srt[a + i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
+    if (off) {
+        // off[b] = first sorted position whose bin is >= b: position i writes
+        // the bins in (bin(i - 1), bin(i)], position n those up to the end
+        auto bin_at = [&](int64_t i) -> int {
+            if (i >= n) return kLinkRowBins;
+            return row_bin(float_from_order_key((uint32_t)(keys[i] >> 32)), bin_w);
+        };
+        for (int64_t i = threadIdx.x; i <= n; i += blockDim.x) {
+            const int prev = i == 0 ? -1 : bin_at(i - 1), cur = bin_at(i);
+            for (int b = prev + 1; b <= cur; b++) off[b] = (int32_t)i;
+        }
+    }
 }
 
-// First sorted position of group t whose row key is >= klo, and first > khi.
-__device__ __forceinline__ void row_range(const LinkInput& in, const uint32_t* srt, int t, float lo, float hi,
+// Sorted positions [p0, p1) of group t that hold every row in [lo, hi]: the
+// first position whose row key is >= klo and the first > khi, or, with the
+// row-bin index, the positions of the bins that lo and hi fall in (a few
+// more rows, which the exact distance test rejects).
+__device__ __forceinline__ void row_range(const LinkInput& in, const LinkLists& L, int t, float lo, float hi,
                                           int64_t* p0, int64_t* p1) {
+    if (L.bins) {
+        const int32_t* off = L.bins + (size_t)t * (kLinkRowBins + 1);
+        *p0 = off[row_bin(lo, L.bin_w)];
+        *p1 = off[row_bin(hi, L.bin_w) + 1];
+        return;
+    }
+    const uint32_t* srt = L.srt;
     const int64_t a = gbase(in, t), n = gsize(in, t);
     const uint32_t klo = float_order_key(lo), khi = float_order_key(hi);
     int64_t x = 0, y = n;
@@ -151,7 +187,7 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
         }
         if (t < ve && t < ready && !qnan && !skip) {
             int64_t s0, s1;
-            row_range(in, L.srt, t, lo, hi, &s0, &s1);
+            row_range(in, L, t, lo, hi, &s0, &s1);
             const int64_t a = gbase(in, t);
             int32_t* out = kMode ? L.f_pts + L.f_off[lix(L, p, K, k - 1)] : nullptr;
             for (int64_t m = s0; m < s1; m++) {
@@ -182,7 +218,7 @@ __global__ void lists_kernel(LinkInput in, LinkLists L, int64_t* f_cnt, int64_t*
         }
         if (t >= vb && !qnan && !skip) {
             int64_t s0, s1;
-            row_range(in, L.srt, t, lo, hi, &s0, &s1);
+            row_range(in, L, t, lo, hi, &s0, &s1);
             const int64_t a = gbase(in, t);
             int32_t* out = kMode ? L.b_pts + L.b_off[lix(L, p, K, k - 1)] : nullptr;
             float* outd = kMode ? L.b_dist + L.b_off[lix(L, p, K, k - 1)] : nullptr;
@@ -980,15 +1016,18 @@ cudaError_t link_sort_groups(const LinkInput& in, uint32_t* srt, uint8_t* scratc
                              int max_group, cudaStream_t st) {
     (void)max_group;
     if (in.ngroups == 0) return cudaSuccess;
-    sort_groups_kernel<<<in.ngroups, kLinkThreads, 0, st>>>(in, srt, (uint64_t*)scratch, scratch_per_group / 8, 0);
+    sort_groups_kernel<<<in.ngroups, kLinkThreads, 0, st>>>(in, srt, (uint64_t*)scratch, scratch_per_group / 8, 0,
+                                                           nullptr, 0.0f);
     return cudaGetLastError();
 }
 
-cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, cudaStream_t st) {
+cudaError_t link_sort_groups_range(const LinkInput& in, uint32_t* srt, int g0, int g1, int32_t* bins, float bin_w,
+                                   cudaStream_t st) {
     if (g1 <= g0) return cudaSuccess;
     // groups of at most kSortSmem points sort in shared memory; no scratch
     if (in.slot_stride > kSortSmem) return cudaErrorInvalidValue;
-    sort_groups_kernel<<<g1 - g0, kLinkThreads, 0, st>>>(in, srt, nullptr, 0, g0);
+    if (bins && !(bin_w > 0.0f)) return cudaErrorInvalidValue;
+    sort_groups_kernel<<<g1 - g0, kLinkThreads, 0, st>>>(in, srt, nullptr, 0, g0, bins, bin_w);
     return cudaGetLastError();
 }
 

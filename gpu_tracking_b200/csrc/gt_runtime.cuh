@@ -149,7 +149,7 @@ struct gt_ctx {
     DBuf vd_src, vd_dec, vd_blk, vd_bad;  // video files decoded on the device: streams, bytes, blocks, flag
     int64_t last_walk_starts = 0;
     int32_t illum_rint = 0;
-    DBuf w_srt, w_scan, w_scratch, w_ids, w_dur, w_state, w_cnt, w_flags, w_vgrp, w_reset;
+    DBuf w_srt, w_bins, w_scan, w_scratch, w_ids, w_dur, w_state, w_cnt, w_flags, w_vgrp, w_reset;
     // two sets of window neighbour lists: the lists of window w + 1 are built
     // while the linker reads those of window w
     DBuf w_fcnt[2], w_bcnt[2], w_foff[2], w_boff[2], w_fpts[2], w_bpts[2], w_bdist[2];
