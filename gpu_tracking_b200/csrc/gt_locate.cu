@@ -451,7 +451,9 @@ walk_kernel_fixed(const float* __restrict__ processed, const T* __restrict__ fra
                   const uint32_t* __restrict__ cand_keys, uint32_t cand_cap, const int32_t* __restrict__ angle_off,
                   const float2* __restrict__ angles, Feature* __restrict__ feats, uint32_t* __restrict__ feat_count,
                   uint32_t feat_cap, uint32_t* __restrict__ flags, const RaggedFrame* __restrict__ rf) {
-    const int f = blockIdx.y;
+    // frames in reverse order: the strip kernel wrote the last frames' processed
+    // images last, so the first blocks find them in L2
+    const int f = gridDim.y - 1 - blockIdx.y;
     const uint32_t n = min(cand_count[f], cand_cap);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1078,9 +1080,11 @@ __device__ __forceinline__ float warp_upper_median_regs(const T* __restrict__ ra
         key[q] = 0xFFFFFFFFu;  // never below a trial value: left out of every count
         if (k < n_inds) {
             const short2 d = inds[k];
-            const int64_t a = (int64_t)mu + d.x, b = (int64_t)mv + d.y;
-            if (a >= 0 && a < H && b >= 0 && b < W) {
-                key[q] = MedKey<T>::key(raw, (size_t)a * W + b);
+            // 32-bit row / column tests (wrapping unsigned sums: a negative or
+            // saturated centre fails them) and index (frames hold < 2^31 pixels)
+            const uint32_t a = (uint32_t)mu + (uint32_t)(int32_t)d.x, b = (uint32_t)mv + (uint32_t)(int32_t)d.y;
+            if (a < (uint32_t)H && b < (uint32_t)W) {
+                key[q] = MedKey<T>::key(raw, a * (uint32_t)W + b);
                 kor |= key[q];
                 kand &= key[q];
                 nv++;
@@ -1135,9 +1139,10 @@ __device__ __forceinline__ void doughnut_warp(const T* __restrict__ raw, int H, 
             bool ok = false;
             if (k < n_sig) {
                 const short2 d = sig[k];
-                const int64_t a = (int64_t)mu + d.x, bb = (int64_t)mv + d.y;
-                ok = (a >= 0 && a < H && bb >= 0 && bb < W);
-                if (ok) acc += (uint32_t)load_px<T>(raw, (size_t)a * W + bb);
+                const uint32_t a = (uint32_t)mu + (uint32_t)(int32_t)d.x;
+                const uint32_t bb = (uint32_t)mv + (uint32_t)(int32_t)d.y;
+                ok = a < (uint32_t)H && bb < (uint32_t)W;
+                if (ok) acc += (uint32_t)load_px<T>(raw, a * (uint32_t)W + bb);
             }
             nsig += __popc(__ballot_sync(0xffffffffu, ok));
         }
