@@ -4,6 +4,7 @@
 // public interface is include/gpu_tracking_b200.h.
 #pragma once
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda.h>
 
 #include <algorithm>
@@ -223,12 +224,16 @@ inline gt_status set_err(gt_ctx* ctx, gt_status st, const char* fmt, ...) {
 // --------------------------------------------------------------- profiling
 // Counts every kernel launch of the engine; with profiling enabled also
 // brackets it with CUDA events on the compute stream.
+// Every Prof and HostSpan is also an NVTX range under its name (header-only
+// NVTX v3: the ranges cost a branch unless a profiler such as Nsight Systems
+// is attached, which then shows each stage's launches and host phases).
 struct Prof {
     gt_ctx* ctx;
     const char* name;
     cudaStream_t stream;
     cudaEvent_t a = nullptr, b = nullptr;
     Prof(gt_ctx* c, const char* n, cudaStream_t s = nullptr) : ctx(c), name(n), stream(s ? s : c->st) {
+        nvtxRangePushA(name);
         ctx->launch_count[name]++;
         if (!ctx->profile) return;
         a = take();
@@ -246,6 +251,7 @@ struct Prof {
         return e;
     }
     ~Prof() {
+        nvtxRangePop();
         if (!ctx->profile) return;
         cudaEventRecord(b, stream);
         ctx->pending.push_back({name, {a, b}});
@@ -259,8 +265,11 @@ struct HostSpan {
     gt_ctx* ctx;
     const char* name;
     std::chrono::steady_clock::time_point t0;
-    HostSpan(gt_ctx* c, const char* n) : ctx(c), name(n), t0(std::chrono::steady_clock::now()) {}
+    HostSpan(gt_ctx* c, const char* n) : ctx(c), name(n), t0(std::chrono::steady_clock::now()) {
+        nvtxRangePushA(name);
+    }
     ~HostSpan() {
+        nvtxRangePop();
         if (!ctx->profile) return;
         auto& s = ctx->stats[name];
         s.launches++;
