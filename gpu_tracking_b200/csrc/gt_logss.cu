@@ -35,7 +35,7 @@ namespace gt {
 namespace {
 
 constexpr int kSSTH = 16, kSSTW = 128, kSSThreads = 256;
-constexpr int kSSCB = 5;                 // pass B columns per task ((TW + 2) = 26 * 5)
+constexpr int kSSCB = 10;                // pass B columns per task ((TW + 2) = 13 * 10: one round of 234 tasks)
 constexpr int kSSBatch = 8;              // raw-tile loads a thread keeps in flight
 static_assert((kSSTW + 2) % kSSCB == 0, "pass B column blocks");
 constexpr int kSSPW = kSSTW + 2;         // plane tile width (tile +- 1)
