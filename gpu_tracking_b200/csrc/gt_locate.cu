@@ -44,14 +44,29 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
     float* sv = sp + PH * PW;
     const int tid = threadIdx.x;
 
-    // raw tile with clamp-to-edge addressing (the boxcar's addressing)
-    for (int idx = tid; idx < XH * RW; idx += blockDim.x) {
-        int rr = idx / RW, cc = idx - rr * RW;
-        int gr = min(max(xr0 + rr, 0), H - 1);
-        int gc = min(max(rc0 + cc, 0), W - 1);
-        sraw[idx] = load_px<T>(img, (size_t)gr * W + gc);
+    // raw tile with clamp-to-edge addressing (the boxcar's addressing); 8
+    // independent loads per thread in flight before their shared-memory stores
+    for (int i0 = 0; i0 < XH * RW; i0 += 8 * (int)blockDim.x) {
+        float v[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int idx = i0 + b * (int)blockDim.x + tid;
+            const int rr = idx / RW, cc = idx - rr * RW;
+            const int gr = min(max(xr0 + rr, 0), H - 1);
+            const int gc = min(max(rc0 + cc, 0), W - 1);
+            v[b] = idx < XH * RW ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+        }
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int idx = i0 + b * (int)blockDim.x + tid;
+            if (idx < XH * RW) sraw[idx] = v[b];
+        }
     }
     __syncthreads();
+    // a tile whose raw rows and columns all lie inside the frame needs no
+    // per-tap bounds tests or clamps (every tap counts, every clamp is the
+    // identity: the same operation sequence)
+    const bool inside = xr0 >= 0 && xr0 + XH <= H && rc0 >= 0 && rc0 + RW <= W;
 
     // preprocess_rows.wgsl:30-54 — Gaussian taps skip out-of-frame columns,
     // the boxcar sums clamped columns; temp = (g / gauss_norm, box)
@@ -60,11 +75,19 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
         const float* rowp = sraw + rr * RW + cc;
         const int gcol = pc0 + cc;
         float gs = 0.0f, cs = 0.0f;
-        for (int i = 0; i <= 2 * R; i++) {
-            float x = rowp[i];
-            int gc = gcol + i - R;
-            if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
-            cs = __fadd_rn(cs, x);
+        if (inside) {
+            for (int i = 0; i <= 2 * R; i++) {
+                const float x = rowp[i];
+                gs = __fmaf_rn(c.taps[i], x, gs);
+                cs = __fadd_rn(cs, x);
+            }
+        } else {
+            for (int i = 0; i <= 2 * R; i++) {
+                float x = rowp[i];
+                int gc = gcol + i - R;
+                if (gc >= 0 && gc < W) gs = __fmaf_rn(c.taps[i], x, gs);
+                cs = __fadd_rn(cs, x);
+            }
         }
         sxg[idx] = __fdiv_rn(gs, c.gnorm);
         sxb[idx] = cs;
@@ -81,13 +104,23 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
             continue;
         }
         float gs = 0.0f, cs = 0.0f;
-        for (int i = 0; i <= 2 * R; i++) {
-            int gr = grow + i - R;
-            int xrow = min(max(gr, 0), H - 1) - xr0;
-            float xg = sxg[xrow * PW + pc];
-            float xb = sxb[xrow * PW + pc];
-            if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], xg, gs);
-            cs = __fadd_rn(cs, xb);
+        if (inside) {
+            // rows grow - R .. grow + R are raw rows pr .. pr + 2R of the tile
+            const float* pg = sxg + pr * PW + pc;
+            const float* pb = sxb + pr * PW + pc;
+            for (int i = 0; i <= 2 * R; i++) {
+                gs = __fmaf_rn(c.taps[i], pg[i * PW], gs);
+                cs = __fadd_rn(cs, pb[i * PW]);
+            }
+        } else {
+            for (int i = 0; i <= 2 * R; i++) {
+                int gr = grow + i - R;
+                int xrow = min(max(gr, 0), H - 1) - xr0;
+                float xg = sxg[xrow * PW + pc];
+                float xb = sxb[xrow * PW + pc];
+                if (gr >= 0 && gr < H) gs = __fmaf_rn(c.taps[i], xg, gs);
+                cs = __fadd_rn(cs, xb);
+            }
         }
         float res = __fsub_rn(__fdiv_rn(gs, c.gnorm), __fdiv_rn(cs, c.kk));
         if (c.truncate && res < trunc_thr) res = 0.0f;
