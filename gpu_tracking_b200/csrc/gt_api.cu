@@ -778,7 +778,8 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                                                      loff.as<int32_t>(), lrint.as<int32_t>(), lng.as<float>(),
                                                      lnd.as<float>(), lt->max_rint, (int)lt->taps_g.size(), nf,
                                                      ctx->cand_count.as<uint32_t>(), ctx->cand_keys.as<uint32_t>(),
-                                                     cand_cap, flags, ctx->st));
+                                                     cand_cap, flags, lt->taps_g.data(), lt->taps_d.data(),
+                                                     lt->tap_off.data(), lt->rints.data(), ctx->st));
                     } else {
                         {
                             Prof pf(ctx, "laplace");

@@ -215,7 +215,8 @@ cudaError_t launch_log_scale_space(const T* frames, int64_t frame_stride, const 
                                    const float* taps_g, const float* taps_d, const int32_t* tap_off,
                                    const int32_t* rints, const float* norm_g, const float* norm_d, int max_rint,
                                    int ntaps_total, int nframes, uint32_t* cand_count, uint32_t* cand_keys,
-                                   uint32_t cand_cap, uint32_t* flags, cudaStream_t st);
+                                   uint32_t cand_cap, uint32_t* flags, const float* h_taps_g, const float* h_taps_d,
+                                   const int32_t* h_tap_off, const int32_t* h_rints, cudaStream_t st);
 
 // mean frame (src/execute_gpu.rs:819-847)
 template <typename T>

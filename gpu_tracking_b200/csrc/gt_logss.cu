@@ -44,6 +44,17 @@ constexpr int kSSPH = kSSTH + 2;
 // radius, so the vertical pass's tap loads are constant offsets
 constexpr int kSSRW = kSSPW + 2 * kLogSSMaxR;
 
+// Tap weights of every compile-time radius R (= rint) at offset R * R (radii
+// 0 .. R-1 take sum(2r + 1) = R^2 slots), passed as a kernel parameter: a tap
+// chain then reads its weights as constant-bank operands instead of one
+// shared-memory load per tap.  Usable when the radii of a call have distinct
+// rints (the host falls back to shared-memory taps otherwise).
+constexpr int kSSParamTaps = (kLogSSMaxR + 1) * (kLogSSMaxR + 1);
+struct SSTaps {
+    float g[kSSParamTaps];
+    float d[kSSParamTaps];
+};
+
 struct SSGeom {
     int RMAX, RH, RW;   // raw tile: RH rows of RW used columns (row stride kSSRW, as the pass A planes)
     size_t off_a, off_b, off_ring, off_taps, floats;
@@ -242,14 +253,14 @@ __device__ void ss_maxima(const float* __restrict__ ring, int km, int n, int f, 
     }
 }
 
-template <typename T>
+template <typename T, bool kPT>
 __global__ void __launch_bounds__(kSSThreads, 2)
 log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const float* __restrict__ processed,
                        const LogConsts lc, const float* __restrict__ taps_g, const float* __restrict__ taps_d,
                        const int32_t* __restrict__ tap_off, const int32_t* __restrict__ rints,
                        const float* __restrict__ norm_g, const float* __restrict__ norm_d, int rmax, int ntaps_total,
                        uint32_t* __restrict__ cand_count, uint32_t* __restrict__ cand_keys, uint32_t cand_cap,
-                       uint32_t* __restrict__ flags) {
+                       uint32_t* __restrict__ flags, const __grid_constant__ SSTaps tp) {
     extern __shared__ float4 ss_sm4[];
     float* sm = (float*)ss_sm4;
     const SSGeom g = ss_geom(rmax, ntaps_total);
@@ -264,10 +275,11 @@ log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const
     const int r0 = blockIdx.y * kSSTH, c0 = blockIdx.x * kSSTW;
     const T* img = frames + (size_t)f * frame_stride;
     const float* proc = processed + (size_t)f * H * W;
-    for (int i = threadIdx.x; i < ntaps_total; i += kSSThreads) {
-        stg[i] = taps_g[i];
-        std_[i] = taps_d[i];
-    }
+    if (!kPT)
+        for (int i = threadIdx.x; i < ntaps_total; i += kSSThreads) {
+            stg[i] = taps_g[i];
+            std_[i] = taps_d[i];
+        }
     // raw tile: rows r0 - 1 - RMAX .., columns c0 - 1 - RMAX .., zero outside
     // the frame; kSSBatch independent loads per thread are in flight before
     // their shared-memory stores
@@ -296,9 +308,12 @@ log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const
         const float* td = std_ + tap_off[k];
         float* plane = ring + (size_t)(k % 3) * kSSPH * kSSPW;
         switch (R) {
-#define GT_SS_CASE(RR)                                                            \
-    case RR:                                                                      \
-        ss_radius<RR>(raw, g, sa, sb, plane, tg, td, norm_g[k], norm_d[k]);       \
+#define GT_SS_CASE(RR)                                                                                 \
+    case RR:                                                                                           \
+        if (kPT)                                                                                       \
+            ss_radius<RR>(raw, g, sa, sb, plane, tp.g + RR * RR, tp.d + RR * RR, norm_g[k], norm_d[k]); \
+        else                                                                                           \
+            ss_radius<RR>(raw, g, sa, sb, plane, tg, td, norm_g[k], norm_d[k]);                        \
         break;
             GT_SS_CASES(GT_SS_CASE)
 #undef GT_SS_CASE
@@ -326,13 +341,39 @@ cudaError_t launch_log_scale_space(const T* frames, int64_t frame_stride, const 
                                    const float* taps_g, const float* taps_d, const int32_t* tap_off,
                                    const int32_t* rints, const float* norm_g, const float* norm_d, int max_rint,
                                    int ntaps_total, int nframes, uint32_t* cand_count, uint32_t* cand_keys,
-                                   uint32_t cand_cap, uint32_t* flags, cudaStream_t st) {
+                                   uint32_t cand_cap, uint32_t* flags, const float* h_taps_g, const float* h_taps_d,
+                                   const int32_t* h_tap_off, const int32_t* h_rints, cudaStream_t st) {
     dim3 grid((lc.W + kSSTW - 1) / kSSTW, (lc.H + kSSTH - 1) / kSSTH, nframes);
     const size_t smem = log_scale_space_smem_bytes(max_rint, ntaps_total);
-    cudaFuncSetAttribute(log_scale_space_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    log_scale_space_kernel<T><<<grid, kSSThreads, smem, st>>>(frames, frame_stride, processed, lc, taps_g, taps_d,
-                                                               tap_off, rints, norm_g, norm_d, max_rint, ntaps_total,
-                                                               cand_count, cand_keys, cand_cap, flags);
+    // taps as a kernel parameter when every radius has its own rint
+    static_assert(sizeof(SSTaps) + 512 <= 32764, "kernel parameters stay within the launch limit");
+    SSTaps tp;
+    bool param_taps = h_taps_g && h_taps_d && h_tap_off && h_rints;
+    uint64_t seen[(kLogSSMaxR + 64) / 64] = {};
+    for (int k = 0; param_taps && k < lc.n_radii; k++) {
+        const int R = h_rints[k];
+        if (R < 0 || R > kLogSSMaxR || (seen[R / 64] >> (R % 64) & 1u)) {
+            param_taps = false;
+            break;
+        }
+        seen[R / 64] |= 1ull << (R % 64);
+        for (int i = 0; i < 2 * R + 1; i++) {
+            tp.g[R * R + i] = h_taps_g[h_tap_off[k] + i];
+            tp.d[R * R + i] = h_taps_d[h_tap_off[k] + i];
+        }
+    }
+    if (param_taps) {
+        cudaFuncSetAttribute(log_scale_space_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        log_scale_space_kernel<T, true><<<grid, kSSThreads, smem, st>>>(
+            frames, frame_stride, processed, lc, taps_g, taps_d, tap_off, rints, norm_g, norm_d, max_rint, ntaps_total,
+            cand_count, cand_keys, cand_cap, flags, tp);
+    } else {
+        cudaFuncSetAttribute(log_scale_space_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        log_scale_space_kernel<T, false><<<grid, kSSThreads, smem, st>>>(
+            frames, frame_stride, processed, lc, taps_g, taps_d, tap_off, rints, norm_g, norm_d, max_rint, ntaps_total,
+            cand_count, cand_keys, cand_cap, flags, tp);
+    }
     return cudaGetLastError();
 }
 
@@ -340,7 +381,8 @@ cudaError_t launch_log_scale_space(const T* frames, int64_t frame_stride, const 
     template cudaError_t launch_log_scale_space<T>(const T*, int64_t, const float*, const LogConsts&, const float*, \
                                                    const float*, const int32_t*, const int32_t*, const float*,       \
                                                    const float*, int, int, int, uint32_t*, uint32_t*, uint32_t,      \
-                                                   uint32_t*, cudaStream_t);
+                                                   uint32_t*, const float*, const float*, const int32_t*,            \
+                                                   const int32_t*, cudaStream_t);
 GT_SS_INST(uint16_t)
 GT_SS_INST(float)
 GT_SS_INST(uint8_t)
