@@ -105,6 +105,27 @@ __device__ __forceinline__ float float_from_order_key(uint32_t k) {
 // WGSL max(a, b): b if a < b else a.
 __device__ __forceinline__ float wgsl_max(float a, float b) { return (a < b) ? b : a; }
 
+// Row and column of element idx = r * w + c of a tile whose width w is a
+// runtime value, stepped `step` elements at a time: two divisions when the
+// stepping starts instead of one per element.
+struct TileRowCol {
+    int r, c, dq, dr, w;
+    __device__ __forceinline__ TileRowCol(int idx, int step, int w_) : w(w_) {
+        r = idx / w;
+        c = idx - r * w;
+        dq = step / w;
+        dr = step - dq * w;
+    }
+    __device__ __forceinline__ void advance() {
+        r += dq;
+        c += dr;
+        if (c >= w) {
+            c -= w;
+            r++;
+        }
+    }
+};
+
 // Rust `f32 as i32` (saturating, NaN -> 0) and WGSL i32(f32) for finite values.
 __device__ __forceinline__ int32_t sat_f2i(float f) {
     if (f != f) return 0;

@@ -46,15 +46,16 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
 
     // raw tile with clamp-to-edge addressing (the boxcar's addressing); 8
     // independent loads per thread in flight before their shared-memory stores
+    TileRowCol rc(tid, (int)blockDim.x, RW);  // this thread's elements in order
     for (int i0 = 0; i0 < XH * RW; i0 += 8 * (int)blockDim.x) {
         float v[8];
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int idx = i0 + b * (int)blockDim.x + tid;
-            const int rr = idx / RW, cc = idx - rr * RW;
-            const int gr = min(max(xr0 + rr, 0), H - 1);
-            const int gc = min(max(rc0 + cc, 0), W - 1);
+            const int gr = min(max(xr0 + rc.r, 0), H - 1);
+            const int gc = min(max(rc0 + rc.c, 0), W - 1);
             v[b] = idx < XH * RW ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+            rc.advance();
         }
 #pragma unroll
         for (int b = 0; b < 8; b++) {
@@ -70,8 +71,9 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
 
     // preprocess_rows.wgsl:30-54 — Gaussian taps skip out-of-frame columns,
     // the boxcar sums clamped columns; temp = (g / gauss_norm, box)
-    for (int idx = tid; idx < XH * PW; idx += blockDim.x) {
-        int rr = idx / PW, cc = idx - rr * PW;
+    TileRowCol rp(tid, (int)blockDim.x, PW);
+    for (int idx = tid; idx < XH * PW; idx += blockDim.x, rp.advance()) {
+        const int rr = rp.r, cc = rp.c;
         const float* rowp = sraw + rr * RW + cc;
         const int gcol = pc0 + cc;
         float gs = 0.0f, cs = 0.0f;
@@ -96,8 +98,9 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
 
     // preprocess_cols.wgsl:29-59
     const float trunc_thr = 1.0f / 255.0f;
-    for (int idx = tid; idx < PH * PW; idx += blockDim.x) {
-        int pr = idx / PW, pc = idx - pr * PW;
+    TileRowCol cp(tid, (int)blockDim.x, PW);
+    for (int idx = tid; idx < PH * PW; idx += blockDim.x, cp.advance()) {
+        const int pr = cp.r, pc = cp.c;
         int grow = pr0 + pr, gcol = pc0 + pc;
         if (grow < 0 || grow >= H || gcol < 0 || gcol >= W) {
             sp[idx] = -INFINITY;  // outside the frame: never part of a dilation window
@@ -138,8 +141,9 @@ bandpass_kernel(const T* __restrict__ frames, int64_t frame_stride, float* __res
 
     // max_rows.wgsl + extract_max.wgsl: the pixel is a candidate iff no value in
     // its kd x kd window (out-of-frame cells skipped) exceeds it
-    for (int idx = tid; idx < TH * PW; idx += blockDim.x) {
-        int r = idx / PW, cc = idx - r * PW;
+    TileRowCol mp(tid, (int)blockDim.x, PW);
+    for (int idx = tid; idx < TH * PW; idx += blockDim.x, mp.advance()) {
+        const int r = mp.r, cc = mp.c;
         float m = -INFINITY;
         for (int j = 0; j < kd; j++) m = fmaxf(m, sp[(r + j) * PW + cc]);
         sv[idx] = m;

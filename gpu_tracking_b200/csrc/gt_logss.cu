@@ -153,11 +153,19 @@ __device__ __forceinline__ void ss_hchain(const float* __restrict__ p, const flo
     for (int c = 0; c < kSSCB; c++) acc[c] = 0.0f;
 #pragma unroll
     for (int j0 = 0; j0 < NT; j0 += kSSChunk) {
+        // the window is read in 8-byte pairs (p + j0 is 8-byte aligned: even
+        // row stride, even task column, even chunk); a pair's second value
+        // past the window is a loaded but unused float of the same tile row
+        // or the next one
         constexpr int NXC = kSSChunk + kSSCB - 1;
-        float x[NXC];
+        float x[NXC + 1];
 #pragma unroll
-        for (int m = 0; m < NXC; m++)
-            if (j0 + m < NT + kSSCB - 1) x[m] = p[j0 + m];
+        for (int m = 0; m < NXC; m += 2)
+            if (j0 + m < NT + kSSCB - 1) {
+                const float2 v2 = *reinterpret_cast<const float2*>(p + j0 + m);
+                x[m] = v2.x;
+                x[m + 1] = v2.y;
+            }
 #pragma unroll
         for (int jj = 0; jj < kSSChunk; jj++) {
             if (j0 + jj < NT) {
@@ -283,23 +291,24 @@ log_scale_space_kernel(const T* __restrict__ frames, int64_t frame_stride, const
     // raw tile: rows r0 - 1 - RMAX .., columns c0 - 1 - RMAX .., zero outside
     // the frame; kSSBatch independent loads per thread are in flight before
     // their shared-memory stores
+    // each thread's elements (row, column) stepped without a division per element
     const int gr0 = r0 - 1 - rmax, gc0 = c0 - 1 - rmax;
-    const int nraw = g.RH * g.RW;
-    for (int i0 = 0; i0 < nraw; i0 += kSSBatch * kSSThreads) {
+    TileRowCol rc(threadIdx.x, kSSThreads, g.RW);
+    while (rc.r < g.RH) {
         float v[kSSBatch];
+        int at[kSSBatch];
 #pragma unroll
         for (int b = 0; b < kSSBatch; b++) {
-            const int i = i0 + b * kSSThreads + threadIdx.x;
-            const int rr = i / g.RW, cc = i - rr * g.RW;
+            const int rr = rc.r, cc = rc.c;
             const int gr = gr0 + rr, gc = gc0 + cc;
-            v[b] = (i < nraw && gr >= 0 && gr < H && gc >= 0 && gc < W) ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+            const bool in_tile = rr < g.RH;
+            at[b] = in_tile ? rr * kSSRW + cc : -1;
+            v[b] = (in_tile && gr >= 0 && gr < H && gc >= 0 && gc < W) ? load_px<T>(img, (size_t)gr * W + gc) : 0.0f;
+            rc.advance();
         }
 #pragma unroll
-        for (int b = 0; b < kSSBatch; b++) {
-            const int i = i0 + b * kSSThreads + threadIdx.x;
-            const int rr = i / g.RW, cc = i - rr * g.RW;
-            if (i < nraw) raw[rr * kSSRW + cc] = v[b];
-        }
+        for (int b = 0; b < kSSBatch; b++)
+            if (at[b] >= 0) raw[at[b]] = v[b];
     }
     __syncthreads();
     for (int k = 0; k < n; k++) {
