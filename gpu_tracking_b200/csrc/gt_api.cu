@@ -769,8 +769,14 @@ gt_status locate_pass(gt_ctx* ctx, const gt_params& p, const T* frames, bool on_
                 } else {
                     {
                         Prof pf(ctx, "bandpass");
-                        CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
-                                              ctx->st));
+                        cudaError_t es = cudaSuccess;
+                        if (launch_strip_processed<TS>(src, (int64_t)npx, proc, c, nf, ctx->cand_count.as<uint32_t>(),
+                                                       ctx->cand_keys.as<uint32_t>(), flags, ctx->st, &es)) {
+                            CK(es);
+                        } else {
+                            CK(launch_bandpass<TS>(src, (int64_t)npx, proc, c, nf, false, nullptr, nullptr, 0, flags,
+                                                  ctx->st));
+                        }
                     }
                     if (lt->fused()) {
                         Prof pf(ctx, "log_scale_space");

@@ -162,6 +162,15 @@ template <typename T>
 bool launch_strip(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                   uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags, cudaStream_t st,
                   cudaError_t* err);
+// The processed image alone through the strip kernel, for smoothing radii
+// 3..10 (the LoG style's bandpass, which takes no local-maximum candidates):
+// the same processed values as bandpass_kernel<T, false>.  False when the
+// radius has no specialisation or integer pixels lack the proven division;
+// cand_count / cand_keys are never written.
+template <typename T>
+bool launch_strip_processed(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c,
+                            int nframes, uint32_t* cand_count, uint32_t* cand_keys, uint32_t* flags, cudaStream_t st,
+                            cudaError_t* err);
 
 // True when fma(x, zh, x*zl) equals IEEE x/d for every x in [1, 2) (checked
 // on the device once per (d, zh, zl) and remembered).

@@ -829,7 +829,8 @@ template <typename T, int R, int KD, bool FAST>
 cudaError_t strip_launch(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c, int nframes,
                          uint32_t* cand_count, uint32_t* cand_keys, uint32_t cand_cap, uint32_t* flags,
                          cudaStream_t st) {
-    const int SH = c.H > 1024 ? 512 : c.H;
+    // row segments of at most 512 rows: enough CTAs for whole waves at 1024 rows and up
+    const int SH = c.H > 512 ? 512 : c.H;
     dim3 grid((c.W + kStripTW - 1) / kStripTW, (c.H + SH - 1) / SH, nframes);
     const size_t smem = strip_smem<T, R, KD>();
     // 4-pixel loads need every row start (and the frames) aligned to 4 pixels
@@ -918,12 +919,45 @@ int strip_tile_width(const LocateConsts& c) {
     return 0;
 }
 
+// Processed image only: the dilation width is fixed at 8 (the smallest the
+// tile geometry supports; the processed values do not depend on it) and the
+// margin covers the whole frame, so the candidate test rejects every pixel
+// (NaN and infinite values included) and no candidate list is touched.
+#define GT_STRIP_PROC_CASES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+constexpr int kStripProcKD = 8;
+
+template <typename T>
+bool launch_strip_processed(const T* frames, int64_t frame_stride, float* processed, const LocateConsts& c,
+                            int nframes, uint32_t* cand_count, uint32_t* cand_keys, uint32_t* flags, cudaStream_t st,
+                            cudaError_t* err) {
+    constexpr bool kInt = IsIntPix<T>::value;
+    if (kInt && !c.fast_div) return false;
+    LocateConsts cb = c;
+    cb.kd = kStripProcKD;
+    cb.o = (int32_t)((float)kStripProcKD / 2.0f - 0.5f);
+    cb.margin = c.H > c.W ? c.H : c.W;
+    cb.skip_zero = 0;
+    cb.frame_std = nullptr;
+    cb.thr = 0.0f;
+#define GT_STRIP_PROC_TRY(RR)                                                                                  \
+    if (c.R == RR) {                                                                                           \
+        *err = strip_launch<T, RR, kStripProcKD, kInt>(frames, frame_stride, processed, cb, nframes, cand_count, \
+                                                       cand_keys, 0, flags, st);                               \
+        return true;                                                                                           \
+    }
+    GT_STRIP_PROC_CASES(GT_STRIP_PROC_TRY)
+#undef GT_STRIP_PROC_TRY
+    return false;
+}
+
 #define GT_STRIP_RAGGED_INST(T)                                                                                  \
     template bool launch_strip_ragged<T>(const RaggedFrame*, const StripTask*, const int32_t*, int, float*,      \
                                          const LocateConsts&, uint32_t*, uint32_t*, uint32_t, uint32_t*,         \
                                          cudaStream_t, cudaError_t*);                                            \
     template int strip_blocks_per_sm<T>(const LocateConsts&);                                                    \
-    template int strip_tile_width<T>(const LocateConsts&);
+    template int strip_tile_width<T>(const LocateConsts&);                                                       \
+    template bool launch_strip_processed<T>(const T*, int64_t, float*, const LocateConsts&, int, uint32_t*,      \
+                                            uint32_t*, uint32_t*, cudaStream_t, cudaError_t*);
 GT_STRIP_RAGGED_INST(uint16_t)
 GT_STRIP_RAGGED_INST(float)
 GT_STRIP_RAGGED_INST(uint8_t)
